@@ -1,0 +1,943 @@
+// Host side of the B200 ring-Ising statevector engine: pass planner,
+// scheduler, buffer ownership and the C ABI declared in include/rsv.h.
+//
+// Reference counterparts (zzEncounter/GPU_Simulation):
+//   RingIsingCudaBackend::Impl            cpp/ising_cuda_backend.cu:333-404
+//   build_structured_forward_rotation_chunks / apply_structured_forward_layers
+//                                         cpp/ising_cuda_structured_adjoint_modes.inc:18-148
+//   run_structured_backward_sweep         cpp/ising_cuda_structured_adjoint_modes.inc:188-307
+//   run_energy_and_grad_structured_adjoint cpp/ising_cuda_structured_adjoint_modes.inc:309-373
+//   StageProfiler                         cpp/ising_cuda_backend.cu:24-106
+//   benchmark_structured_forward_graph    cpp/ising_cuda_backend.cu:444-541
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/rsv.h"
+#include "rsv_device.cuh"
+#include "rsv_launch.h"
+#include "rsv_types.h"
+
+namespace rsv {
+namespace {
+
+thread_local std::string g_last_error;
+
+struct Error : std::runtime_error {
+  rsv_status status;
+  Error(rsv_status s, const std::string &m) : std::runtime_error(m), status(s) {}
+};
+
+void check(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return;
+  const rsv_status s = (e == cudaErrorMemoryAllocation) ? RSV_ERR_OUT_OF_MEMORY : RSV_ERR_CUDA;
+  throw Error(s, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+[[noreturn]] void invalid(const std::string &m) { throw Error(RSV_ERR_INVALID_ARGUMENT, m); }
+
+// ------------------------------------------------------------------------
+// Planner
+// ------------------------------------------------------------------------
+
+struct Tile {
+  u64 vec[12]{};
+  int gate_wire[12];
+  int num_runs = 0;
+  int run_start[4]{};
+  int run_len[4]{};
+  u64 num_tiles = 1;
+  bool unit = true;
+  Tile() { std::fill(gate_wire, gate_wire + 12, -1); }
+};
+
+// Tile whose 12 directions are the unit vectors of `bits` (physical bit
+// indices); `phys` is the number of physical index bits.  Gates are placed on
+// the tile bits whose physical bit is listed in `gates`.
+Tile unit_tile(int phys, const std::vector<int> &bits, const std::vector<int> &gates) {
+  if (bits.size() != 12) throw Error(RSV_ERR_INTERNAL, "tile needs 12 directions");
+  Tile t;
+  std::vector<bool> in(phys, false);
+  for (int b = 0; b < 12; ++b) {
+    t.vec[b] = u64{1} << bits[b];
+    in[bits[b]] = true;
+    if (std::find(gates.begin(), gates.end(), bits[b]) != gates.end()) t.gate_wire[b] = bits[b];
+  }
+  for (int p = 0; p < phys;) {
+    if (in[p]) {
+      ++p;
+      continue;
+    }
+    int q = p;
+    while (q < phys && !in[q]) ++q;
+    if (t.num_runs == kMaxRuns) throw Error(RSV_ERR_INTERNAL, "too many coset runs");
+    t.run_start[t.num_runs] = p;
+    t.run_len[t.num_runs] = q - p;
+    ++t.num_runs;
+    p = q;
+  }
+  t.num_tiles = u64{1} << (phys - 12);
+  return t;
+}
+
+// "Antipodal" tile span(e_0..e_10, all-ones): its image under P^{-1} is the
+// contiguous block span(e_0..e_11), so a scatter through P^{-1} from it writes
+// whole 4096-amplitude blocks.  Gates on wires 0..10.  Needs n >= 13.
+Tile antipodal_tile(int n) {
+  Tile t;
+  for (int b = 0; b < 11; ++b) {
+    t.vec[b] = u64{1} << b;
+    t.gate_wire[b] = b;
+  }
+  t.vec[11] = (u64{1} << n) - 1;
+  t.num_runs = 1;
+  t.run_start[0] = 11;
+  t.run_len[0] = n - 12;
+  t.num_tiles = u64{1} << (n - 12);
+  t.unit = false;
+  return t;
+}
+
+// Split wires [lo, n) into high tiles with `c` contiguous low bits each;
+// c is chosen to minimise the number of passes, then maximised (longer DRAM
+// segments).  Returns the tiles (gates on the split wires).
+std::vector<Tile> high_tiles(int n, int lo, int min_c = 2) {
+  std::vector<Tile> out;
+  const int m = n - lo;
+  if (m <= 0) return out;
+  int best_c = min_c, best_passes = 1 << 30;
+  for (int c = min_c; c <= 10; ++c) {
+    const int g = 12 - c;
+    if (c > lo) break;  // contiguity bits must lie below the gated wires
+    const int passes = (m + g - 1) / g;
+    if (passes < best_passes || (passes == best_passes && c > best_c)) {
+      best_passes = passes;
+      best_c = c;
+    }
+  }
+  const int g = 12 - best_c;
+  for (int start = lo; start < n; start += g) {
+    const int end = std::min(n, start + g);
+    std::vector<int> gates;
+    for (int w = start; w < end; ++w) gates.push_back(w);
+    const int cprime = 12 - static_cast<int>(gates.size());
+    std::vector<int> bits;
+    for (int b = 0; b < cprime; ++b) bits.push_back(b);
+    for (int w : gates) bits.push_back(w);
+    out.push_back(unit_tile(n, bits, gates));
+  }
+  return out;
+}
+
+struct Step {
+  bool bwd = false;
+  int layer = 0;
+  Tile tile;
+  int psi_load = kLoadNatural, lam_load = kLoadNatural;
+  int psi_store = kStoreNatural, lam_store = kStoreNone;
+  int phase = 0, phi_grad = 0;
+  int psi_in = -1, psi_out = -1, lam_in = -1, lam_out = -1;
+  int pass_index = -1;  // backward partial record
+  int grid = 1;
+};
+
+struct Plan {
+  int n = 0, L = 0, phys = 0;
+  std::vector<Step> fwd, bwd;
+  int chi_buf = 0, mu_buf = 1;
+  std::vector<int> theta_pass, theta_slot, phi_pass;
+  int max_grid = 1;
+};
+
+Plan make_plan(int n, int L, int sms) {
+  Plan pl;
+  pl.n = n;
+  pl.L = L;
+  pl.phys = std::max(n, kTileBits);
+  const bool single = (pl.phys == kTileBits);
+  const int fwd_ctas = std::max(1, 2 * sms), bwd_ctas = std::max(1, sms);
+
+  std::vector<int> all_bits(12), real_wires;
+  for (int b = 0; b < 12; ++b) all_bits[b] = b;
+  for (int w = 0; w < std::min(n, 12); ++w) real_wires.push_back(w);
+
+  std::vector<Tile> fwd_tiles, bwd_tiles;
+  if (single) {
+    fwd_tiles.push_back(unit_tile(pl.phys, all_bits, real_wires));
+    bwd_tiles.push_back(unit_tile(pl.phys, all_bits, real_wires));
+  } else {
+    fwd_tiles = high_tiles(n, 12);
+    fwd_tiles.insert(fwd_tiles.begin(), unit_tile(n, all_bits, all_bits));
+    bwd_tiles = high_tiles(n, 11);
+    std::reverse(bwd_tiles.begin(), bwd_tiles.end());  // highest wires first
+    bwd_tiles.push_back(antipodal_tile(n));
+  }
+  auto grid_for = [](const Tile &t, int ctas) {
+    return static_cast<int>(std::min<u64>(t.num_tiles, static_cast<u64>(ctas)));
+  };
+
+  // Forward.  Layer 0 is the analytic product state; layers 1..L-1 run
+  // their passes; the last pass of each layer applies the RZ phase and, except
+  // for the final layer, scatters through P into the other buffer.
+  int cur = 0, other = 1;
+  if (L == 1) {
+    Step s;
+    s.tile = unit_tile(pl.phys, all_bits, {});
+    s.psi_load = kLoadProductPlain;
+    s.psi_out = cur;
+    s.psi_store = kStoreNatural;
+    s.grid = grid_for(s.tile, fwd_ctas);
+    pl.fwd.push_back(s);
+  }
+  for (int layer = 1; layer < L; ++layer) {
+    for (size_t gi = 0; gi < fwd_tiles.size(); ++gi) {
+      const bool first = gi == 0, last = gi + 1 == fwd_tiles.size();
+      Step s;
+      s.layer = layer;
+      s.tile = fwd_tiles[gi];
+      s.psi_load = first ? (layer == 1 ? kLoadProduct : kLoadNatural) : kLoadNatural;
+      s.psi_in = (s.psi_load == kLoadNatural) ? cur : -1;
+      s.phase = last ? 1 : 0;
+      if (last && layer + 1 < L) {
+        s.psi_store = kStoreScatterP;
+        s.psi_out = other;
+        std::swap(cur, other);
+      } else {
+        s.psi_store = kStoreNatural;
+        s.psi_out = cur;
+      }
+      s.grid = grid_for(s.tile, fwd_ctas);
+      pl.fwd.push_back(s);
+    }
+  }
+  pl.chi_buf = cur;
+  pl.mu_buf = other;
+
+  // Backward.  Buffers: psi, lam, and one free.  The first pass of layer l
+  // gathers lambda through P (undoing the ring of layer l+1) into the free
+  // buffer; the last pass scatters psi through P^{-1} into the free buffer.
+  int psi = cur, lam = other, freeb = 3 - cur - other;
+  pl.theta_pass.assign(static_cast<size_t>(n) * L, -1);
+  pl.theta_slot.assign(static_cast<size_t>(n) * L, -1);
+  pl.phi_pass.assign(L, -1);
+  int pass_index = 0;
+  for (int layer = L - 1; layer >= 0; --layer) {
+    for (size_t gi = 0; gi < bwd_tiles.size(); ++gi) {
+      const bool first = gi == 0, last = gi + 1 == bwd_tiles.size();
+      Step s;
+      s.bwd = true;
+      s.layer = layer;
+      s.tile = bwd_tiles[gi];
+      s.phase = first ? 1 : 0;
+      s.phi_grad = first ? 1 : 0;
+      if (s.phi_grad && !s.tile.unit) throw Error(RSV_ERR_INTERNAL, "phi pass needs a unit tile");
+      s.psi_load = kLoadNatural;
+      s.psi_in = psi;
+      s.lam_load = (first && layer + 1 < L) ? kLoadGatherP : kLoadNatural;
+      s.lam_in = lam;
+      const bool scatter_psi = last && layer > 0;
+      const bool final_pass = last && layer == 0;
+      if (single) {
+        // One CTA holds the whole state: every permutation is done in place.
+        s.psi_out = psi;
+        s.lam_out = lam;
+        s.psi_store = final_pass ? kStoreNone : (scatter_psi ? kStoreScatterPinv : kStoreNatural);
+        s.lam_store = final_pass ? kStoreNone : kStoreNatural;
+      } else {
+        if (s.lam_load == kLoadGatherP) {
+          s.lam_out = freeb;
+          freeb = lam;
+          lam = s.lam_out;
+        } else {
+          s.lam_out = lam;
+        }
+        s.lam_store = final_pass ? kStoreNone : kStoreNatural;
+        if (scatter_psi) {
+          s.psi_store = kStoreScatterPinv;
+          s.psi_out = freeb;
+          freeb = psi;
+          psi = s.psi_out;
+        } else {
+          s.psi_store = final_pass ? kStoreNone : kStoreNatural;
+          s.psi_out = psi;
+        }
+      }
+      s.pass_index = pass_index++;
+      s.grid = grid_for(s.tile, bwd_ctas);
+      for (int b = 0; b < 12; ++b) {
+        const int w = s.tile.gate_wire[b];
+        if (w < 0) continue;
+        const size_t k = static_cast<size_t>(layer) * n + w;
+        if (pl.theta_pass[k] >= 0) throw Error(RSV_ERR_INTERNAL, "wire planned twice");
+        pl.theta_pass[k] = s.pass_index;
+        pl.theta_slot[k] = b;
+      }
+      if (first) pl.phi_pass[layer] = s.pass_index;
+      pl.max_grid = std::max(pl.max_grid, s.grid);
+      pl.bwd.push_back(s);
+    }
+  }
+  for (size_t k = 0; k < pl.theta_pass.size(); ++k)
+    if (pl.theta_pass[k] < 0) throw Error(RSV_ERR_INTERNAL, "wire without a backward pass");
+  return pl;
+}
+
+const char *load_name(int m) {
+  switch (m) {
+    case kLoadNatural: return "load";
+    case kLoadGatherP: return "gatherP";
+    case kLoadProduct: return "product(P)";
+    case kLoadProductPlain: return "product";
+  }
+  return "?";
+}
+
+const char *store_name(int m) {
+  switch (m) {
+    case kStoreNatural: return "store";
+    case kStoreScatterP: return "scatterP";
+    case kStoreScatterPinv: return "scatterPinv";
+    case kStoreNone: return "none";
+  }
+  return "?";
+}
+
+std::string describe(const Plan &pl) {
+  std::ostringstream os;
+  auto tile_str = [](const Tile &t) {
+    std::ostringstream ts;
+    ts << "dirs=[";
+    for (int b = 0; b < 12; ++b) {
+      if (b) ts << ",";
+      if ((t.vec[b] & (t.vec[b] - 1)) == 0) {
+        int bit = 0;
+        while (!((t.vec[b] >> bit) & 1)) ++bit;
+        ts << bit;
+      } else {
+        ts << "0x" << std::hex << t.vec[b] << std::dec;
+      }
+    }
+    ts << "] gates=[";
+    bool any = false;
+    for (int b = 0; b < 12; ++b)
+      if (t.gate_wire[b] >= 0) {
+        ts << (any ? "," : "") << t.gate_wire[b];
+        any = true;
+      }
+    ts << "] runs=[";
+    for (int r = 0; r < t.num_runs; ++r) ts << (r ? "," : "") << t.run_start[r] << ":" << t.run_len[r];
+    ts << "] tiles=" << t.num_tiles;
+    return ts.str();
+  };
+  os << "n=" << pl.n << " L=" << pl.L << " phys=" << pl.phys << "\n";
+  for (const auto &s : pl.fwd)
+    os << "fwd layer=" << s.layer << " " << tile_str(s.tile) << " psi:" << load_name(s.psi_load)
+       << "(" << s.psi_in << ")->" << store_name(s.psi_store) << "(" << s.psi_out << ")"
+       << (s.phase ? " phase" : "") << " grid=" << s.grid << "\n";
+  os << "energy chi=" << pl.chi_buf << " mu=" << pl.mu_buf << "\n";
+  for (const auto &s : pl.bwd)
+    os << "bwd layer=" << s.layer << " pass=" << s.pass_index << " " << tile_str(s.tile)
+       << " psi:" << load_name(s.psi_load) << "(" << s.psi_in << ")->" << store_name(s.psi_store)
+       << "(" << s.psi_out << ") lam:" << load_name(s.lam_load) << "(" << s.lam_in << ")->"
+       << store_name(s.lam_store) << "(" << s.lam_out << ")" << (s.phase ? " phase" : "")
+       << (s.phi_grad ? " phi" : "") << " grid=" << s.grid << "\n";
+  os << "finalize\n";
+  return os.str();
+}
+
+// ------------------------------------------------------------------------
+// Backend
+// ------------------------------------------------------------------------
+
+template <typename T>
+struct DevBuf {
+  T *p = nullptr;
+  size_t count = 0;
+  void alloc(size_t n) {
+    release();
+    if (n == 0) return;
+    check(cudaMalloc(&p, n * sizeof(T)), "cudaMalloc");
+    count = n;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    count = 0;
+  }
+  ~DevBuf() { release(); }
+};
+
+template <typename T>
+struct HostBuf {
+  T *p = nullptr;
+  void alloc(size_t n) {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    if (n) check(cudaMallocHost(&p, n * sizeof(T)), "cudaMallocHost");
+  }
+  ~HostBuf() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
+constexpr int kNumStages = 8;
+const char *kStageNames[kNumStages] = {
+    "build_ops_host_ms",  "zero_state_ms",    "forward_apply_ms",  "hamiltonian_ms",
+    "energy_dot_ms",      "gradient_zero_ms", "backward_sweep_ms", "gradient_copy_ms"};
+
+}  // namespace
+}  // namespace rsv
+
+struct rsv_backend {
+  int n = 0, L = 0;
+  double field = 0.0;
+  size_t num_params = 0;
+  size_t state_len = 0;  // amplitudes per buffer (2^max(n,12))
+  int device = 0, sms = 0;
+  cudaStream_t stream = nullptr;
+  rsv::Plan plan;
+  rsv::DevBuf<double2> buf[3];
+  rsv::DevBuf<double4> coef;
+  rsv::DevBuf<double2> ptab, prod;
+  rsv::DevBuf<double> energy_partials, pass_partials, outputs;  // outputs: [1 + num_params]
+  rsv::DevBuf<int> tables;  // pass_grid | theta_pass | theta_slot | phi_pass
+  rsv::HostBuf<double4> coef_host;
+  rsv::HostBuf<double> out_host;
+  int energy_grid = 1;
+  int num_bwd_passes = 0;
+  // Bumped by every call that overwrites the state buffers; a forward-only
+  // call records its value so that a deferred backward can check it.
+  unsigned long long generation = 0;
+  bool forward_only_state = false;
+  // launch timing (rsv_set_launch_timing)
+  bool timing = false;
+  struct Rec {
+    cudaEvent_t a, b;
+    int kind;
+    double bytes;
+  };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> event_pool;
+};
+
+namespace rsv {
+namespace {
+
+void fill_pass_params(rsv_backend *B, const Step &s, PassParams &P) {
+  std::memset(&P, 0, sizeof(P));
+  P.n = B->n;
+  P.layer = s.layer;
+  P.num_runs = s.tile.num_runs;
+  for (int r = 0; r < 4; ++r) {
+    P.run_start[r] = s.tile.run_start[r];
+    P.run_len[r] = s.tile.run_len[r];
+  }
+  P.num_tiles = s.tile.num_tiles;
+  for (int b = 0; b < 32; ++b) P.wire_tile_bit[b] = -1;
+  bool l1 = false, l2 = false;
+  for (int b = 0; b < 12; ++b) {
+    P.vec[b] = s.tile.vec[b];
+    P.gate_wire[b] = s.tile.gate_wire[b];
+    if (s.tile.gate_wire[b] >= 0 && b < 8) l1 = true;
+    if (s.tile.gate_wire[b] >= 0 && b < 4) l2 = true;
+    if (s.tile.unit) {
+      int bit = 0;
+      while (!((s.tile.vec[b] >> bit) & 1)) ++bit;
+      if (bit < 32) P.wire_tile_bit[bit] = b;
+    }
+  }
+  P.need_l1 = l1 ? 1 : 0;
+  P.need_l2 = l2 ? 1 : 0;
+  P.psi_load = s.psi_load;
+  P.lam_load = s.lam_load;
+  P.psi_store = s.psi_store;
+  P.lam_store = s.lam_store;
+  P.phase = s.phase;
+  P.phi_grad = s.phi_grad;
+  P.sync_after_load = (s.tile.num_tiles == 1) ? 1 : 0;
+  P.psi_in = s.psi_in >= 0 ? B->buf[s.psi_in].p : nullptr;
+  P.psi_out = s.psi_out >= 0 ? B->buf[s.psi_out].p : nullptr;
+  P.lam_in = s.lam_in >= 0 ? B->buf[s.lam_in].p : nullptr;
+  P.lam_out = s.lam_out >= 0 ? B->buf[s.lam_out].p : nullptr;
+  P.coef = B->coef.p;
+  P.ptab = B->ptab.p + static_cast<size_t>(s.layer) * 1024;
+  P.prod = B->prod.p;
+  P.partials = s.bwd ? B->pass_partials.p + static_cast<size_t>(s.pass_index) * B->plan.max_grid *
+                                                 kPartialStride
+                     : nullptr;
+}
+
+cudaEvent_t take_event(rsv_backend *B) {
+  if (!B->event_pool.empty()) {
+    cudaEvent_t e = B->event_pool.back();
+    B->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  check(cudaEventCreate(&e), "cudaEventCreate");
+  return e;
+}
+
+// Launch `body` and, when launch timing is on, bracket it with events.
+template <typename F>
+void timed(rsv_backend *B, cudaStream_t st, int kind, double bytes, F &&body) {
+  if (!B->timing) {
+    body();
+    return;
+  }
+  rsv_backend::Rec r{take_event(B), take_event(B), kind, bytes};
+  check(cudaEventRecord(r.a, st), "cudaEventRecord");
+  body();
+  check(cudaEventRecord(r.b, st), "cudaEventRecord");
+  B->recs.push_back(r);
+}
+
+// Minimum DRAM bytes of a pass: 16 B per amplitude for every buffer it must
+// read (gathers and natural loads) and every buffer it must write.
+double pass_bytes(const rsv_backend *B, const Step &s) {
+  const double amp = 16.0 * static_cast<double>(u64{1} << B->n);
+  double k = 0.0;
+  if (s.psi_load == kLoadNatural || s.psi_load == kLoadGatherP) k += 1;
+  if (s.psi_store != kStoreNone) k += 1;
+  if (s.bwd) {
+    if (s.lam_load == kLoadNatural || s.lam_load == kLoadGatherP) k += 1;
+    if (s.lam_store != kStoreNone) k += 1;
+  }
+  return k * amp;
+}
+
+void run_forward(rsv_backend *B, cudaStream_t st) {
+  PassParams P;
+  for (const auto &s : B->plan.fwd) {
+    fill_pass_params(B, s, P);
+    timed(B, st, 1, pass_bytes(B, s),
+          [&] { check(launch_pass(P, false, s.grid, st), "forward pass launch"); });
+  }
+}
+
+void run_energy(rsv_backend *B, cudaStream_t st) {
+  const double bytes = 2.0 * 16.0 * static_cast<double>(u64{1} << B->n);
+  timed(B, st, 2, bytes, [&] {
+    check(launch_energy(B->buf[B->plan.chi_buf].p, B->buf[B->plan.mu_buf].p, B->n, B->field,
+                        u64{1} << B->n, B->energy_partials.p, B->energy_grid, st),
+          "energy launch");
+  });
+}
+
+void run_backward(rsv_backend *B, cudaStream_t st) {
+  PassParams P;
+  for (const auto &s : B->plan.bwd) {
+    fill_pass_params(B, s, P);
+    timed(B, st, 3, pass_bytes(B, s),
+          [&] { check(launch_pass(P, true, s.grid, st), "backward pass launch"); });
+  }
+}
+
+void run_finalize(rsv_backend *B, bool grad, double *energy_out, double *grad_out,
+                  cudaStream_t st) {
+  FinalizeParams F{};
+  F.n = B->n;
+  F.L = B->L;
+  F.num_energy_partials = B->energy_grid;
+  F.energy_partials = B->energy_partials.p;
+  F.pass_partials = B->pass_partials.p;
+  F.max_grid = B->plan.max_grid;
+  const int np = B->num_bwd_passes;
+  const size_t nl = static_cast<size_t>(B->n) * B->L;
+  F.pass_grid = B->tables.p;
+  F.theta_pass = B->tables.p + np;
+  F.theta_slot = B->tables.p + np + nl;
+  F.phi_pass = B->tables.p + np + 2 * nl;
+  F.energy_out = energy_out;
+  F.grad_out = grad ? grad_out : nullptr;
+  timed(B, st, 4, 0.0, [&] { check(launch_finalize(F, st), "finalize launch"); });
+}
+
+void upload_host_coefs(rsv_backend *B, const double *params, cudaStream_t st) {
+  // cos/sin of the half angles on the host, exactly as the reference
+  // (cpp/ising_cuda_rotation_kernels.cu:661-675).
+  const size_t count = static_cast<size_t>(B->n) * B->L;
+  for (size_t k = 0; k < count; ++k) {
+    const double ry = params[2 * k] * 0.5, rz = params[2 * k + 1] * 0.5;
+    B->coef_host.p[k] = make_double4(std::cos(ry), std::sin(ry), std::cos(rz), std::sin(rz));
+  }
+  check(cudaMemcpyAsync(B->coef.p, B->coef_host.p, count * sizeof(double4),
+                        cudaMemcpyHostToDevice, st),
+        "coefficient upload");
+}
+
+void run_all(rsv_backend *B, bool grad, double *energy_out, double *grad_out, cudaStream_t st) {
+  ++B->generation;
+  B->forward_only_state = false;
+  timed(B, st, 0, 0.0, [&] {
+    check(launch_tables(B->coef.p, B->n, B->L, B->ptab.p, B->prod.p, st), "tables launch");
+  });
+  run_forward(B, st);
+  run_energy(B, st);
+  if (grad) run_backward(B, st);
+  run_finalize(B, grad, energy_out, grad_out, st);
+}
+
+cudaStream_t pick_stream(rsv_backend *B, void *stream) {
+  return stream ? static_cast<cudaStream_t>(stream) : B->stream;
+}
+
+void validate_params(rsv_backend *B, const void *params, size_t num_params) {
+  if (B == nullptr) invalid("backend is null");
+  if (num_params != B->num_params) invalid("num_params does not match the circuit.");
+  if (params == nullptr) invalid("params is null");
+}
+
+template <typename F>
+rsv_status guarded(F &&f) {
+  try {
+    f();
+    g_last_error.clear();
+    return RSV_OK;
+  } catch (const Error &e) {
+    g_last_error = e.what();
+    return e.status;
+  } catch (const std::bad_alloc &) {
+    g_last_error = "host allocation failed";
+    return RSV_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception &e) {
+    g_last_error = e.what();
+    return RSV_ERR_INTERNAL;
+  }
+}
+
+bool configured = false;
+
+}  // namespace
+}  // namespace rsv
+
+using namespace rsv;
+
+extern "C" {
+
+const char *rsv_version(void) { return "rsv 0.1 (sm_100a)"; }
+
+const char *rsv_last_error(void) { return g_last_error.c_str(); }
+
+int rsv_num_stages(void) { return kNumStages; }
+
+const char *rsv_stage_name(int i) { return (i >= 0 && i < kNumStages) ? kStageNames[i] : ""; }
+
+unsigned long long rsv_ring_map(unsigned long long index, int num_qubits, int inverse) {
+  if (num_qubits < 2 || num_qubits > kMaxQubits) return 0;
+  return inverse ? ring_pinv(index, num_qubits) : ring_p(index, num_qubits);
+}
+
+rsv_status rsv_describe_plan(int num_qubits, int num_layers, char *buf, size_t buf_size,
+                             size_t *length_out) {
+  return guarded([&] {
+    if (num_qubits < 2 || num_qubits > kMaxQubits) invalid("num_qubits out of range");
+    if (num_layers < 1) invalid("num_layers must be at least 1");
+    const Plan pl = make_plan(num_qubits, num_layers, 148);
+    const std::string s = describe(pl);
+    if (length_out) *length_out = s.size();
+    if (buf && buf_size) {
+      const size_t k = std::min(buf_size - 1, s.size());
+      std::memcpy(buf, s.data(), k);
+      buf[k] = '\0';
+    }
+  });
+}
+
+rsv_status rsv_create(int num_qubits, int num_layers, double field, const char *gradient_strategy,
+                      int structured_rotation_chunk_width, int double_buffer, rsv_backend **out) {
+  return guarded([&] {
+    if (out == nullptr) invalid("out is null");
+    *out = nullptr;
+    const std::string strat = gradient_strategy ? gradient_strategy : "structured_adjoint";
+    if (strat != "structured_adjoint" && strat != "inverse_walk_cuQuantum" &&
+        strat != "inverse_walk_cuquantum" && strat != "dense_scan")
+      invalid(
+          "Unknown gradient strategy. Expected one of: inverse_walk_cuQuantum, "
+          "structured_adjoint, dense_scan.");
+    if (num_qubits < 2) invalid("num_qubits must be at least 2.");
+    if (num_qubits > kMaxQubits)
+      invalid("num_qubits exceeds the supported maximum of 31 (three state buffers must fit one GPU).");
+    if (num_layers < 1) invalid("num_layers must be at least 1.");
+    if (structured_rotation_chunk_width < 1)
+      invalid("structured_rotation_chunk_width must be at least 1.");
+    if (structured_rotation_chunk_width > 8)
+      invalid("structured_rotation_chunk_width exceeds supported maximum.");
+    if (strat == "dense_scan" && num_qubits > 8) invalid("dense_scan requires num_qubits <= 8.");
+    (void)double_buffer;
+
+    auto B = std::make_unique<rsv_backend>();
+    B->n = num_qubits;
+    B->L = num_layers;
+    B->field = field;
+    B->num_params = static_cast<size_t>(2) * num_qubits * num_layers;
+    check(cudaGetDevice(&B->device), "cudaGetDevice");
+    check(cudaDeviceGetAttribute(&B->sms, cudaDevAttrMultiProcessorCount, B->device),
+          "cudaDeviceGetAttribute");
+    if (!configured) {
+      check(configure_pass_kernels(), "configure pass kernels");
+      configured = true;
+    }
+    B->plan = make_plan(num_qubits, num_layers, B->sms);
+    B->num_bwd_passes = static_cast<int>(B->plan.bwd.size());
+    B->state_len = size_t{1} << B->plan.phys;
+    for (auto &b : B->buf) {
+      b.alloc(B->state_len);
+      check(cudaMemset(b.p, 0, B->state_len * sizeof(double2)), "state memset");
+    }
+    const size_t nl = static_cast<size_t>(num_qubits) * num_layers;
+    B->coef.alloc(nl);
+    B->ptab.alloc(static_cast<size_t>(num_layers) * 1024);
+    B->prod.alloc(1024);
+    B->energy_grid = static_cast<int>(std::min<u64>(
+        std::max<u64>(1, (u64{1} << num_qubits) / 256), static_cast<u64>(B->sms) * 8));
+    B->energy_partials.alloc(B->energy_grid);
+    B->pass_partials.alloc(static_cast<size_t>(std::max(1, B->num_bwd_passes)) * B->plan.max_grid *
+                           kPartialStride);
+    B->outputs.alloc(1 + B->num_params);
+    std::vector<int> tab;
+    for (const auto &s : B->plan.bwd) tab.push_back(s.grid);
+    tab.insert(tab.end(), B->plan.theta_pass.begin(), B->plan.theta_pass.end());
+    tab.insert(tab.end(), B->plan.theta_slot.begin(), B->plan.theta_slot.end());
+    tab.insert(tab.end(), B->plan.phi_pass.begin(), B->plan.phi_pass.end());
+    B->tables.alloc(tab.size());
+    check(cudaMemcpy(B->tables.p, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice),
+          "plan table upload");
+    B->coef_host.alloc(nl);
+    B->out_host.alloc(1 + B->num_params);
+    check(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    *out = B.release();
+  });
+}
+
+rsv_status rsv_destroy(rsv_backend *backend) {
+  return guarded([&] {
+    if (backend == nullptr) return;
+    cudaStreamSynchronize(backend->stream);
+    for (auto &r : backend->recs) {
+      cudaEventDestroy(r.a);
+      cudaEventDestroy(r.b);
+    }
+    for (auto e : backend->event_pool) cudaEventDestroy(e);
+    cudaStreamDestroy(backend->stream);
+    delete backend;
+  });
+}
+
+rsv_status rsv_energy_and_grad(rsv_backend *B, const double *params, size_t num_params,
+                               int compute_gradient, double *energy_out, double *gradient_out,
+                               void *stream) {
+  return guarded([&] {
+    validate_params(B, params, num_params);
+    if (energy_out == nullptr) invalid("energy_out is null");
+    if (compute_gradient && gradient_out == nullptr) invalid("gradient_out is null");
+    cudaStream_t st = pick_stream(B, stream);
+    upload_host_coefs(B, params, st);
+    const bool grad = compute_gradient != 0;
+    run_all(B, grad, B->outputs.p, B->outputs.p + 1, st);
+    const size_t count = grad ? 1 + B->num_params : 1;
+    check(cudaMemcpyAsync(B->out_host.p, B->outputs.p, count * sizeof(double),
+                          cudaMemcpyDeviceToHost, st),
+          "result download");
+    check(cudaStreamSynchronize(st), "energy_and_grad");
+    *energy_out = B->out_host.p[0];
+    if (grad) std::memcpy(gradient_out, B->out_host.p + 1, B->num_params * sizeof(double));
+  });
+}
+
+rsv_status rsv_energy_and_grad_device(rsv_backend *B, const double *d_params, size_t num_params,
+                                      double *d_energy_out, double *d_gradient_out, void *stream) {
+  return guarded([&] {
+    validate_params(B, d_params, num_params);
+    if (d_energy_out == nullptr) invalid("d_energy_out is null");
+    cudaStream_t st = pick_stream(B, stream);
+    timed(B, st, 0, 0.0, [&] {
+      check(launch_coef(d_params, B->coef.p, static_cast<int>(B->n * B->L), st), "coef launch");
+    });
+    run_all(B, d_gradient_out != nullptr, d_energy_out, d_gradient_out, st);
+  });
+}
+
+rsv_status rsv_forward_device(rsv_backend *B, const double *d_params, size_t num_params,
+                              double *d_energy_out, unsigned long long *generation_out,
+                              void *stream) {
+  return guarded([&] {
+    validate_params(B, d_params, num_params);
+    if (d_energy_out == nullptr) invalid("d_energy_out is null");
+    cudaStream_t st = pick_stream(B, stream);
+    check(launch_coef(d_params, B->coef.p, static_cast<int>(B->n * B->L), st), "coef launch");
+    run_all(B, false, d_energy_out, nullptr, st);
+    B->forward_only_state = true;
+    if (generation_out) *generation_out = B->generation;
+  });
+}
+
+rsv_status rsv_backward_device(rsv_backend *B, unsigned long long generation,
+                               double *d_gradient_out, void *stream) {
+  return guarded([&] {
+    if (B == nullptr) invalid("backend is null");
+    if (d_gradient_out == nullptr) invalid("d_gradient_out is null");
+    if (!B->forward_only_state || generation != B->generation)
+      invalid("backward needs the state of the matching forward; the backend ran another call since");
+    cudaStream_t st = pick_stream(B, stream);
+    run_backward(B, st);
+    // energy is rewritten with the same value into the outputs scratch slot
+    run_finalize(B, true, B->outputs.p, d_gradient_out, st);
+    B->forward_only_state = false;
+    ++B->generation;
+  });
+}
+
+rsv_status rsv_profile_energy_and_grad(rsv_backend *B, const double *params, size_t num_params,
+                                       int compute_gradient, double *energy_out,
+                                       double *gradient_out, double *stage_ms_out) {
+  return guarded([&] {
+    validate_params(B, params, num_params);
+    if (energy_out == nullptr || stage_ms_out == nullptr) invalid("output pointer is null");
+    if (compute_gradient && gradient_out == nullptr) invalid("gradient_out is null");
+    cudaStream_t st = B->stream;
+    cudaEvent_t ev[8];
+    for (auto &e : ev) check(cudaEventCreate(&e), "cudaEventCreate");
+    const bool grad = compute_gradient != 0;
+    for (int i = 0; i < kNumStages; ++i) stage_ms_out[i] = 0.0;
+    check(cudaStreamSynchronize(st), "profile pre-sync");
+    const auto t0 = std::chrono::steady_clock::now();
+    upload_host_coefs(B, params, st);
+    const auto t1 = std::chrono::steady_clock::now();
+    stage_ms_out[0] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    ++B->generation;
+    B->forward_only_state = false;
+    cudaEventRecord(ev[0], st);
+    check(launch_tables(B->coef.p, B->n, B->L, B->ptab.p, B->prod.p, st), "tables launch");
+    cudaEventRecord(ev[1], st);
+    run_forward(B, st);
+    cudaEventRecord(ev[2], st);
+    run_energy(B, st);
+    cudaEventRecord(ev[3], st);
+    if (grad) run_backward(B, st);
+    cudaEventRecord(ev[4], st);
+    run_finalize(B, grad, B->outputs.p, B->outputs.p + 1, st);
+    const size_t count = grad ? 1 + B->num_params : 1;
+    check(cudaMemcpyAsync(B->out_host.p, B->outputs.p, count * sizeof(double),
+                          cudaMemcpyDeviceToHost, st),
+          "result download");
+    cudaEventRecord(ev[5], st);
+    check(cudaStreamSynchronize(st), "profile");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    stage_ms_out[1] = ms;
+    cudaEventElapsedTime(&ms, ev[1], ev[2]);
+    stage_ms_out[2] = ms;
+    cudaEventElapsedTime(&ms, ev[2], ev[3]);
+    stage_ms_out[3] = ms;
+    cudaEventElapsedTime(&ms, ev[3], ev[4]);
+    stage_ms_out[6] = ms;
+    cudaEventElapsedTime(&ms, ev[4], ev[5]);
+    stage_ms_out[7] = ms;
+    for (auto &e : ev) cudaEventDestroy(e);
+    *energy_out = B->out_host.p[0];
+    if (grad) std::memcpy(gradient_out, B->out_host.p + 1, B->num_params * sizeof(double));
+  });
+}
+
+rsv_status rsv_benchmark_forward_graph(rsv_backend *B, const double *params, size_t num_params,
+                                       size_t repeats, double *normal_ms_out,
+                                       double *graph_ms_out) {
+  return guarded([&] {
+    validate_params(B, params, num_params);
+    if (repeats == 0) invalid("repeats must be at least 1.");
+    if (normal_ms_out == nullptr || graph_ms_out == nullptr) invalid("output pointer is null");
+    cudaStream_t st = B->stream;
+    ++B->generation;
+    B->forward_only_state = false;
+    upload_host_coefs(B, params, st);
+    auto forward = [&] {
+      check(launch_tables(B->coef.p, B->n, B->L, B->ptab.p, B->prod.p, st), "tables launch");
+      run_forward(B, st);
+    };
+    cudaEvent_t a, b;
+    check(cudaEventCreate(&a), "cudaEventCreate");
+    check(cudaEventCreate(&b), "cudaEventCreate");
+    forward();
+    check(cudaStreamSynchronize(st), "warmup");
+    auto time_ms = [&](auto &&body) {
+      cudaEventRecord(a, st);
+      for (size_t r = 0; r < repeats; ++r) body();
+      cudaEventRecord(b, st);
+      check(cudaEventSynchronize(b), "cudaEventSynchronize");
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, a, b);
+      return static_cast<double>(ms) / static_cast<double>(repeats);
+    };
+    *normal_ms_out = time_ms(forward);
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    forward();
+    check(cudaStreamEndCapture(st, &graph), "end capture");
+    check(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+    check(cudaGraphLaunch(exec, st), "graph warmup");
+    check(cudaStreamSynchronize(st), "graph warmup sync");
+    *graph_ms_out = time_ms([&] { check(cudaGraphLaunch(exec, st), "graph launch"); });
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  });
+}
+
+rsv_status rsv_set_launch_timing(rsv_backend *B, int enable) {
+  return guarded([&] {
+    if (B == nullptr) invalid("backend is null");
+    B->timing = enable != 0;
+  });
+}
+
+rsv_status rsv_launch_stats(rsv_backend *B, int *counts, double *total_ms, double *total_bytes) {
+  return guarded([&] {
+    if (B == nullptr) invalid("backend is null");
+    if (counts == nullptr || total_ms == nullptr || total_bytes == nullptr)
+      invalid("output pointer is null");
+    for (int k = 0; k < RSV_NUM_KINDS; ++k) {
+      counts[k] = 0;
+      total_ms[k] = 0.0;
+      total_bytes[k] = 0.0;
+    }
+    for (auto &r : B->recs) {
+      check(cudaEventSynchronize(r.b), "cudaEventSynchronize");
+      float ms = 0.f;
+      check(cudaEventElapsedTime(&ms, r.a, r.b), "cudaEventElapsedTime");
+      counts[r.kind] += 1;
+      total_ms[r.kind] += ms;
+      total_bytes[r.kind] += r.bytes;
+      B->event_pool.push_back(r.a);
+      B->event_pool.push_back(r.b);
+    }
+    B->recs.clear();
+  });
+}
+
+rsv_status rsv_backend_info(rsv_backend *B, int *num_qubits, int *num_layers, size_t *num_params,
+                            size_t *device_bytes) {
+  return guarded([&] {
+    if (B == nullptr) invalid("backend is null");
+    if (num_qubits) *num_qubits = B->n;
+    if (num_layers) *num_layers = B->L;
+    if (num_params) *num_params = B->num_params;
+    if (device_bytes)
+      *device_bytes = 3 * B->state_len * sizeof(double2) + B->pass_partials.count * sizeof(double) +
+                      B->energy_partials.count * sizeof(double);
+  });
+}
+
+}  // extern "C"

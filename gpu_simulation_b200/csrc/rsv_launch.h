@@ -1,0 +1,21 @@
+// Host-callable launchers of the kernels in rsv_kernels.cu.
+#pragma once
+
+#include <cstddef>
+#include <cuda_runtime.h>
+
+#include "rsv_types.h"
+
+namespace rsv {
+
+cudaError_t launch_coef(const double *params, double4 *coef, int count, cudaStream_t s);
+cudaError_t launch_tables(const double4 *coef, int n, int L, double2 *ptab, double2 *prod,
+                          cudaStream_t s);
+cudaError_t configure_pass_kernels();
+size_t pass_smem_bytes(bool bwd);
+cudaError_t launch_pass(const PassParams &P, bool bwd, int grid, cudaStream_t s);
+cudaError_t launch_energy(const double2 *chi, double2 *mu, int n, double field,
+                          unsigned long long size, double *partials, int grid, cudaStream_t s);
+cudaError_t launch_finalize(const FinalizeParams &F, cudaStream_t s);
+
+}  // namespace rsv

@@ -1,0 +1,75 @@
+// Host/device shared descriptors for the statevector pass kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace rsv {
+
+// How a pass obtains its input amplitudes.
+enum LoadMode : int {
+  kLoadNatural = 0,   // buf[p]
+  kLoadGatherP = 1,   // buf[P(p)]      (undo one ring layer: out = P^{-1} in)
+  kLoadProduct = 2,   // analytic layer-0 product state at P^{-1}(p) (= P applied to it)
+  kLoadProductPlain = 3,  // analytic layer-0 product state at p
+};
+
+// How a pass writes its output amplitudes.
+enum StoreMode : int {
+  kStoreNatural = 0,    // buf[p] = v
+  kStoreScatterP = 1,   // buf[P(p)] = v     (apply one ring layer)
+  kStoreScatterPinv = 2,// buf[P^{-1}(p)] = v (undo one ring layer)
+  kStoreNone = 3,
+};
+
+// Per-CTA partial record written by every backward pass (doubles):
+//   [0, 12)   theta partial sums per tile bit
+//   [16, 47)  phi: sum of Im(conj(lambda) psi) over amplitudes whose wire-w bit is 1
+//   [47]      phi: sum of Im(conj(lambda) psi) over all amplitudes
+constexpr int kPartialStride = 48;
+constexpr int kPartialPhi = 16;
+constexpr int kPartialTot = 47;
+
+struct PassParams {
+  int n;                 // real qubits
+  int layer;             // ansatz layer whose gates this pass applies
+  int num_runs;          // coset deposit runs (complement of the tile subspace)
+  int run_start[4];
+  int run_len[4];
+  unsigned long long num_tiles;
+  unsigned long long vec[12];  // physical XOR vector of each tile bit
+  int gate_wire[12];           // wire gated on tile bit b, or -1
+  int wire_tile_bit[32];       // tile bit of wire w for unit-vector tiles, or -1
+  int need_l1;                 // any gate on tile bits 0..7 (needs the second layout)
+  int need_l2;                 // any gate on tile bits 0..3 (needs the third layout)
+  int psi_load, lam_load;
+  int psi_store, lam_store;
+  int phase;                   // fwd: apply D after gates; bwd: apply D^dagger before gates
+  int phi_grad;                // bwd: accumulate the phi-gradient sums of the layer
+  int sync_after_load;         // single-tile in-place permutation: all loads before any store
+  const double2 *psi_in;
+  double2 *psi_out;
+  const double2 *lam_in;
+  double2 *lam_out;
+  const double4 *coef;         // [L * n] (cos t/2, sin t/2, cos p/2, sin p/2)
+  const double2 *ptab;         // phase byte tables of this layer, [4][256]
+  const double2 *prod;         // layer-0 product-state byte tables, [4][256]
+  double *partials;            // [gridDim.x][kPartialStride] for this pass
+};
+
+// Inputs of the deterministic final reduction (energy + gradient).
+struct FinalizeParams {
+  int n, L;
+  int num_energy_partials;
+  const double *energy_partials;
+  const double *pass_partials;   // [num_passes][max_grid][kPartialStride]
+  int max_grid;
+  const int *pass_grid;          // grid size of every pass
+  const int *theta_pass;         // [L*n]
+  const int *theta_slot;         // [L*n]
+  const int *phi_pass;           // [L]
+  double *energy_out;
+  double *grad_out;              // [2 L n] or null
+};
+
+}  // namespace rsv

@@ -1,0 +1,178 @@
+/*
+ * rsv.h -- C ABI of the B200 ring-Ising statevector engine (librsv.so).
+ *
+ * The engine computes the energy and the adjoint gradient of the ring-Ising
+ * VQE ansatz (layers of RY.RZ on every wire followed by the CNOT ring;
+ * H = -sum Z_i Z_{i+1} - h sum X_i) on a complex128 statevector, entirely on
+ * one NVIDIA B200 (sm_100a).  It is the drop-in replacement for the
+ * structured_adjoint path of zzEncounter/GPU_Simulation; each entry point
+ * names the reference interface it replaces.
+ *
+ * Conventions: params is a flat f64 array of 2*num_qubits*num_layers values,
+ * index (layer*num_qubits + wire)*2 + {0: theta of RY, 1: phi of RZ}
+ * (reference cpp/ising_cuda_backend.cu:131-133).  Gradients use the same
+ * layout.  Amplitude index bit w is wire w.
+ *
+ * Errors: every function returns an rsv_status; no C++ exception crosses
+ * this boundary.  rsv_last_error() returns a message for the calling thread.
+ * RSV_ERR_INVALID_ARGUMENT maps to the reference's std::invalid_argument
+ * (Python ValueError); every other non-zero status maps to its
+ * std::runtime_error (Python RuntimeError).
+ *
+ * Threading: one rsv_backend owns its device buffers and is not re-entrant
+ * (reference cpp/ising_cuda_backend.hpp:22-49); use one handle per thread.
+ */
+#ifndef RSV_H
+#define RSV_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum rsv_status {
+  RSV_OK = 0,
+  RSV_ERR_INVALID_ARGUMENT = 1,
+  RSV_ERR_CUDA = 2,
+  RSV_ERR_OUT_OF_MEMORY = 3,
+  RSV_ERR_UNSUPPORTED = 4,
+  RSV_ERR_INTERNAL = 5
+} rsv_status;
+
+typedef struct rsv_backend rsv_backend;
+
+/* Version string of the library. */
+const char *rsv_version(void);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *rsv_last_error(void);
+
+/* Number of stage timings reported by rsv_profile_energy_and_grad and the
+ * name of stage i (reference StageProfiler names, cpp/ising_cuda_backend.cu:24-106). */
+int rsv_num_stages(void);
+const char *rsv_stage_name(int i);
+
+/*
+ * Create a backend bound to the current CUDA device.
+ * Replaces RingIsingCudaBackend::RingIsingCudaBackend
+ * (reference cpp/ising_cuda_backend.hpp:26-29, cpp/ising_cuda_backend.cu:388-404,
+ *  bound at cpp/ising_cuda_bindings.cpp:74-80).
+ * gradient_strategy: "structured_adjoint", "inverse_walk_cuQuantum" (alias
+ * "inverse_walk_cuquantum") or "dense_scan"; all run the structured engine
+ * (their results agree to rounding).  structured_rotation_chunk_width must be
+ * in [1, 8] and double_buffer is accepted; both are validated as the
+ * reference does and otherwise ignored (the engine plans its own tiles).
+ * Allocates three state buffers of 16 * 2^max(n,12) bytes.
+ */
+rsv_status rsv_create(int num_qubits, int num_layers, double field,
+                      const char *gradient_strategy, int structured_rotation_chunk_width,
+                      int double_buffer, rsv_backend **out);
+
+/* Release a backend and its device memory.  Accepts NULL. */
+rsv_status rsv_destroy(rsv_backend *backend);
+
+/*
+ * Energy and (optionally) gradient from host parameters; synchronous.
+ * Replaces RingIsingCudaBackend::energy_and_grad(params, num_params,
+ * compute_gradient, profile=false) (reference cpp/ising_cuda_backend.cu:429-442,
+ * bound at cpp/ising_cuda_bindings.cpp:81-98).
+ * params: host f64[num_params]; gradient_out: host f64[num_params], written
+ * only when compute_gradient != 0 (may be NULL otherwise).
+ * stream: a cudaStream_t, or NULL for the backend's own stream.
+ */
+rsv_status rsv_energy_and_grad(rsv_backend *backend, const double *params, size_t num_params,
+                               int compute_gradient, double *energy_out, double *gradient_out,
+                               void *stream);
+
+/*
+ * Same computation with DEVICE pointers, asynchronous on `stream` (no host
+ * synchronisation, no host copies).  Used by the torch.autograd path.
+ * d_params: device f64[num_params]; d_energy_out: device f64[1];
+ * d_gradient_out: device f64[num_params] or NULL for energy only.
+ * No reference counterpart (the reference always round-trips through the host).
+ */
+rsv_status rsv_energy_and_grad_device(rsv_backend *backend, const double *d_params,
+                                      size_t num_params, double *d_energy_out,
+                                      double *d_gradient_out, void *stream);
+
+/*
+ * Split form of rsv_energy_and_grad_device for autograd: rsv_forward_device
+ * runs the forward sweep and the energy (d_energy_out, device f64[1]) and
+ * keeps the final state and lambda = H psi on the device; a later
+ * rsv_backward_device runs only the adjoint sweep and writes the gradient of
+ * that same forward (d_gradient_out, device f64[num_params]).  *generation_out
+ * (may be NULL) identifies the forward; rsv_backward_device fails with
+ * RSV_ERR_INVALID_ARGUMENT if another call has run on the backend since.
+ * No reference counterpart.
+ */
+rsv_status rsv_forward_device(rsv_backend *backend, const double *d_params, size_t num_params,
+                              double *d_energy_out, unsigned long long *generation_out,
+                              void *stream);
+rsv_status rsv_backward_device(rsv_backend *backend, unsigned long long generation,
+                               double *d_gradient_out, void *stream);
+
+/*
+ * energy_and_grad with a per-stage timing breakdown (milliseconds, CUDA events).
+ * Replaces the profile=true path of RingIsingCudaBackend::energy_and_grad
+ * (reference cpp/ising_cuda_backend.cu:24-106, cpp/ising_cuda_bindings.cpp:39-55).
+ * stage_ms_out: host double[rsv_num_stages()].
+ */
+rsv_status rsv_profile_energy_and_grad(rsv_backend *backend, const double *params,
+                                       size_t num_params, int compute_gradient,
+                                       double *energy_out, double *gradient_out,
+                                       double *stage_ms_out);
+
+/*
+ * Time the forward sweep launched directly and as a captured CUDA graph.
+ * Replaces RingIsingCudaBackend::benchmark_structured_forward_graph
+ * (reference cpp/ising_cuda_backend.cu:444-541, cpp/ising_cuda_bindings.cpp:99-114).
+ */
+rsv_status rsv_benchmark_forward_graph(rsv_backend *backend, const double *params,
+                                       size_t num_params, size_t repeats, double *normal_ms_out,
+                                       double *graph_ms_out);
+
+/*
+ * Per-launch timing over a measured region (for roofline reporting).
+ * rsv_set_launch_timing(backend, 1) makes every following call record a CUDA
+ * event pair around each of its kernel launches, on the launch stream;
+ * rsv_launch_stats synchronises, and returns per kernel kind (0 tables,
+ * 1 forward pass, 2 energy, 3 backward pass, 4 finalize) the launch count,
+ * the summed duration in ms and the summed algorithmic DRAM bytes (the
+ * minimum traffic: every amplitude a launch must read or write, 16 B each),
+ * then clears the record.  Arrays have RSV_NUM_KINDS entries.
+ * No reference counterpart.
+ */
+#define RSV_NUM_KINDS 5
+rsv_status rsv_set_launch_timing(rsv_backend *backend, int enable);
+rsv_status rsv_launch_stats(rsv_backend *backend, int *counts, double *total_ms,
+                            double *total_bytes);
+
+/* Geometry of a backend: qubits, layers, parameter count and device bytes held. */
+rsv_status rsv_backend_info(rsv_backend *backend, int *num_qubits, int *num_layers,
+                            size_t *num_params, size_t *device_bytes);
+
+/*
+ * Host-only description of the pass schedule the engine would run for
+ * (num_qubits, num_layers), as text (one line per kernel launch).  Needs no
+ * GPU.  Writes at most buf_size bytes including the terminating NUL and
+ * returns the full length in *length_out.  No reference counterpart (it
+ * replaces the reading of build_structured_forward_rotation_chunks and
+ * run_structured_backward_sweep, reference
+ * cpp/ising_cuda_structured_adjoint_modes.inc:18-71, 272-307).
+ */
+rsv_status rsv_describe_plan(int num_qubits, int num_layers, char *buf, size_t buf_size,
+                             size_t *length_out);
+
+/*
+ * Host-only reference of the engine's ring-CNOT index maps (P and P^-1),
+ * for checking the closed forms without a GPU.  Replaces
+ * ring_cnot_layer_transformed_index (reference cpp/ising_cuda_kernels.cu:178-205).
+ */
+unsigned long long rsv_ring_map(unsigned long long index, int num_qubits, int inverse);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RSV_H */

@@ -1,0 +1,231 @@
+"""Numpy execution of the engine's pass plan (host-logic check, no GPU).
+
+``librsv.so`` describes the launch sequence it would run (``rsv_describe_plan``):
+every pass's tile directions, gated wires, load/store modes (natural, gather
+through P, scatter through P or P^-1, analytic product state), RZ-phase and
+phi-gradient flags and buffer ids.  This module executes that description
+with whole-state numpy operations, using the same algebra as the CUDA
+kernels (RZ folded into one phase per amplitude per layer, theta gradient
+Re(conj(lam1) psi0) - Re(conj(lam0) psi1) in the RZ-free frame, phi gradient
+tot - 2*B_w), and also enumerates every tile/thread/register index of each
+pass to check that a pass touches every amplitude exactly once.  Tests
+compare the result with the oracle.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import re
+
+import numpy as np
+
+from gpu_simulation_b200._lib import load_library
+
+
+def describe_plan(n: int, layers: int) -> str:
+    lib = load_library()
+    buf = ctypes.create_string_buffer(1 << 20)
+    ln = ctypes.c_size_t()
+    rc = lib.rsv_describe_plan(n, layers, buf, len(buf), ctypes.byref(ln))
+    if rc != 0:
+        raise ValueError(lib.rsv_last_error().decode())
+    return buf.value.decode()
+
+
+_STEP = re.compile(
+    r"(?P<dir>fwd|bwd) layer=(?P<layer>\d+)(?: pass=(?P<pass>\d+))? dirs=\[(?P<dirs>[^\]]*)\] "
+    r"gates=\[(?P<gates>[^\]]*)\] runs=\[(?P<runs>[^\]]*)\] tiles=(?P<tiles>\d+) "
+    r"psi:(?P<pl>[\w()]+)\((?P<pi>-?\d+)\)->(?P<ps>\w+)\((?P<po>-?\d+)\)"
+    r"(?: lam:(?P<ll>[\w()]+)\((?P<li>-?\d+)\)->(?P<ls>\w+)\((?P<lo>-?\d+)\))?"
+    r"(?P<flags>.*) grid=(?P<grid>\d+)"
+)
+
+
+def parse_plan(text: str) -> dict:
+    lines = text.strip().splitlines()
+    head = dict(kv.split("=") for kv in lines[0].split())
+    steps = []
+    energy = None
+    for ln in lines[1:]:
+        if ln.startswith("energy"):
+            kv = dict(x.split("=") for x in ln.split()[1:])
+            energy = (int(kv["chi"]), int(kv["mu"]))
+            continue
+        if ln.startswith("finalize"):
+            continue
+        m = _STEP.match(ln)
+        if not m:
+            raise ValueError(f"cannot parse plan line: {ln}")
+        dirs = []
+        for d in m["dirs"].split(","):
+            dirs.append(int(d, 16) if d.startswith("0x") else (1 << int(d)))
+        gates = [int(g) for g in m["gates"].split(",") if g]
+        runs = [tuple(int(x) for x in r.split(":")) for r in m["runs"].split(",") if r]
+        steps.append(dict(
+            bwd=m["dir"] == "bwd", layer=int(m["layer"]),
+            pass_index=int(m["pass"]) if m["pass"] else -1,
+            dirs=dirs, gates=gates, runs=runs, tiles=int(m["tiles"]),
+            psi_load=m["pl"], psi_in=int(m["pi"]), psi_store=m["ps"], psi_out=int(m["po"]),
+            lam_load=m["ll"], lam_in=int(m["li"]) if m["li"] else -1,
+            lam_store=m["ls"], lam_out=int(m["lo"]) if m["lo"] else -1,
+            phase=" phase" in m["flags"], phi=" phi" in m["flags"], grid=int(m["grid"]),
+        ))
+    return dict(n=int(head["n"]), L=int(head["L"]), phys=int(head["phys"]), steps=steps,
+                energy=energy)
+
+
+def ring_p(i: np.ndarray, n: int) -> np.ndarray:
+    mask = (1 << n) - 1
+    lo = i & mask
+    pre = lo.copy()
+    for s in (1, 2, 4, 8, 16):
+        pre ^= pre << s
+    pre &= mask
+    par = np.zeros_like(lo)
+    x = lo >> 1
+    while np.any(x):
+        par ^= x & 1
+        x >>= 1
+    return (i & ~mask) | (pre & ~1) | par
+
+
+def ring_pinv(j: np.ndarray, n: int) -> np.ndarray:
+    mask = (1 << n) - 1
+    lo = j & mask
+    t = (lo ^ (lo << 1)) & mask
+    t = np.where((lo >> (n - 1)) & 1, t ^ 3, t)
+    return (j & ~mask) | t
+
+
+def tile_indices(step: dict) -> np.ndarray:
+    """Physical index of every (tile, thread, register) of a pass, computed
+    the way the kernel does (deposit + XOR of tile directions)."""
+    tiles = np.arange(step["tiles"], dtype=np.int64)
+    base = np.zeros_like(tiles)
+    rem = tiles.copy()
+    for start, ln in step["runs"]:
+        base |= (rem & ((1 << ln) - 1)) << start
+        rem >>= ln
+    t = np.arange(4096, dtype=np.int64)
+    off = np.zeros_like(t)
+    for b, v in enumerate(step["dirs"]):
+        off ^= np.where((t >> b) & 1, v, 0)
+    return (base[:, None] ^ off[None, :]).reshape(-1)
+
+
+def simulate(n: int, layers: int, field: float, params: np.ndarray, check_indices: bool = True):
+    """Run the plan with numpy.  Returns (energy, gradient flat f64[2nL])."""
+    plan = parse_plan(describe_plan(n, layers))
+    phys = plan["phys"]
+    size = 1 << phys
+    p = np.asarray(params, dtype=np.float64).reshape(layers, n, 2)
+    c, s = np.cos(p[..., 0] * 0.5), np.sin(p[..., 0] * 0.5)
+    ch, sh = np.cos(p[..., 1] * 0.5), np.sin(p[..., 1] * 0.5)
+    idx = np.arange(size, dtype=np.int64)
+    bits = (idx[:, None] >> np.arange(phys)[None, :]) & 1
+
+    def phase(layer):
+        ph = np.ones(size, dtype=np.complex128)
+        for w in range(n):
+            ph *= np.where(bits[:, w] == 1, ch[layer, w] + 1j * sh[layer, w], ch[layer, w] - 1j * sh[layer, w])
+        return ph
+
+    def product(j):
+        amp = np.ones(j.shape, dtype=np.complex128)
+        for w in range(phys):
+            b = (j >> w) & 1
+            if w < n:
+                f0 = c[0, w] * (ch[0, w] - 1j * sh[0, w])
+                f1 = s[0, w] * (ch[0, w] + 1j * sh[0, w])
+                amp *= np.where(b == 1, f1, f0)
+            else:
+                amp *= np.where(b == 1, 0.0, 1.0)
+        return amp
+
+    bufs = [np.zeros(size, dtype=np.complex128) for _ in range(3)]
+
+    def load(mode, bid):
+        if mode == "load":
+            return bufs[bid].copy()
+        if mode == "gatherP":
+            return bufs[bid][ring_p(idx, n)]
+        if mode == "product(P)":
+            return product(ring_pinv(idx, n))
+        if mode == "product":
+            return product(idx)
+        raise ValueError(mode)
+
+    def store(mode, bid, v):
+        if mode == "store":
+            bufs[bid][:] = v
+        elif mode == "scatterP":
+            out = np.empty_like(v)
+            out[ring_p(idx, n)] = v
+            bufs[bid][:] = out
+        elif mode == "scatterPinv":
+            out = np.empty_like(v)
+            out[ring_pinv(idx, n)] = v
+            bufs[bid][:] = out
+        elif mode != "none":
+            raise ValueError(mode)
+
+    theta = np.zeros((layers, n))
+    phi = np.zeros((layers, n))
+    energy = None
+    for st in plan["steps"]:
+        if check_indices:
+            ids = tile_indices(st)
+            if ids.size != size or not np.array_equal(np.sort(ids), idx):
+                raise AssertionError(f"pass does not cover the state exactly once: {st}")
+        layer = st["layer"]
+        if not st["bwd"]:
+            a = load(st["psi_load"], st["psi_in"])
+            for w in st["gates"]:
+                m = 1 << w
+                lo = idx[(idx & m) == 0]
+                a0, a1 = a[lo].copy(), a[lo | m].copy()
+                a[lo] = c[layer, w] * a0 - s[layer, w] * a1
+                a[lo | m] = s[layer, w] * a0 + c[layer, w] * a1
+            if st["phase"]:
+                a = a * phase(layer)
+            store(st["psi_store"], st["psi_out"], a)
+            continue
+        if energy is None:
+            chi_b, mu_b = plan["energy"]
+            chi = bufs[chi_b]
+            mu = np.zeros(size, dtype=np.complex128)
+            real = idx < (1 << n)
+            pi = ring_p(idx, n) & ((1 << n) - 1)
+            rot = ((pi << 1) & ((1 << n) - 1)) | (pi >> (n - 1))
+            walls = np.zeros(size, dtype=np.int64)
+            x = pi ^ rot
+            for w in range(n):
+                walls += (x >> w) & 1
+            mu = (2.0 * walls - n) * chi
+            for w in range(n):
+                mu = mu - field * chi[idx ^ int(ring_pinv(np.array([1 << w]), n)[0])]
+            mu = np.where(real, mu, 0.0)
+            energy = float(np.sum((np.conj(chi) * mu).real))
+            bufs[mu_b][:] = mu
+        a = load(st["psi_load"], st["psi_in"])
+        b = load(st["lam_load"], st["lam_in"])
+        if st["phase"]:
+            ph = np.conj(phase(layer))
+            a, b = a * ph, b * ph
+        if st["phi"]:
+            q = (np.conj(b) * a).imag
+            tot = q.sum()
+            for w in range(n):
+                phi[layer, w] = tot - 2.0 * q[bits[:, w] == 1].sum()
+        for w in st["gates"]:
+            m = 1 << w
+            lo = idx[(idx & m) == 0]
+            a0, a1, b0, b1 = a[lo].copy(), a[lo | m].copy(), b[lo].copy(), b[lo | m].copy()
+            theta[layer, w] = np.sum((np.conj(b1) * a0).real - (np.conj(b0) * a1).real)
+            cc, ss = c[layer, w], s[layer, w]
+            a[lo], a[lo | m] = cc * a0 + ss * a1, -ss * a0 + cc * a1
+            b[lo], b[lo | m] = cc * b0 + ss * b1, -ss * b0 + cc * b1
+        store(st["psi_store"], st["psi_out"], a)
+        store(st["lam_store"], st["lam_out"], b)
+    grad = np.stack([theta, phi], axis=-1).reshape(-1)
+    return energy, grad

@@ -1,0 +1,120 @@
+"""Host logic of the engine without a GPU: the C ABI library loads and exports
+every entry point of include/rsv.h, the pass plan executed in numpy equals
+the oracle, the ring maps equal the reference's closed form, and invalid
+arguments are rejected before any device call."""
+
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+from gpu_simulation_b200 import _lib, describe_plan
+from tests import plan_sim
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_functions() -> list[str]:
+    text = (ROOT / "include" / "rsv.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(rsv_[a-z_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load_library()
+    names = declared_functions()
+    assert len(names) >= 14
+    for name in names:
+        assert hasattr(lib, name), name
+        assert name in _lib._SIGNATURES, f"{name} has no ctypes signature"
+
+
+def test_dropin_module_exports_reference_api():
+    import standalone_backend._cuda_backend as m
+
+    assert hasattr(m, "RingIsingCudaBackend")
+    assert hasattr(m, "energy_and_grad")
+    cls = m.RingIsingCudaBackend
+    assert hasattr(cls, "energy_and_grad")
+    assert hasattr(cls, "benchmark_structured_forward_graph")
+
+
+def test_ring_map_matches_oracle_closed_form():
+    lib = _lib.load_library()
+    rng = np.random.default_rng(1)
+    for n in (2, 3, 5, 12, 20, 28, 31):
+        for i in rng.integers(0, 1 << n, 64):
+            i = int(i)
+            assert lib.rsv_ring_map(i, n, 0) == oracle.ring_perm(i, n)
+            assert lib.rsv_ring_map(i, n, 1) == oracle.ring_perm(i, n, inverse=True)
+
+
+@pytest.mark.parametrize("n,L,h", [
+    (2, 1, 0.7), (2, 3, 1.0), (3, 2, 1.1), (5, 4, 0.3), (8, 2, 1.0), (11, 2, 0.9),
+    (12, 3, 1.0), (13, 1, 1.2), (13, 3, 0.8), (14, 2, 1.0), (16, 2, 2.0), (17, 2, 0.5),
+])
+def test_plan_executed_in_numpy_matches_oracle(n, L, h):
+    rng = np.random.default_rng(100 + n * 10 + L)
+    p = rng.uniform(0, 2 * np.pi, 2 * n * L)
+    e_sim, g_sim = plan_sim.simulate(n, L, h, p)
+    e_ref, g_ref = oracle.energy_and_grad(n, L, h, p)
+    assert abs(e_sim - e_ref) < 1e-11
+    np.testing.assert_allclose(g_sim, g_ref, atol=1e-11, rtol=0)
+
+
+@pytest.mark.parametrize("n,L", [(20, 4), (24, 4), (28, 4), (30, 4), (31, 2)])
+def test_large_plans_cover_every_wire_once_with_three_buffers(n, L):
+    plan = plan_sim.parse_plan(describe_plan(n, L))
+    seen = {}
+    for st in plan["steps"]:
+        for b in ("psi_in", "psi_out", "lam_in", "lam_out"):
+            assert st[b] in (-1, 0, 1, 2)
+        if st["bwd"]:
+            for w in st["gates"]:
+                key = (st["layer"], w)
+                assert key not in seen
+                seen[key] = st["pass_index"]
+    assert len(seen) == n * L
+    # at most three backward passes per layer for these sizes
+    bwd = [s for s in plan["steps"] if s["bwd"]]
+    assert len(bwd) <= 3 * L
+
+
+def test_plan_rejects_bad_shapes():
+    with pytest.raises(ValueError):
+        describe_plan(1, 2)
+    with pytest.raises(ValueError):
+        describe_plan(32, 2)
+    with pytest.raises(ValueError):
+        describe_plan(8, 0)
+
+
+@pytest.mark.parametrize("kwargs,msg", [
+    (dict(num_qubits=1, num_layers=2, strategy="structured_adjoint", width=8), "num_qubits"),
+    (dict(num_qubits=4, num_layers=0, strategy="structured_adjoint", width=8), "num_layers"),
+    (dict(num_qubits=4, num_layers=2, strategy="checkpoint", width=8), "Unknown gradient strategy"),
+    (dict(num_qubits=4, num_layers=2, strategy="structured_adjoint", width=0), "at least 1"),
+    (dict(num_qubits=4, num_layers=2, strategy="structured_adjoint", width=9), "exceeds"),
+    (dict(num_qubits=9, num_layers=2, strategy="dense_scan", width=8), "dense_scan"),
+])
+def test_create_validates_arguments_before_touching_the_gpu(kwargs, msg):
+    lib = _lib.load_library()
+    h = ctypes.c_void_p()
+    rc = lib.rsv_create(kwargs["num_qubits"], kwargs["num_layers"], 1.0, kwargs["strategy"].encode(),
+                        kwargs["width"], 0, ctypes.byref(h))
+    assert rc == _lib.RSV_ERR_INVALID_ARGUMENT
+    assert msg in lib.rsv_last_error().decode()
+    assert not h.value
+
+
+def test_null_backend_calls_are_rejected():
+    lib = _lib.load_library()
+    e = ctypes.c_double()
+    rc = lib.rsv_energy_and_grad(None, None, 0, 1, ctypes.byref(e), None, None)
+    assert rc == _lib.RSV_ERR_INVALID_ARGUMENT
+    assert lib.rsv_destroy(None) == 0
