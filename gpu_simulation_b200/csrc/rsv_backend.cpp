@@ -465,6 +465,22 @@ void fill_pass_params(rsv_backend *B, const Step &s, PassParams &P) {
   P.phase = s.phase;
   P.phi_grad = s.phi_grad;
   P.sync_after_load = (s.tile.num_tiles == 1) ? 1 : 0;
+  // A direction with several physical bits that overlaps a gated wire flips
+  // that wire's bit; the planner's only such direction is tile bit 11 of the
+  // antipodal tile, which overlaps every gated wire.
+  P.flip_bit = kTileBits;
+  for (int b = 0; b < 12; ++b) {
+    const u64 v = s.tile.vec[b];
+    if ((v & (v - 1)) == 0) continue;
+    for (int g = 0; g < 12; ++g) {
+      const int w = s.tile.gate_wire[g];
+      if (w >= 0 && ((v >> w) & 1)) {
+        if (P.flip_bit != kTileBits && P.flip_bit != b)
+          throw Error(RSV_ERR_INTERNAL, "tile with two flipping directions");
+        P.flip_bit = b;
+      }
+    }
+  }
   P.psi_in = s.psi_in >= 0 ? B->buf[s.psi_in].p : nullptr;
   P.psi_out = s.psi_out >= 0 ? B->buf[s.psi_out].p : nullptr;
   P.lam_in = s.lam_in >= 0 ? B->buf[s.lam_in].p : nullptr;

@@ -131,34 +131,61 @@ __device__ __forceinline__ void store_amp(int mode, double2 *buf, u64 p, int n, 
   }
 }
 
+// One rotation step on a register pair (x0, x1) = (|0>, |1>) of one wire.
+template <bool BWD>
+__device__ __forceinline__ void rotate_pair(double c, double s, double2 &a0, double2 &a1, double2 &b0,
+                                            double2 &b1, double &acc) {
+  const double2 x0 = a0, x1 = a1;
+  if (!BWD) {
+    a0 = make_double2(fma(c, x0.x, -s * x1.x), fma(c, x0.y, -s * x1.y));
+    a1 = make_double2(fma(s, x0.x, c * x1.x), fma(s, x0.y, c * x1.y));
+  } else {
+    const double2 y0 = b0, y1 = b1;
+    // theta: Re(conj(lam1) psi0) - Re(conj(lam0) psi1), in the frame with the
+    // layer's RZ removed; equal to the reference's 2 Re<lam_mid|dRY|psi_before>
+    // (cpp/ising_cuda_statevector_grad_kernels.cu:289-307) after simplification.
+    acc += fma(y1.x, x0.x, y1.y * x0.y) - fma(y0.x, x1.x, y0.y * x1.y);
+    a0 = make_double2(fma(c, x0.x, s * x1.x), fma(c, x0.y, s * x1.y));
+    a1 = make_double2(fma(-s, x0.x, c * x1.x), fma(-s, x0.y, c * x1.y));
+    b0 = make_double2(fma(c, y0.x, s * y1.x), fma(c, y0.y, s * y1.y));
+    b1 = make_double2(fma(-s, y0.x, c * y1.x), fma(-s, y0.y, c * y1.y));
+  }
+}
+
 // Rotate the register pairs of the four tile bits TB0..TB0+3 (register bit j
-// is tile bit TB0 + j in the current layout).
-template <bool BWD, int TB0>
-__device__ __forceinline__ void apply_reg_gates(const PassParams &P, double2 (&a)[kRegs],
-                                                double2 (&b)[kRegs], double (&acc)[12]) {
+// is tile bit TB0 + j in layout LAYOUT).  When the tile has a direction with
+// more than one physical bit (P.flip_bit < 12, the all-ones direction of the
+// antipodal tile), that direction also flips the gated wire's bit: elements
+// whose flip coordinate is 1 hold the pair as (|1>, |0>), so the roles swap.
+template <bool BWD, int TB0, int LAYOUT>
+__device__ __forceinline__ void apply_reg_gates(const PassParams &P, int lane, int warp,
+                                                double2 (&a)[kRegs], double2 (&b)[kRegs],
+                                                double (&acc)[12]) {
+  const int thread_t = tile_index<LAYOUT>(lane, warp, 0);
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     const int w = P.gate_wire[TB0 + j];
     if (w < 0) continue;
     const double2 cs = __ldg(reinterpret_cast<const double2 *>(&P.coef[P.layer * P.n + w]));
     const double c = cs.x, s = cs.y;
+    if (P.flip_bit >= kTileBits) {
 #pragma unroll
-    for (int r = 0; r < kRegs; ++r) {
-      if (r & (1 << j)) continue;
-      const int r1 = r | (1 << j);
-      const double2 a0 = a[r], a1 = a[r1];
-      if (!BWD) {
-        a[r] = make_double2(fma(c, a0.x, -s * a1.x), fma(c, a0.y, -s * a1.y));
-        a[r1] = make_double2(fma(s, a0.x, c * a1.x), fma(s, a0.y, c * a1.y));
-      } else {
-        const double2 b0 = b[r], b1 = b[r1];
-        // theta: Re(conj(lam1) psi0) - Re(conj(lam0) psi1), in the frame with
-        // the layer's RZ removed (grad_kernels.cu:289-307 simplified).
-        acc[TB0 + j] += fma(b1.x, a0.x, b1.y * a0.y) - fma(b0.x, a1.x, b0.y * a1.y);
-        a[r] = make_double2(fma(c, a0.x, s * a1.x), fma(c, a0.y, s * a1.y));
-        a[r1] = make_double2(fma(-s, a0.x, c * a1.x), fma(-s, a0.y, c * a1.y));
-        b[r] = make_double2(fma(c, b0.x, s * b1.x), fma(c, b0.y, s * b1.y));
-        b[r1] = make_double2(fma(-s, b0.x, c * b1.x), fma(-s, b0.y, c * b1.y));
+      for (int r = 0; r < kRegs; ++r) {
+        if (r & (1 << j)) continue;
+        const int r1 = r | (1 << j);
+        rotate_pair<BWD>(c, s, a[r], a[r1], b[r], b[r1], acc[TB0 + j]);
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < kRegs; ++r) {
+        if (r & (1 << j)) continue;
+        const int r1 = r | (1 << j);
+        const bool flip = ((thread_t | tile_index<LAYOUT>(0, 0, r)) >> P.flip_bit) & 1;
+        if (flip) {
+          rotate_pair<BWD>(c, s, a[r1], a[r], b[r1], b[r], acc[TB0 + j]);
+        } else {
+          rotate_pair<BWD>(c, s, a[r], a[r1], b[r], b[r1], acc[TB0 + j]);
+        }
       }
     }
   }
@@ -290,13 +317,13 @@ __global__ void __launch_bounds__(kThreads, BWD ? 1 : 2) pass_kernel(const PassP
       __syncthreads();
     }
 
-    apply_reg_gates<BWD, 8>(P, a, b, acc);
+    apply_reg_gates<BWD, 8, 0>(P, lane, warp, a, b, acc);
     if (P.need_l1) {
       transpose<BWD, 0, 1>(sm, lane, warp, a, b);
-      apply_reg_gates<BWD, 4>(P, a, b, acc);
+      apply_reg_gates<BWD, 4, 1>(P, lane, warp, a, b, acc);
       if (P.need_l2) {
         transpose<BWD, 1, 2>(sm, lane, warp, a, b);
-        apply_reg_gates<BWD, 0>(P, a, b, acc);
+        apply_reg_gates<BWD, 0, 2>(P, lane, warp, a, b, acc);
         transpose<BWD, 2, 0>(sm, lane, warp, a, b);
       } else {
         transpose<BWD, 1, 0>(sm, lane, warp, a, b);

@@ -47,6 +47,7 @@ struct PassParams {
   int phase;                   // fwd: apply D after gates; bwd: apply D^dagger before gates
   int phi_grad;                // bwd: accumulate the phi-gradient sums of the layer
   int sync_after_load;         // single-tile in-place permutation: all loads before any store
+  int flip_bit;                // tile bit whose direction also flips gated wires (12 = none)
   const double2 *psi_in;
   double2 *psi_out;
   const double2 *lam_in;

@@ -113,6 +113,28 @@ def tile_indices(step: dict) -> np.ndarray:
     return (base[:, None] ^ off[None, :]).reshape(-1)
 
 
+def check_pair_roles(step: dict, n: int) -> None:
+    """The kernel rotates register pairs along tile bit b as (|0>, |1>) of the
+    gated wire w, swapping the roles where the tile's multi-bit direction
+    (flip bit) has coordinate 1.  Check that rule against the physical bit w
+    of every element of every tile."""
+    dirs = step["dirs"]
+    flip = 12
+    for b, v in enumerate(dirs):
+        if v & (v - 1) and any((v >> w) & 1 for w in step["gates"]):
+            flip = b
+    ids = tile_indices(step).reshape(step["tiles"], 4096)
+    t = np.arange(4096, dtype=np.int64)
+    flip_coord = (t >> flip) & 1 if flip < 12 else np.zeros_like(t)
+    for w in step["gates"]:
+        b = [i for i, v in enumerate(dirs) if v == (1 << w)]
+        assert len(b) == 1, "a gated wire needs its unit direction in the tile"
+        expected = ((t >> b[0]) & 1) ^ flip_coord
+        actual = (ids >> w) & 1
+        if not np.array_equal(actual, np.broadcast_to(expected, actual.shape)):
+            raise AssertionError(f"pair roles of wire {w} disagree with the kernel rule: {step}")
+
+
 def simulate(n: int, layers: int, field: float, params: np.ndarray, check_indices: bool = True):
     """Run the plan with numpy.  Returns (energy, gradient flat f64[2nL])."""
     plan = parse_plan(describe_plan(n, layers))
@@ -177,6 +199,7 @@ def simulate(n: int, layers: int, field: float, params: np.ndarray, check_indice
             ids = tile_indices(st)
             if ids.size != size or not np.array_equal(np.sort(ids), idx):
                 raise AssertionError(f"pass does not cover the state exactly once: {st}")
+            check_pair_roles(st, n)
         layer = st["layer"]
         if not st["bwd"]:
             a = load(st["psi_load"], st["psi_in"])
