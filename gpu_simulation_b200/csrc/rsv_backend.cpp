@@ -604,9 +604,14 @@ void run_all(rsv_backend *B, bool grad, double *energy_out, double *grad_out, cu
   run_finalize(B, grad, energy_out, grad_out, st);
 }
 
+// Synchronous host entry points: NULL selects the backend's own stream.
 cudaStream_t pick_stream(rsv_backend *B, void *stream) {
   return stream ? static_cast<cudaStream_t>(stream) : B->stream;
 }
+
+// Asynchronous device entry points: the stream is used as given, so 0 is the
+// legacy default stream (the CUDA convention, and torch's default stream).
+cudaStream_t device_stream(void *stream) { return static_cast<cudaStream_t>(stream); }
 
 void validate_params(rsv_backend *B, const void *params, size_t num_params) {
   if (B == nullptr) invalid("backend is null");
@@ -776,7 +781,7 @@ rsv_status rsv_energy_and_grad_device(rsv_backend *B, const double *d_params, si
   return guarded([&] {
     validate_params(B, d_params, num_params);
     if (d_energy_out == nullptr) invalid("d_energy_out is null");
-    cudaStream_t st = pick_stream(B, stream);
+    cudaStream_t st = device_stream(stream);
     timed(B, st, 0, 0.0, [&] {
       check(launch_coef(d_params, B->coef.p, static_cast<int>(B->n * B->L), st), "coef launch");
     });
@@ -790,7 +795,7 @@ rsv_status rsv_forward_device(rsv_backend *B, const double *d_params, size_t num
   return guarded([&] {
     validate_params(B, d_params, num_params);
     if (d_energy_out == nullptr) invalid("d_energy_out is null");
-    cudaStream_t st = pick_stream(B, stream);
+    cudaStream_t st = device_stream(stream);
     check(launch_coef(d_params, B->coef.p, static_cast<int>(B->n * B->L), st), "coef launch");
     run_all(B, false, d_energy_out, nullptr, st);
     B->forward_only_state = true;
@@ -805,7 +810,7 @@ rsv_status rsv_backward_device(rsv_backend *B, unsigned long long generation,
     if (d_gradient_out == nullptr) invalid("d_gradient_out is null");
     if (!B->forward_only_state || generation != B->generation)
       invalid("backward needs the state of the matching forward; the backend ran another call since");
-    cudaStream_t st = pick_stream(B, stream);
+    cudaStream_t st = device_stream(stream);
     run_backward(B, st);
     // energy is rewritten with the same value into the outputs scratch slot
     run_finalize(B, true, B->outputs.p, d_gradient_out, st);

@@ -88,6 +88,8 @@ rsv_status rsv_energy_and_grad(rsv_backend *backend, const double *params, size_
 /*
  * Same computation with DEVICE pointers, asynchronous on `stream` (no host
  * synchronisation, no host copies).  Used by the torch.autograd path.
+ * `stream` is used as given: 0 is the legacy default stream (for all device
+ * entry points below as well).
  * d_params: device f64[num_params]; d_energy_out: device f64[1];
  * d_gradient_out: device f64[num_params] or NULL for energy only.
  * No reference counterpart (the reference always round-trips through the host).
