@@ -27,7 +27,7 @@ CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 NVCC = str(CUDA_HOME / "bin" / "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["rsv_kernels.cu"]
+CU_SOURCES = ["rsv_kernels.cu", "rsv_pass.cu"]
 CPP_SOURCES = ["rsv_backend.cpp"]
 HEADERS = ["rsv_device.cuh", "rsv_types.h", "rsv_launch.h"]
 

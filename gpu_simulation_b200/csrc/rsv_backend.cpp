@@ -458,6 +458,31 @@ void fill_pass_params(rsv_backend *B, const Step &s, PassParams &P) {
   }
   P.need_l1 = l1 ? 1 : 0;
   P.need_l2 = l2 ? 1 : 0;
+  // Register layouts: 0 holds tile bits 8..11 in registers, 1 holds 4..7,
+  // 2 holds 0..3.  Forward passes load and store in layout 0; backward passes
+  // start in any layout (they read from the shared-memory staging area) and
+  // store from layout 0.
+  bool hi = false, mid = false, lo = false;
+  for (int b = 0; b < 12; ++b) {
+    if (s.tile.gate_wire[b] < 0) continue;
+    (b >= 8 ? hi : (b >= 4 ? mid : lo)) = true;
+  }
+  P.nseq = 0;
+  auto visit = [&](int layout, bool apply) {
+    P.seq_layout[P.nseq] = layout;
+    P.seq_apply[P.nseq] = apply ? 1 : 0;
+    ++P.nseq;
+  };
+  if (!s.bwd) {
+    visit(0, hi);
+    if (mid) visit(1, true);
+    if (lo) visit(2, true);
+    if (P.nseq > 1) visit(0, false);
+  } else {
+    if (mid) visit(1, true);
+    if (lo) visit(2, true);
+    visit(0, hi);
+  }
   P.psi_load = s.psi_load;
   P.lam_load = s.lam_load;
   P.psi_store = s.psi_store;

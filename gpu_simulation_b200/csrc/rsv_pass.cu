@@ -1,0 +1,482 @@
+// Tile-pass kernels of the ring-Ising structured adjoint (sm_100a).
+//
+// Replaces the reference's per-chunk rotation kernels
+// (zzEncounter/GPU_Simulation cpp/ising_cuda_rotation_kernels.cu:95-552 forward,
+// cpp/ising_cuda_statevector_grad_kernels.cu:223-1437 backward) and its ring-CNOT
+// kernels (cpp/ising_cuda_kernels.cu:207-236):
+//
+//   * a pass streams the state once, tile by tile; a tile is a coset of a
+//     12-dimensional GF(2) subspace of indices (4096 amplitudes) held in
+//     registers, 16 per thread of a 256-thread CTA;
+//   * the wires whose directions lie in the tile are rotated in registers;
+//     shared-memory transposes move the other tile directions into registers
+//     ("layouts" 0, 1, 2 below), so one pass covers up to 12 wires;
+//   * the CNOT ring is folded into a pass's load (gather through P) or store
+//     (scatter through P or P^-1); the layer's RZ gates are one diagonal phase
+//     per amplitude from four 256-entry byte tables;
+//   * backward passes stream psi and lambda: the next tile is prefetched into
+//     shared memory with cp.async while the current tile is processed, and the
+//     theta/phi gradient sums are accumulated on chip and written as one
+//     deterministic record per CTA (no FP64 atomics).
+//
+// The load/store variants are template parameters, so every instantiation
+// carries only the code of its own variant; the register gate code exists
+// once and is visited once per layout.
+#include "rsv_device.cuh"
+#include "rsv_types.h"
+
+namespace rsv {
+namespace {
+
+using u32 = unsigned int;
+
+// Thread layouts of a tile (tile index t has 12 bits):
+//   layout 0: lanes -> t bits 0..4, warps -> 5..7,  registers -> 8..11 (global load/store)
+//   layout 1: lanes -> t bits 8..11,0, warps -> 1..3, registers -> 4..7
+//   layout 2: lanes -> t bits 4..8, warps -> 9..11, registers -> 0..3
+__device__ __forceinline__ int thread_part(int layout, int lane, int warp) {
+  if (layout == 0) return lane | (warp << 5);
+  if (layout == 1) return (lane >> 4) | (warp << 1) | ((lane & 15) << 8);
+  return (lane << 4) | (warp << 9);
+}
+__device__ __forceinline__ int reg_shift(int layout) { return layout == 0 ? 8 : (layout == 1 ? 4 : 0); }
+
+// Tile bit held by lane bit j / warp bit j of a layout.
+__device__ __forceinline__ int lane_tile_bit(int layout, int j) {
+  if (layout == 0) return j;
+  if (layout == 1) return j < 4 ? 8 + j : 0;
+  return 4 + j;
+}
+__device__ __forceinline__ int warp_tile_bit(int layout, int j) {
+  if (layout == 0) return 5 + j;
+  if (layout == 1) return 1 + j;
+  return 9 + j;
+}
+
+// XOR-fold swizzle: the 8 lanes of a quarter warp hit distinct 16-byte bank
+// groups for every layout (their tile bits are 3 consecutive bits).
+__device__ __forceinline__ int swz(int t) { return t ^ (((t >> 3) ^ (t >> 6) ^ (t >> 9)) & 7); }
+
+__device__ __forceinline__ u32 deposit(const PassParams &P, u32 tile) {
+  u32 base = 0;
+#pragma unroll
+  for (int r = 0; r < kMaxRuns; ++r) {
+    if (r < P.num_runs) {
+      const int len = P.run_len[r];
+      base |= (tile & ((1u << len) - 1u)) << P.run_start[r];
+      tile >>= len;
+    }
+  }
+  return base;
+}
+
+// Physical offset of the thread part of a layout.
+__device__ __forceinline__ u32 thread_offset(const PassParams &P, int tp) {
+  u32 o = 0;
+#pragma unroll
+  for (int b = 0; b < 12; ++b)
+    if ((tp >> b) & 1) o ^= static_cast<u32>(P.vec[b]);
+  return o;
+}
+
+// Physical offset of register r in a layout whose register directions are v0..v3.
+__device__ __forceinline__ u32 reg_offset(int r, u32 v0, u32 v1, u32 v2, u32 v3) {
+  return ((r & 1) ? v0 : 0u) ^ ((r & 2) ? v1 : 0u) ^ ((r & 4) ? v2 : 0u) ^ ((r & 8) ? v3 : 0u);
+}
+
+__device__ __forceinline__ double2 table4(const double2 *__restrict__ t, u32 p) {
+  double2 v = __ldg(&t[p & 255]);
+  v = cmul(v, __ldg(&t[256 + ((p >> 8) & 255)]));
+  v = cmul(v, __ldg(&t[512 + ((p >> 16) & 255)]));
+  v = cmul(v, __ldg(&t[768 + (p >> 24)]));
+  return v;
+}
+
+template <int SRC>
+__device__ __forceinline__ u32 source_index(u32 p, int n) {
+  if (SRC == kLoadGatherP) return static_cast<u32>(ring_p(p, n));
+  return p;
+}
+
+template <int DST>
+__device__ __forceinline__ void store_amp(double2 *buf, u32 p, int n, double2 v) {
+  if (DST == kStoreNatural) __stcs(&buf[p], v);
+  if (DST == kStoreScatterP) __stcs(&buf[static_cast<u32>(ring_p(p, n))], v);
+  if (DST == kStoreScatterPinv) __stcs(&buf[static_cast<u32>(ring_pinv(p, n))], v);
+}
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const u32 s = static_cast<u32>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Rotate the register pairs of the four register bits of `layout`.  Pair
+// (r, r | 2^j) holds (|0>, |1>) of wire gate_wire[rb + j] -- or (|1>, |0>) where
+// the tile's flip coordinate is 1 (antipodal tile), which is the same update
+// with s -> -s and the theta contribution negated.
+template <bool BWD>
+__device__ __forceinline__ void apply_gates(const PassParams &P, int layout, int tp,
+                                            double2 (&a)[kRegs], double2 (&b)[kRegs],
+                                            double (&acc)[4]) {
+  const int rb = reg_shift(layout);
+  const int fb = P.flip_bit;
+  const bool thread_flip = fb < kTileBits && ((tp >> fb) & 1);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    acc[j] = 0.0;
+    const int w = P.gate_wire[rb + j];
+    if (w < 0) continue;
+    const double2 cs = __ldg(reinterpret_cast<const double2 *>(&P.coef[P.layer * P.n + w]));
+    const double c = cs.x;
+#pragma unroll
+    for (int r = 0; r < kRegs; ++r) {
+      if (r & (1 << j)) continue;
+      const int r1 = r | (1 << j);
+      // flip coordinate of this register pair (equal for r and r1: the flip
+      // direction is never gated)
+      const bool reg_flip = fb < kTileBits && (((r << rb) >> fb) & 1);
+      const double sg = (thread_flip != reg_flip) ? -1.0 : 1.0;
+      const double s = sg * cs.y;
+      const double2 x0 = a[r], x1 = a[r1];
+      if (!BWD) {
+        a[r] = make_double2(fma(c, x0.x, -s * x1.x), fma(c, x0.y, -s * x1.y));
+        a[r1] = make_double2(fma(s, x0.x, c * x1.x), fma(s, x0.y, c * x1.y));
+      } else {
+        const double2 y0 = b[r], y1 = b[r1];
+        // theta: Re(conj(lam1) psi0) - Re(conj(lam0) psi1) in the frame with the
+        // layer's RZ removed: the reference's 2 Re<lam_mid|dRY|psi_before>
+        // (cpp/ising_cuda_statevector_grad_kernels.cu:289-307) simplified.
+        acc[j] += sg * (fma(y1.x, x0.x, y1.y * x0.y) - fma(y0.x, x1.x, y0.y * x1.y));
+        a[r] = make_double2(fma(c, x0.x, s * x1.x), fma(c, x0.y, s * x1.y));
+        a[r1] = make_double2(fma(-s, x0.x, c * x1.x), fma(-s, x0.y, c * x1.y));
+        b[r] = make_double2(fma(c, y0.x, s * y1.x), fma(c, y0.y, s * y1.y));
+        b[r1] = make_double2(fma(-s, y0.x, c * y1.x), fma(-s, y0.y, c * y1.y));
+      }
+    }
+  }
+}
+
+// Register values of layout `from` -> layout `to` through shared memory.
+__device__ __forceinline__ void transpose(double2 *sm, int tp_from, int rb_from, int tp_to, int rb_to,
+                                          double2 (&a)[kRegs]) {
+#pragma unroll
+  for (int r = 0; r < kRegs; ++r) sm[swz(tp_from | (r << rb_from))] = a[r];
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kRegs; ++r) a[r] = sm[swz(tp_to | (r << rb_to))];
+  __syncthreads();
+}
+
+// Backward-only: phi-gradient sums of one tile (q = Im(conj(lam) psi) per
+// amplitude), folded into per-CTA accumulators phi_sm[w] (sum of q over
+// amplitudes with bit w set) and phi_sm[32] (sum of q).
+__device__ __forceinline__ void accumulate_phi(const PassParams &P, int layout, u32 base, int lane,
+                                               int warp, const double2 (&a)[kRegs],
+                                               const double2 (&b)[kRegs], double (*red)[12],
+                                               double *phi_sm) {
+  double q_tot = 0.0, q_reg[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int r = 0; r < kRegs; ++r) {
+    const double q = fma(b[r].x, a[r].y, -b[r].y * a[r].x);
+    q_tot += q;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if ((r >> j) & 1) q_reg[j] += q;
+  }
+  double v[10];
+  v[0] = q_tot;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) v[1 + j] = q_reg[j];
+#pragma unroll
+  for (int j = 0; j < 5; ++j) v[5 + j] = ((lane >> j) & 1) ? q_tot : 0.0;
+#pragma unroll
+  for (int j = 0; j < 10; ++j) v[j] = warp_sum(v[j]);
+  if (lane == 0) {
+#pragma unroll
+    for (int j = 0; j < 10; ++j) red[warp][j] = v[j];
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int w = threadIdx.x;
+    double qt = 0.0;
+#pragma unroll
+    for (int ww = 0; ww < 8; ++ww) qt += red[ww][0];
+    if (w < P.n) {
+      const int tb = P.wire_tile_bit[w];
+      const int rb = reg_shift(layout);
+      double add = 0.0;
+      if (tb < 0) {
+        if ((base >> w) & 1) add = qt;  // coset bit: set for the whole tile
+      } else if (tb >= rb && tb < rb + 4) {
+        for (int ww = 0; ww < 8; ++ww) add += red[ww][1 + tb - rb];
+      } else {
+        bool done = false;
+        for (int j = 0; j < 5 && !done; ++j)
+          if (lane_tile_bit(layout, j) == tb) {
+            for (int ww = 0; ww < 8; ++ww) add += red[ww][5 + j];
+            done = true;
+          }
+        for (int j = 0; j < 3 && !done; ++j)
+          if (warp_tile_bit(layout, j) == tb) {
+            for (int ww = 0; ww < 8; ++ww)
+              if ((ww >> j) & 1) add += red[ww][0];
+            done = true;
+          }
+      }
+      phi_sm[w] += add;
+    }
+    if (w == 31) phi_sm[32] += qt;
+  }
+  __syncthreads();
+}
+
+// Shared memory of the backward kernel (dynamic): staging psi | staging lam |
+// transpose buffer | theta accumulators [12][256].
+constexpr size_t kBwdStage = 2 * kTileSize * sizeof(double2);
+constexpr size_t kBwdTrans = kTileSize * sizeof(double2);
+constexpr size_t kBwdTheta = 12 * kThreads * sizeof(double);
+constexpr size_t kBwdSmem = kBwdStage + kBwdTrans + kBwdTheta;
+constexpr size_t kFwdSmem = kTileSize * sizeof(double2);
+
+// ---------------------------------------------------------------- backward
+template <int LSRC, int PDST, int LDST, bool PHASE>
+__global__ void __launch_bounds__(kThreads, 1) bwd_pass_kernel(const PassParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2 *stage_a = reinterpret_cast<double2 *>(smem_raw);
+  double2 *stage_b = stage_a + kTileSize;
+  double2 *trans = stage_b + kTileSize;
+  double *theta_sm = reinterpret_cast<double *>(trans + kTileSize);
+  __shared__ double red[8][12];
+  __shared__ double phi_sm[33];
+
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int n = P.n;
+  const int first_layout = P.seq_layout[0];
+
+  const int tp0 = thread_part(0, lane, warp);
+  const u32 toff0 = thread_offset(P, tp0);
+  const u32 v8 = P.vec[8], v9 = P.vec[9], v10 = P.vec[10], v11 = P.vec[11];
+  const int tpf = thread_part(first_layout, lane, warp);
+  const u32 tofff = thread_offset(P, tpf);
+  const int rbf = reg_shift(first_layout);
+  const u32 f0 = P.vec[rbf], f1 = P.vec[rbf + 1], f2 = P.vec[rbf + 2], f3 = P.vec[rbf + 3];
+
+#pragma unroll
+  for (int b = 0; b < 12; ++b) theta_sm[b * kThreads + threadIdx.x] = 0.0;
+  if (PHASE && threadIdx.x < 33) phi_sm[threadIdx.x] = 0.0;
+
+  const u32 num_tiles = static_cast<u32>(P.num_tiles);
+  auto issue = [&](u32 tile) {
+    const u32 base = deposit(P, tile) ^ toff0;
+#pragma unroll
+    for (int r = 0; r < kRegs; ++r) {
+      const u32 p = base ^ reg_offset(r, v8, v9, v10, v11);
+      const int s = swz(tp0 | (r << 8));
+      cp_async16(&stage_a[s], &P.psi_in[p]);
+      cp_async16(&stage_b[s], &P.lam_in[source_index<LSRC>(p, n)]);
+    }
+    cp_async_commit();
+  };
+  if (blockIdx.x < num_tiles) issue(blockIdx.x);
+
+  for (u32 tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
+    cp_async_wait_all();
+    __syncthreads();
+    double2 a[kRegs], b[kRegs];
+#pragma unroll
+    for (int r = 0; r < kRegs; ++r) {
+      const int s = swz(tpf | (r << rbf));
+      a[r] = stage_a[s];
+      b[r] = stage_b[s];
+    }
+    __syncthreads();
+    if (tile + gridDim.x < num_tiles) issue(tile + gridDim.x);
+
+    const u32 cbase = deposit(P, tile);
+    if (PHASE) {
+      const u32 base = cbase ^ tofff;
+#pragma unroll
+      for (int r = 0; r < kRegs; ++r) {
+        const double2 ph = table4(P.ptab, base ^ reg_offset(r, f0, f1, f2, f3));
+        a[r] = cmul_conj(a[r], ph);
+        b[r] = cmul_conj(b[r], ph);
+      }
+      accumulate_phi(P, first_layout, cbase, lane, warp, a, b, red, phi_sm);
+    }
+
+    int prev = first_layout;
+    for (int k = 0; k < P.nseq; ++k) {
+      const int layout = P.seq_layout[k];
+      const int tp = thread_part(layout, lane, warp);
+      if (k > 0) {
+        const int tpp = thread_part(prev, lane, warp);
+        transpose(trans, tpp, reg_shift(prev), tp, reg_shift(layout), a);
+        transpose(trans, tpp, reg_shift(prev), tp, reg_shift(layout), b);
+      }
+      if (P.seq_apply[k]) {
+        double acc[4];
+        apply_gates<true>(P, layout, tp, a, b, acc);
+        const int rb = reg_shift(layout);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) theta_sm[(rb + j) * kThreads + threadIdx.x] += acc[j];
+      }
+      prev = layout;
+    }
+
+    // stores from layout 0
+    if (PDST != kStoreNone || LDST != kStoreNone) {
+      const u32 base = cbase ^ toff0;
+#pragma unroll
+      for (int r = 0; r < kRegs; ++r) {
+        const u32 p = base ^ reg_offset(r, v8, v9, v10, v11);
+        store_amp<PDST>(P.psi_out, p, n, a[r]);
+        store_amp<LDST>(P.lam_out, p, n, b[r]);
+      }
+    }
+  }
+
+  // CTA reduction of the theta sums, then one record per CTA.
+  __syncthreads();
+  double *rec = P.partials + static_cast<size_t>(blockIdx.x) * kPartialStride;
+  {
+    // 12 tile bits x 256 threads: warp w reduces tile bits w and w + 8 (< 12)
+    for (int tb = warp; tb < 12; tb += 8) {
+      double s = 0.0;
+      for (int t = lane; t < kThreads; t += 32) s += theta_sm[tb * kThreads + t];
+      s = warp_sum(s);
+      if (lane == 0) rec[tb] = s;
+    }
+  }
+  if (PHASE) {
+    if (threadIdx.x < 31) rec[kPartialPhi + threadIdx.x] = phi_sm[threadIdx.x];
+    if (threadIdx.x == 31) rec[kPartialTot] = phi_sm[32];
+  }
+}
+
+// ----------------------------------------------------------------- forward
+template <int PSRC, int PDST, bool PHASE>
+__global__ void __launch_bounds__(kThreads, 2) fwd_pass_kernel(const PassParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2 *trans = reinterpret_cast<double2 *>(smem_raw);
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int n = P.n;
+  const int tp0 = thread_part(0, lane, warp);
+  const u32 toff0 = thread_offset(P, tp0);
+  const u32 v8 = P.vec[8], v9 = P.vec[9], v10 = P.vec[10], v11 = P.vec[11];
+  const u32 num_tiles = static_cast<u32>(P.num_tiles);
+  double acc[4];
+  double2 dummy[kRegs];
+
+  for (u32 tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
+    const u32 base = deposit(P, tile) ^ toff0;
+    double2 a[kRegs];
+#pragma unroll
+    for (int r = 0; r < kRegs; ++r) {
+      const u32 p = base ^ reg_offset(r, v8, v9, v10, v11);
+      if (PSRC == kLoadNatural) a[r] = __ldcs(&P.psi_in[p]);
+      if (PSRC == kLoadProduct) a[r] = table4(P.prod, static_cast<u32>(ring_pinv(p, n)));
+      if (PSRC == kLoadProductPlain) a[r] = table4(P.prod, p);
+    }
+    if (P.sync_after_load) __syncthreads();
+
+    int prev = 0;
+    for (int k = 0; k < P.nseq; ++k) {
+      const int layout = P.seq_layout[k];
+      const int tp = thread_part(layout, lane, warp);
+      if (k > 0) transpose(trans, thread_part(prev, lane, warp), reg_shift(prev), tp, reg_shift(layout), a);
+      if (P.seq_apply[k]) apply_gates<false>(P, layout, tp, a, dummy, acc);
+      prev = layout;
+    }
+
+    if (PHASE) {
+#pragma unroll
+      for (int r = 0; r < kRegs; ++r) a[r] = cmul(a[r], table4(P.ptab, base ^ reg_offset(r, v8, v9, v10, v11)));
+    }
+#pragma unroll
+    for (int r = 0; r < kRegs; ++r) store_amp<PDST>(P.psi_out, base ^ reg_offset(r, v8, v9, v10, v11), n, a[r]);
+  }
+}
+
+template <int LSRC, int PDST, int LDST, bool PHASE>
+cudaError_t launch_bwd(const PassParams &P, int grid, cudaStream_t s) {
+  auto k = bwd_pass_kernel<LSRC, PDST, LDST, PHASE>;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(kBwdSmem));
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  k<<<grid, kThreads, kBwdSmem, s>>>(P);
+  return cudaGetLastError();
+}
+
+template <int PSRC, int PDST, bool PHASE>
+cudaError_t launch_fwd(const PassParams &P, int grid, cudaStream_t s) {
+  auto k = fwd_pass_kernel<PSRC, PDST, PHASE>;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(kFwdSmem));
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  k<<<grid, kThreads, kFwdSmem, s>>>(P);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_pass(const PassParams &P, bool bwd, int grid, cudaStream_t s) {
+  if (bwd) {
+    if (P.psi_load != kLoadNatural) return cudaErrorInvalidValue;
+    const bool phase = P.phase != 0;
+    const bool gather = P.lam_load == kLoadGatherP;
+    if (P.lam_load != kLoadNatural && !gather) return cudaErrorInvalidValue;
+    if (P.phi_grad != P.phase) return cudaErrorInvalidValue;
+    const int ps = P.psi_store, ls = P.lam_store;
+    // (psi, lambda) stores used by the planner: (natural, natural),
+    // (scatter P^-1, natural), (none, none)
+    if (ps == kStoreNatural && ls == kStoreNatural) {
+      if (phase) return gather ? launch_bwd<kLoadGatherP, kStoreNatural, kStoreNatural, true>(P, grid, s)
+                               : launch_bwd<kLoadNatural, kStoreNatural, kStoreNatural, true>(P, grid, s);
+      if (!gather) return launch_bwd<kLoadNatural, kStoreNatural, kStoreNatural, false>(P, grid, s);
+    } else if (ps == kStoreScatterPinv && ls == kStoreNatural) {
+      if (phase) return gather ? launch_bwd<kLoadGatherP, kStoreScatterPinv, kStoreNatural, true>(P, grid, s)
+                               : launch_bwd<kLoadNatural, kStoreScatterPinv, kStoreNatural, true>(P, grid, s);
+      if (!gather) return launch_bwd<kLoadNatural, kStoreScatterPinv, kStoreNatural, false>(P, grid, s);
+    } else if (ps == kStoreNone && ls == kStoreNone) {
+      if (phase) return gather ? launch_bwd<kLoadGatherP, kStoreNone, kStoreNone, true>(P, grid, s)
+                               : launch_bwd<kLoadNatural, kStoreNone, kStoreNone, true>(P, grid, s);
+      if (!gather) return launch_bwd<kLoadNatural, kStoreNone, kStoreNone, false>(P, grid, s);
+    }
+    return cudaErrorInvalidValue;
+  }
+  const bool phase = P.phase != 0;
+  const int src = P.psi_load, dst = P.psi_store;
+  if (src == kLoadProductPlain && dst == kStoreNatural && !phase)
+    return launch_fwd<kLoadProductPlain, kStoreNatural, false>(P, grid, s);
+#define RSV_FWD(SRC)                                                                 \
+  if (src == SRC) {                                                                  \
+    if (dst == kStoreNatural)                                                        \
+      return phase ? launch_fwd<SRC, kStoreNatural, true>(P, grid, s)                \
+                   : launch_fwd<SRC, kStoreNatural, false>(P, grid, s);              \
+    if (dst == kStoreScatterP)                                                       \
+      return phase ? launch_fwd<SRC, kStoreScatterP, true>(P, grid, s)               \
+                   : launch_fwd<SRC, kStoreScatterP, false>(P, grid, s);             \
+  }
+  RSV_FWD(kLoadNatural)
+  RSV_FWD(kLoadProduct)
+#undef RSV_FWD
+  return cudaErrorInvalidValue;
+}
+
+size_t pass_smem_bytes(bool bwd) { return bwd ? kBwdSmem : kFwdSmem; }
+
+cudaError_t configure_pass_kernels() { return cudaSuccess; }
+
+}  // namespace rsv

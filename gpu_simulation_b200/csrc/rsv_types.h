@@ -48,6 +48,9 @@ struct PassParams {
   int phi_grad;                // bwd: accumulate the phi-gradient sums of the layer
   int sync_after_load;         // single-tile in-place permutation: all loads before any store
   int flip_bit;                // tile bit whose direction also flips gated wires (12 = none)
+  int nseq;                    // register layouts visited by the pass, in order
+  int seq_layout[4];           // layout id (0, 1, 2) of each visit; the last is 0
+  int seq_apply[4];            // whether the visit rotates its register tile bits
   const double2 *psi_in;
   double2 *psi_out;
   const double2 *lam_in;
