@@ -169,61 +169,168 @@ __device__ __forceinline__ void transpose(double2 *sm, int tp_from, int rb_from,
   __syncthreads();
 }
 
-// Backward-only: phi-gradient sums of one tile (q = Im(conj(lam) psi) per
-// amplitude), folded into per-CTA accumulators phi_sm[w] (sum of q over
-// amplitudes with bit w set) and phi_sm[32] (sum of q).
-__device__ __forceinline__ void accumulate_phi(const PassParams &P, int layout, u32 base, int lane,
-                                               int warp, const double2 (&a)[kRegs],
-                                               const double2 (&b)[kRegs], double (*red)[12],
-                                               double *phi_sm) {
-  double q_tot = 0.0, q_reg[4] = {0.0, 0.0, 0.0, 0.0};
+// e^{i phi_w} of wire w of a layer (from its cos/sin(phi/2)); 1 for w >= n.
+__device__ __forceinline__ double2 phase_ratio(const PassParams &P, int w) {
+  if (w < 0 || w >= P.n) return make_double2(1.0, 0.0);
+  const double4 k = P.coef[P.layer * P.n + w];
+  return make_double2(fma(k.z, k.z, -k.w * k.w), 2.0 * k.z * k.w);
+}
+
+__device__ __forceinline__ int unit_bit(unsigned long long v) { return v ? __ffsll(v) - 1 : -1; }
+
+// Multiply register r of `a` (and `b`) by its RZ-phase (or conjugate): the
+// phase of element base ^ (register directions of r) is phase(base) times
+// e^{i phi_w} for every register direction e_w set in r (unit directions).
+// Registers are visited in Gray-code order so that one running product is
+// enough.
+template <int NB, bool CONJ, bool TWO>
+__device__ __forceinline__ void apply_phase_gray(double2 ph, const double2 (&ratio)[4],
+                                                 double2 *a, double2 *b) {
+  constexpr int NR = 1 << NB;
 #pragma unroll
-  for (int r = 0; r < kRegs; ++r) {
-    const double q = fma(b[r].x, a[r].y, -b[r].y * a[r].x);
-    q_tot += q;
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-      if ((r >> j) & 1) q_reg[j] += q;
+  for (int k = 0; k < NR; ++k) {
+    const int g = k ^ (k >> 1);
+    if (k > 0) {
+      const int prev = (k - 1) ^ ((k - 1) >> 1);
+      const int flipped = g ^ prev;
+      const int j = flipped == 1 ? 0 : flipped == 2 ? 1 : flipped == 4 ? 2 : 3;
+      ph = (g & flipped) ? cmul(ph, ratio[j]) : cmul_conj(ph, ratio[j]);
+    }
+    if (CONJ) {
+      a[g] = cmul_conj(a[g], ph);
+      if (TWO) b[g] = cmul_conj(b[g], ph);
+    } else {
+      a[g] = cmul(a[g], ph);
+      if (TWO) b[g] = cmul(b[g], ph);
+    }
   }
-  double v[10];
-  v[0] = q_tot;
+}
+
+// ======================================================================
+// Backward pass: 512 threads x 8 amplitudes of psi and lambda each.
+// Register groups of three tile bits: G0 = bits 0..2, G1 = 3..5, G2 = 6..8,
+// G3 = 9..11.  Layout Lk holds group G(3-k) in registers:
+//   L0: lanes -> bits 0..4,        warps -> 5..8,         registers -> 9..11
+//   L1: lanes -> bits 9,10,11,0,1, warps -> 2..5,         registers -> 6..8
+//   L2: lanes -> bits 6..10,       warps -> 11,0,1,2,     registers -> 3..5
+//   L3: lanes -> bits 3..7,        warps -> 8..11,        registers -> 0..2
+// ======================================================================
+namespace bw {
+constexpr int kT = 512;
+constexpr int kR = 8;
+
+__device__ __forceinline__ int tpart(int L, int lane, int warp) {
+  if (L == 0) return lane | (warp << 5);
+  if (L == 1) return (lane >> 3) | (warp << 2) | ((lane & 7) << 9);
+  if (L == 2) return (warp >> 1) | (lane << 6) | ((warp & 1) << 11);
+  return (lane << 3) | (warp << 8);
+}
+__device__ __forceinline__ int rshift(int L) { return 9 - 3 * L; }
+__device__ __forceinline__ int lane_bit(int L, int j) {
+  if (L == 0) return j;
+  if (L == 1) return j < 3 ? 9 + j : j - 3;
+  if (L == 2) return 6 + j;
+  return 3 + j;
+}
+__device__ __forceinline__ int warp_bit(int L, int j) {
+  if (L == 0) return 5 + j;
+  if (L == 1) return 2 + j;
+  if (L == 2) return j == 0 ? 11 : j - 1;
+  return 8 + j;
+}
+
+__device__ __forceinline__ void transpose(double2 *sm, int tp_from, int rb_from, int tp_to, int rb_to,
+                                          double2 (&a)[kR]) {
 #pragma unroll
-  for (int j = 0; j < 4; ++j) v[1 + j] = q_reg[j];
+  for (int r = 0; r < kR; ++r) sm[swz(tp_from | (r << rb_from))] = a[r];
+  __syncthreads();
 #pragma unroll
-  for (int j = 0; j < 5; ++j) v[5 + j] = ((lane >> j) & 1) ? q_tot : 0.0;
+  for (int r = 0; r < kR; ++r) a[r] = sm[swz(tp_to | (r << rb_to))];
+  __syncthreads();
+}
+
+// Backward rotation of the three register bits of layout L (tile bits RB..RB+2).
+template <int L>
+__device__ __forceinline__ void gates(const PassParams &P, int tp, double2 (&a)[kR], double2 (&b)[kR],
+                                      double (&acc)[12]) {
+  constexpr int RB = 9 - 3 * L;
+  const int fb = P.flip_bit;
+  const bool thread_flip = fb < kTileBits && ((tp >> fb) & 1);
 #pragma unroll
-  for (int j = 0; j < 10; ++j) v[j] = warp_sum(v[j]);
+  for (int j = 0; j < 3; ++j) {
+    const int w = P.gate_wire[RB + j];
+    if (w < 0) continue;
+    const double2 cs = __ldg(reinterpret_cast<const double2 *>(&P.coef[P.layer * P.n + w]));
+    const double c = cs.x;
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+      if (r & (1 << j)) continue;
+      const int r1 = r | (1 << j);
+      const bool reg_flip = fb < kTileBits && (((r << RB) >> fb) & 1);
+      const double sg = (thread_flip != reg_flip) ? -1.0 : 1.0;
+      const double s = sg * cs.y;
+      const double2 x0 = a[r], x1 = a[r1], y0 = b[r], y1 = b[r1];
+      // theta: Re(conj(lam1) psi0) - Re(conj(lam0) psi1) in the frame with the
+      // layer's RZ removed: the reference's 2 Re<lam_mid|dRY|psi_before>
+      // (cpp/ising_cuda_statevector_grad_kernels.cu:289-307) simplified.
+      acc[RB + j] += sg * (fma(y1.x, x0.x, y1.y * x0.y) - fma(y0.x, x1.x, y0.y * x1.y));
+      a[r] = make_double2(fma(c, x0.x, s * x1.x), fma(c, x0.y, s * x1.y));
+      a[r1] = make_double2(fma(-s, x0.x, c * x1.x), fma(-s, x0.y, c * x1.y));
+      b[r] = make_double2(fma(c, y0.x, s * y1.x), fma(c, y0.y, s * y1.y));
+      b[r1] = make_double2(fma(-s, y0.x, c * y1.x), fma(-s, y0.y, c * y1.y));
+    }
+  }
+}
+
+// phi-gradient sums of one tile in layout L: q = Im(conj(lam) psi) per
+// amplitude, folded into phi_sm[w] (sum of q with bit w set) and phi_sm[32].
+__device__ __forceinline__ void phi_sums(const PassParams &P, int L, u32 cbase, int lane, int warp,
+                                         const double2 (&a)[kR], const double2 (&b)[kR],
+                                         double (*red)[12], double *phi_sm) {
+  double v[9];
+#pragma unroll
+  for (int j = 0; j < 9; ++j) v[j] = 0.0;
+#pragma unroll
+  for (int r = 0; r < kR; ++r) {
+    const double q = fma(b[r].x, a[r].y, -b[r].y * a[r].x);
+    v[0] += q;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      if ((r >> j) & 1) v[1 + j] += q;
+  }
+#pragma unroll
+  for (int j = 0; j < 5; ++j) v[4 + j] = ((lane >> j) & 1) ? v[0] : 0.0;
+#pragma unroll
+  for (int j = 0; j < 9; ++j) v[j] = warp_sum(v[j]);
   if (lane == 0) {
 #pragma unroll
-    for (int j = 0; j < 10; ++j) red[warp][j] = v[j];
+    for (int j = 0; j < 9; ++j) red[warp][j] = v[j];
   }
   __syncthreads();
   if (threadIdx.x < 32) {
     const int w = threadIdx.x;
     double qt = 0.0;
-#pragma unroll
-    for (int ww = 0; ww < 8; ++ww) qt += red[ww][0];
+    for (int ww = 0; ww < 16; ++ww) qt += red[ww][0];
     if (w < P.n) {
       const int tb = P.wire_tile_bit[w];
-      const int rb = reg_shift(layout);
+      const int rb = rshift(L);
       double add = 0.0;
       if (tb < 0) {
-        if ((base >> w) & 1) add = qt;  // coset bit: set for the whole tile
-      } else if (tb >= rb && tb < rb + 4) {
-        for (int ww = 0; ww < 8; ++ww) add += red[ww][1 + tb - rb];
+        if ((cbase >> w) & 1) add = qt;  // coset bit: set for the whole tile
+      } else if (tb >= rb && tb < rb + 3) {
+        for (int ww = 0; ww < 16; ++ww) add += red[ww][1 + tb - rb];
       } else {
-        bool done = false;
-        for (int j = 0; j < 5 && !done; ++j)
-          if (lane_tile_bit(layout, j) == tb) {
-            for (int ww = 0; ww < 8; ++ww) add += red[ww][5 + j];
-            done = true;
-          }
-        for (int j = 0; j < 3 && !done; ++j)
-          if (warp_tile_bit(layout, j) == tb) {
-            for (int ww = 0; ww < 8; ++ww)
-              if ((ww >> j) & 1) add += red[ww][0];
-            done = true;
-          }
+        int lj = -1, wj = -1;
+        for (int j = 0; j < 5; ++j)
+          if (lane_bit(L, j) == tb) lj = j;
+        for (int j = 0; j < 4; ++j)
+          if (warp_bit(L, j) == tb) wj = j;
+        if (lj >= 0) {
+          for (int ww = 0; ww < 16; ++ww) add += red[ww][4 + lj];
+        } else if (wj >= 0) {
+          for (int ww = 0; ww < 16; ++ww)
+            if ((ww >> wj) & 1) add += red[ww][0];
+        }
       }
       phi_sm[w] += add;
     }
@@ -231,50 +338,61 @@ __device__ __forceinline__ void accumulate_phi(const PassParams &P, int layout, 
   }
   __syncthreads();
 }
+}  // namespace bw
 
 // Shared memory of the backward kernel (dynamic): staging psi | staging lam |
-// transpose buffer | theta accumulators [12][256].
-constexpr size_t kBwdStage = 2 * kTileSize * sizeof(double2);
-constexpr size_t kBwdTrans = kTileSize * sizeof(double2);
-constexpr size_t kBwdTheta = 12 * kThreads * sizeof(double);
-constexpr size_t kBwdSmem = kBwdStage + kBwdTrans + kBwdTheta;
+// transpose buffer.
+constexpr size_t kBwdSmem = 3 * kTileSize * sizeof(double2);
 constexpr size_t kFwdSmem = kTileSize * sizeof(double2);
 
 // ---------------------------------------------------------------- backward
 template <int LSRC, int PDST, int LDST, bool PHASE>
-__global__ void __launch_bounds__(kThreads, 1) bwd_pass_kernel(const PassParams P) {
+__global__ void __launch_bounds__(bw::kT, 1) bwd_pass_kernel(const PassParams P) {
+  using namespace bw;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2 *stage_a = reinterpret_cast<double2 *>(smem_raw);
   double2 *stage_b = stage_a + kTileSize;
   double2 *trans = stage_b + kTileSize;
-  double *theta_sm = reinterpret_cast<double *>(trans + kTileSize);
-  __shared__ double red[8][12];
+  __shared__ double red[16][12];
   __shared__ double phi_sm[33];
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int n = P.n;
-  const int first_layout = P.seq_layout[0];
 
-  const int tp0 = thread_part(0, lane, warp);
-  const u32 toff0 = thread_offset(P, tp0);
-  const u32 v8 = P.vec[8], v9 = P.vec[9], v10 = P.vec[10], v11 = P.vec[11];
-  const int tpf = thread_part(first_layout, lane, warp);
-  const u32 tofff = thread_offset(P, tpf);
-  const int rbf = reg_shift(first_layout);
-  const u32 f0 = P.vec[rbf], f1 = P.vec[rbf + 1], f2 = P.vec[rbf + 2], f3 = P.vec[rbf + 3];
-
+  // groups with gates: G3 (bits 9..11, layout 0) .. G0 (bits 0..2, layout 3)
+  bool gv[4];
 #pragma unroll
-  for (int b = 0; b < 12; ++b) theta_sm[b * kThreads + threadIdx.x] = 0.0;
-  if (PHASE && threadIdx.x < 33) phi_sm[threadIdx.x] = 0.0;
+  for (int g = 0; g < 4; ++g)
+    gv[g] = P.gate_wire[3 * g] >= 0 || P.gate_wire[3 * g + 1] >= 0 || P.gate_wire[3 * g + 2] >= 0;
+  const int first = gv[2] ? 1 : (gv[1] ? 2 : (gv[0] ? 3 : 0));
+
+  const int tp0 = tpart(0, lane, warp);
+  const u32 toff0 = thread_offset(P, tp0);
+  const u32 v9 = P.vec[9], v10 = P.vec[10], v11 = P.vec[11];
+  const int tpf = tpart(first, lane, warp);
+  const int rbf = rshift(first);
+
+  double2 ratio[4];
+  u32 tofff = 0;
+  if (PHASE) {
+    tofff = thread_offset(P, tpf);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) ratio[j] = phase_ratio(P, unit_bit(P.vec[rbf + j]));
+    ratio[3] = make_double2(1.0, 0.0);
+    if (threadIdx.x < 33) phi_sm[threadIdx.x] = 0.0;
+  }
+  double acc[12];
+#pragma unroll
+  for (int i = 0; i < 12; ++i) acc[i] = 0.0;
 
   const u32 num_tiles = static_cast<u32>(P.num_tiles);
   auto issue = [&](u32 tile) {
     const u32 base = deposit(P, tile) ^ toff0;
 #pragma unroll
-    for (int r = 0; r < kRegs; ++r) {
-      const u32 p = base ^ reg_offset(r, v8, v9, v10, v11);
-      const int s = swz(tp0 | (r << 8));
+    for (int r = 0; r < kR; ++r) {
+      const u32 p = base ^ ((r & 1) ? v9 : 0u) ^ ((r & 2) ? v10 : 0u) ^ ((r & 4) ? v11 : 0u);
+      const int s = swz(tp0 | (r << 9));
       cp_async16(&stage_a[s], &P.psi_in[p]);
       cp_async16(&stage_b[s], &P.lam_in[source_index<LSRC>(p, n)]);
     }
@@ -285,9 +403,9 @@ __global__ void __launch_bounds__(kThreads, 1) bwd_pass_kernel(const PassParams 
   for (u32 tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
     cp_async_wait_all();
     __syncthreads();
-    double2 a[kRegs], b[kRegs];
+    double2 a[kR], b[kR];
 #pragma unroll
-    for (int r = 0; r < kRegs; ++r) {
+    for (int r = 0; r < kR; ++r) {
       const int s = swz(tpf | (r << rbf));
       a[r] = stage_a[s];
       b[r] = stage_b[s];
@@ -297,41 +415,43 @@ __global__ void __launch_bounds__(kThreads, 1) bwd_pass_kernel(const PassParams 
 
     const u32 cbase = deposit(P, tile);
     if (PHASE) {
-      const u32 base = cbase ^ tofff;
-#pragma unroll
-      for (int r = 0; r < kRegs; ++r) {
-        const double2 ph = table4(P.ptab, base ^ reg_offset(r, f0, f1, f2, f3));
-        a[r] = cmul_conj(a[r], ph);
-        b[r] = cmul_conj(b[r], ph);
-      }
-      accumulate_phi(P, first_layout, cbase, lane, warp, a, b, red, phi_sm);
+      // RZ^dagger of the layer on psi and lambda, then the phi sums.
+      apply_phase_gray<3, true, true>(table4(P.ptab, cbase ^ tofff), ratio, a, b);
+      phi_sums(P, first, cbase, lane, warp, a, b, red, phi_sm);
     }
 
-    int prev = first_layout;
-    for (int k = 0; k < P.nseq; ++k) {
-      const int layout = P.seq_layout[k];
-      const int tp = thread_part(layout, lane, warp);
-      if (k > 0) {
-        const int tpp = thread_part(prev, lane, warp);
-        transpose(trans, tpp, reg_shift(prev), tp, reg_shift(layout), a);
-        transpose(trans, tpp, reg_shift(prev), tp, reg_shift(layout), b);
-      }
-      if (P.seq_apply[k]) {
-        double acc[4];
-        apply_gates<true>(P, layout, tp, a, b, acc);
-        const int rb = reg_shift(layout);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) theta_sm[(rb + j) * kThreads + threadIdx.x] += acc[j];
-      }
-      prev = layout;
+    int cur = first;
+    if (gv[2]) {
+      gates<1>(P, tpart(1, lane, warp), a, b, acc);
+      cur = 1;
     }
+    if (gv[1]) {
+      if (cur != 2) {
+        transpose(trans, tpart(cur, lane, warp), rshift(cur), tpart(2, lane, warp), 3, a);
+        transpose(trans, tpart(cur, lane, warp), rshift(cur), tpart(2, lane, warp), 3, b);
+      }
+      gates<2>(P, tpart(2, lane, warp), a, b, acc);
+      cur = 2;
+    }
+    if (gv[0]) {
+      if (cur != 3) {
+        transpose(trans, tpart(cur, lane, warp), rshift(cur), tpart(3, lane, warp), 0, a);
+        transpose(trans, tpart(cur, lane, warp), rshift(cur), tpart(3, lane, warp), 0, b);
+      }
+      gates<3>(P, tpart(3, lane, warp), a, b, acc);
+      cur = 3;
+    }
+    if (cur != 0) {
+      transpose(trans, tpart(cur, lane, warp), rshift(cur), tp0, 9, a);
+      transpose(trans, tpart(cur, lane, warp), rshift(cur), tp0, 9, b);
+    }
+    if (gv[3]) gates<0>(P, tp0, a, b, acc);
 
-    // stores from layout 0
     if (PDST != kStoreNone || LDST != kStoreNone) {
       const u32 base = cbase ^ toff0;
 #pragma unroll
-      for (int r = 0; r < kRegs; ++r) {
-        const u32 p = base ^ reg_offset(r, v8, v9, v10, v11);
+      for (int r = 0; r < kR; ++r) {
+        const u32 p = base ^ ((r & 1) ? v9 : 0u) ^ ((r & 2) ? v10 : 0u) ^ ((r & 4) ? v11 : 0u);
         store_amp<PDST>(P.psi_out, p, n, a[r]);
         store_amp<LDST>(P.lam_out, p, n, b[r]);
       }
@@ -340,15 +460,17 @@ __global__ void __launch_bounds__(kThreads, 1) bwd_pass_kernel(const PassParams 
 
   // CTA reduction of the theta sums, then one record per CTA.
   __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 12; ++i) {
+    const double s = warp_sum(acc[i]);
+    if (lane == 0) red[warp][i] = s;
+  }
+  __syncthreads();
   double *rec = P.partials + static_cast<size_t>(blockIdx.x) * kPartialStride;
-  {
-    // 12 tile bits x 256 threads: warp w reduces tile bits w and w + 8 (< 12)
-    for (int tb = warp; tb < 12; tb += 8) {
-      double s = 0.0;
-      for (int t = lane; t < kThreads; t += 32) s += theta_sm[tb * kThreads + t];
-      s = warp_sum(s);
-      if (lane == 0) rec[tb] = s;
-    }
+  if (threadIdx.x < 12) {
+    double s = 0.0;
+    for (int ww = 0; ww < 16; ++ww) s += red[ww][threadIdx.x];
+    rec[threadIdx.x] = s;
   }
   if (PHASE) {
     if (threadIdx.x < 31) rec[kPartialPhi + threadIdx.x] = phi_sm[threadIdx.x];
@@ -370,6 +492,11 @@ __global__ void __launch_bounds__(kThreads, 2) fwd_pass_kernel(const PassParams 
   const u32 num_tiles = static_cast<u32>(P.num_tiles);
   double acc[4];
   double2 dummy[kRegs];
+  double2 ratio[4];
+  if (PHASE) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) ratio[j] = phase_ratio(P, unit_bit(P.vec[8 + j]));
+  }
 
   for (u32 tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
     const u32 base = deposit(P, tile) ^ toff0;
@@ -392,10 +519,7 @@ __global__ void __launch_bounds__(kThreads, 2) fwd_pass_kernel(const PassParams 
       prev = layout;
     }
 
-    if (PHASE) {
-#pragma unroll
-      for (int r = 0; r < kRegs; ++r) a[r] = cmul(a[r], table4(P.ptab, base ^ reg_offset(r, v8, v9, v10, v11)));
-    }
+    if (PHASE) apply_phase_gray<4, false, false>(table4(P.ptab, base), ratio, a, dummy);
 #pragma unroll
     for (int r = 0; r < kRegs; ++r) store_amp<PDST>(P.psi_out, base ^ reg_offset(r, v8, v9, v10, v11), n, a[r]);
   }
@@ -411,7 +535,7 @@ cudaError_t launch_bwd(const PassParams &P, int grid, cudaStream_t s) {
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  k<<<grid, kThreads, kBwdSmem, s>>>(P);
+  k<<<grid, bw::kT, kBwdSmem, s>>>(P);
   return cudaGetLastError();
 }
 
