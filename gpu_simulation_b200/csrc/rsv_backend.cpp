@@ -92,14 +92,17 @@ Tile unit_tile(int phys, const std::vector<int> &bits, const std::vector<int> &g
 
 // "Antipodal" tile span(e_0..e_10, all-ones): its image under P^{-1} is the
 // contiguous block span(e_0..e_11), so a scatter through P^{-1} from it writes
-// whole 4096-amplitude blocks.  Gates on wires 0..10.  Needs n >= 13.
+// whole 4096-amplitude blocks.  Gates on wires 0..10.  Needs n >= 13.  The
+// twelfth direction is stored as bits 11..n-1 (all-ones minus e_0..e_10, the
+// same subspace) so that it never touches a gated wire: every register pair
+// along a gated direction then holds (|0>, |1>) in that order.
 Tile antipodal_tile(int n) {
   Tile t;
   for (int b = 0; b < 11; ++b) {
     t.vec[b] = u64{1} << b;
     t.gate_wire[b] = b;
   }
-  t.vec[11] = (u64{1} << n) - 1;
+  t.vec[11] = ((u64{1} << n) - 1) & ~u64{0x7FF};
   t.num_runs = 1;
   t.run_start[0] = 11;
   t.run_len[0] = n - 12;
@@ -411,6 +414,9 @@ struct rsv_backend {
   rsv::DevBuf<double2> ptab, prod;
   rsv::DevBuf<double> energy_partials, pass_partials, outputs;  // outputs: [1 + num_params]
   rsv::DevBuf<int> tables;  // pass_grid | theta_pass | theta_slot | phi_pass
+  rsv::DevBuf<int> order;   // undo order of the wires within a backward layer
+  rsv::DevBuf<double2> rot;
+  rsv::DevBuf<double> lscale, gscale;
   rsv::HostBuf<double4> coef_host;
   rsv::HostBuf<double> out_host;
   int energy_grid = 1;
@@ -490,20 +496,13 @@ void fill_pass_params(rsv_backend *B, const Step &s, PassParams &P) {
   P.phase = s.phase;
   P.phi_grad = s.phi_grad;
   P.sync_after_load = (s.tile.num_tiles == 1) ? 1 : 0;
-  // A direction with several physical bits that overlaps a gated wire flips
-  // that wire's bit; the planner's only such direction is tile bit 11 of the
-  // antipodal tile, which overlaps every gated wire.
-  P.flip_bit = kTileBits;
+  // Pair roles: a gated wire's bit must come from its unit direction only.
   for (int b = 0; b < 12; ++b) {
     const u64 v = s.tile.vec[b];
     if ((v & (v - 1)) == 0) continue;
     for (int g = 0; g < 12; ++g) {
       const int w = s.tile.gate_wire[g];
-      if (w >= 0 && ((v >> w) & 1)) {
-        if (P.flip_bit != kTileBits && P.flip_bit != b)
-          throw Error(RSV_ERR_INTERNAL, "tile with two flipping directions");
-        P.flip_bit = b;
-      }
+      if (w >= 0 && ((v >> w) & 1)) throw Error(RSV_ERR_INTERNAL, "multi-bit direction overlaps a gated wire");
     }
   }
   P.psi_in = s.psi_in >= 0 ? B->buf[s.psi_in].p : nullptr;
@@ -511,6 +510,8 @@ void fill_pass_params(rsv_backend *B, const Step &s, PassParams &P) {
   P.lam_in = s.lam_in >= 0 ? B->buf[s.lam_in].p : nullptr;
   P.lam_out = s.lam_out >= 0 ? B->buf[s.lam_out].p : nullptr;
   P.coef = B->coef.p;
+  P.rot = B->rot.p;
+  P.lscale = B->lscale.p;
   P.ptab = B->ptab.p + static_cast<size_t>(s.layer) * 1024;
   P.prod = B->prod.p;
   P.partials = s.bwd ? B->pass_partials.p + static_cast<size_t>(s.pass_index) * B->plan.max_grid *
@@ -599,6 +600,7 @@ void run_finalize(rsv_backend *B, bool grad, double *energy_out, double *grad_ou
   F.theta_pass = B->tables.p + np;
   F.theta_slot = B->tables.p + np + nl;
   F.phi_pass = B->tables.p + np + 2 * nl;
+  F.gscale = B->gscale.p;
   F.energy_out = energy_out;
   F.grad_out = grad ? grad_out : nullptr;
   timed(B, st, 4, 0.0, [&] { check(launch_finalize(F, st), "finalize launch"); });
@@ -622,6 +624,10 @@ void run_all(rsv_backend *B, bool grad, double *energy_out, double *grad_out, cu
   B->forward_only_state = false;
   timed(B, st, 0, 0.0, [&] {
     check(launch_tables(B->coef.p, B->n, B->L, B->ptab.p, B->prod.p, st), "tables launch");
+  });
+  timed(B, st, 0, 0.0, [&] {
+    check(launch_rot(B->coef.p, B->n, B->L, B->order.p, B->rot.p, B->lscale.p, B->gscale.p, st),
+          "rot launch");
   });
   run_forward(B, st);
   run_energy(B, st);
@@ -759,6 +765,28 @@ rsv_status rsv_create(int num_qubits, int num_layers, double field, const char *
     B->tables.alloc(tab.size());
     check(cudaMemcpy(B->tables.p, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice),
           "plan table upload");
+    B->rot.alloc(nl);
+    B->lscale.alloc(num_layers);
+    B->gscale.alloc(2 * nl);
+    {
+      // Undo order of the wires within one backward layer, as the backward
+      // pass kernel visits them: passes in plan order; inside a pass the
+      // register groups of tile bits 6..8, 3..5, 0..2, then 9..11.
+      std::vector<int> ord;
+      const int L1 = num_layers - 1;
+      for (const auto &s : B->plan.bwd) {
+        if (s.layer != L1) continue;
+        for (int g : {2, 1, 0, 3})
+          for (int j = 0; j < 3; ++j) {
+            const int w = s.tile.gate_wire[3 * g + j];
+            if (w >= 0) ord.push_back(w);
+          }
+      }
+      if (static_cast<int>(ord.size()) != num_qubits) throw Error(RSV_ERR_INTERNAL, "undo order incomplete");
+      B->order.alloc(ord.size());
+      check(cudaMemcpy(B->order.p, ord.data(), ord.size() * sizeof(int), cudaMemcpyHostToDevice),
+            "order upload");
+    }
     B->coef_host.alloc(nl);
     B->out_host.alloc(1 + B->num_params);
     check(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -865,6 +893,8 @@ rsv_status rsv_profile_energy_and_grad(rsv_backend *B, const double *params, siz
     B->forward_only_state = false;
     cudaEventRecord(ev[0], st);
     check(launch_tables(B->coef.p, B->n, B->L, B->ptab.p, B->prod.p, st), "tables launch");
+    check(launch_rot(B->coef.p, B->n, B->L, B->order.p, B->rot.p, B->lscale.p, B->gscale.p, st),
+          "rot launch");
     cudaEventRecord(ev[1], st);
     run_forward(B, st);
     cudaEventRecord(ev[2], st);
@@ -909,6 +939,8 @@ rsv_status rsv_benchmark_forward_graph(rsv_backend *B, const double *params, siz
     upload_host_coefs(B, params, st);
     auto forward = [&] {
       check(launch_tables(B->coef.p, B->n, B->L, B->ptab.p, B->prod.p, st), "tables launch");
+      check(launch_rot(B->coef.p, B->n, B->L, B->order.p, B->rot.p, B->lscale.p, B->gscale.p, st),
+            "rot launch");
       run_forward(B, st);
     };
     cudaEvent_t a, b;

@@ -60,6 +60,46 @@ __global__ void tables_kernel(const double4 *__restrict__ coef, int n, int L,
   }
 }
 
+// Tangent form of the RY rotations (one FMA per component instead of two).
+// For every (layer, wire): |cos| >= |sin| -> f = cos t/2, RY = f [[1,-k],[k,1]],
+// k = tan t/2 (mode +1); otherwise f = sin t/2, RY = f [[k,-1],[1,k]],
+// k = cot t/2 (mode -1).  |f| >= 1/sqrt(2), so no factor over- or underflows.
+// The passes apply RY / f; the product K_l of a layer's factors is applied
+// once with the layer's RZ phase, so states between layers are exact.
+// Inside a backward layer the state carries the factors of the wires not
+// yet undone; gscale[] holds the exact correction of every gradient sum:
+//   theta of wire w: 1 / (prod of f over the wires of its layer still pending
+//                         when w is undone, w included)^2,
+//   phi of the layer: 1 / K_l^2.
+// order[n] is the undo order of the wires within a backward layer.
+// grid: L blocks of 32 threads.
+__global__ void rot_kernel(const double4 *__restrict__ coef, int n, int L, const int *__restrict__ order,
+                           double2 *__restrict__ rot, double *__restrict__ lscale,
+                           double *__restrict__ gscale) {
+  const int layer = blockIdx.x;
+  if (layer >= L) return;
+  for (int w = threadIdx.x; w < n; w += blockDim.x) {
+    const double4 k = coef[layer * n + w];
+    rot[layer * n + w] = (fabs(k.x) >= fabs(k.y)) ? make_double2(k.y / k.x, 1.0)
+                                                   : make_double2(k.x / k.y, -1.0);
+  }
+  if (threadIdx.x != 0) return;
+  auto factor = [&](int w) {
+    const double4 k = coef[layer * n + w];
+    return (fabs(k.x) >= fabs(k.y)) ? k.x : k.y;
+  };
+  double K = 1.0;
+  for (int w = 0; w < n; ++w) K *= factor(w);
+  lscale[layer] = K;
+  double pending = K;
+  for (int i = 0; i < n; ++i) {
+    const int w = order[i];
+    gscale[2 * (layer * n + w)] = 1.0 / (pending * pending);
+    gscale[2 * (layer * n + w) + 1] = 1.0 / (K * K);
+    pending /= factor(w);
+  }
+}
+
 // ------------------------------------------------------------------------
 // Energy: mu = (P^T H P) chi and E = sum Re(conj(chi) mu), in the frame of the
 // last layer before its CNOT ring (the ring is folded into H).  Equivalent to
@@ -136,7 +176,7 @@ __global__ void finalize_kernel(const FinalizeParams F) {
       const double *rec = F.pass_partials + static_cast<size_t>(pass) * F.max_grid * kPartialStride;
       double s = 0.0;
       for (int c = 0; c < F.pass_grid[pass]; ++c) s += rec[static_cast<size_t>(c) * kPartialStride + slot];
-      F.grad_out[2 * k] = s;
+      F.grad_out[2 * k] = s * F.gscale[2 * k];
     }
     {
       const int pass = F.phi_pass[layer];
@@ -146,7 +186,7 @@ __global__ void finalize_kernel(const FinalizeParams F) {
         tot += rec[static_cast<size_t>(c) * kPartialStride + kPartialTot];
         bw += rec[static_cast<size_t>(c) * kPartialStride + kPartialPhi + w];
       }
-      F.grad_out[2 * k + 1] = tot - 2.0 * bw;
+      F.grad_out[2 * k + 1] = (tot - 2.0 * bw) * F.gscale[2 * k + 1];
     }
   }
 }
@@ -163,6 +203,12 @@ cudaError_t launch_coef(const double *params, double4 *coef, int count, cudaStre
 cudaError_t launch_tables(const double4 *coef, int n, int L, double2 *ptab, double2 *prod,
                           cudaStream_t s) {
   tables_kernel<<<(L + 1) * 4, 256, 0, s>>>(coef, n, L, ptab, prod);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rot(const double4 *coef, int n, int L, const int *order, double2 *rot,
+                       double *lscale, double *gscale, cudaStream_t s) {
+  rot_kernel<<<L, 32, 0, s>>>(coef, n, L, order, rot, lscale, gscale);
   return cudaGetLastError();
 }
 

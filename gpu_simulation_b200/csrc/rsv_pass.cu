@@ -112,47 +112,34 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-// Rotate the register pairs of the four register bits of `layout`.  Pair
-// (r, r | 2^j) holds (|0>, |1>) of wire gate_wire[rb + j] -- or (|1>, |0>) where
-// the tile's flip coordinate is 1 (antipodal tile), which is the same update
-// with s -> -s and the theta contribution negated.
-template <bool BWD>
-__device__ __forceinline__ void apply_gates(const PassParams &P, int layout, int tp,
-                                            double2 (&a)[kRegs], double2 (&b)[kRegs],
-                                            double (&acc)[4]) {
+// Forward rotation of the four register bits of `layout` (tile bits
+// rb..rb+3): RY / f in tangent form, one FMA per component.
+//   mode +1: [[1,-k],[k,1]]    mode -1: [[k,-1],[1,k]]
+__device__ __forceinline__ void apply_gates_fwd(const PassParams &P, int layout, double2 (&a)[kRegs]) {
   const int rb = reg_shift(layout);
-  const int fb = P.flip_bit;
-  const bool thread_flip = fb < kTileBits && ((tp >> fb) & 1);
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
-    acc[j] = 0.0;
     const int w = P.gate_wire[rb + j];
     if (w < 0) continue;
-    const double2 cs = __ldg(reinterpret_cast<const double2 *>(&P.coef[P.layer * P.n + w]));
-    const double c = cs.x;
+    const double2 km = __ldg(&P.rot[P.layer * P.n + w]);
+    const double k = km.x;
+    if (km.y > 0.0) {
 #pragma unroll
-    for (int r = 0; r < kRegs; ++r) {
-      if (r & (1 << j)) continue;
-      const int r1 = r | (1 << j);
-      // flip coordinate of this register pair (equal for r and r1: the flip
-      // direction is never gated)
-      const bool reg_flip = fb < kTileBits && (((r << rb) >> fb) & 1);
-      const double sg = (thread_flip != reg_flip) ? -1.0 : 1.0;
-      const double s = sg * cs.y;
-      const double2 x0 = a[r], x1 = a[r1];
-      if (!BWD) {
-        a[r] = make_double2(fma(c, x0.x, -s * x1.x), fma(c, x0.y, -s * x1.y));
-        a[r1] = make_double2(fma(s, x0.x, c * x1.x), fma(s, x0.y, c * x1.y));
-      } else {
-        const double2 y0 = b[r], y1 = b[r1];
-        // theta: Re(conj(lam1) psi0) - Re(conj(lam0) psi1) in the frame with the
-        // layer's RZ removed: the reference's 2 Re<lam_mid|dRY|psi_before>
-        // (cpp/ising_cuda_statevector_grad_kernels.cu:289-307) simplified.
-        acc[j] += sg * (fma(y1.x, x0.x, y1.y * x0.y) - fma(y0.x, x1.x, y0.y * x1.y));
-        a[r] = make_double2(fma(c, x0.x, s * x1.x), fma(c, x0.y, s * x1.y));
-        a[r1] = make_double2(fma(-s, x0.x, c * x1.x), fma(-s, x0.y, c * x1.y));
-        b[r] = make_double2(fma(c, y0.x, s * y1.x), fma(c, y0.y, s * y1.y));
-        b[r1] = make_double2(fma(-s, y0.x, c * y1.x), fma(-s, y0.y, c * y1.y));
+      for (int r = 0; r < kRegs; ++r) {
+        if (r & (1 << j)) continue;
+        const int r1 = r | (1 << j);
+        const double2 x0 = a[r], x1 = a[r1];
+        a[r] = make_double2(fma(-k, x1.x, x0.x), fma(-k, x1.y, x0.y));
+        a[r1] = make_double2(fma(k, x0.x, x1.x), fma(k, x0.y, x1.y));
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < kRegs; ++r) {
+        if (r & (1 << j)) continue;
+        const int r1 = r | (1 << j);
+        const double2 x0 = a[r], x1 = a[r1];
+        a[r] = make_double2(fma(k, x0.x, -x1.x), fma(k, x0.y, -x1.y));
+        a[r1] = make_double2(fma(k, x1.x, x0.x), fma(k, x1.y, x0.y));
       }
     }
   }
@@ -249,36 +236,56 @@ __device__ __forceinline__ void transpose(double2 *sm, int tp_from, int rb_from,
   __syncthreads();
 }
 
-// Backward rotation of the three register bits of layout L (tile bits RB..RB+2).
+// Backward rotation of the three register bits of layout L (tile bits
+// RB..RB+2): RY^dagger / f in tangent form, one FMA per component,
+//   mode +1: [[1,k],[-k,1]]    mode -1: [[k,1],[-1,k]],
+// preceded by the theta sum Re(conj(lam1) psi0) - Re(conj(lam0) psi1) of the
+// pair in the frame with the layer's RZ removed -- the reference's
+// 2 Re<lam_mid|dRY|psi_before> (cpp/ising_cuda_statevector_grad_kernels.cu:289-307)
+// simplified; the factors f still pending are corrected in the final reduction.
 template <int L>
-__device__ __forceinline__ void gates(const PassParams &P, int tp, double2 (&a)[kR], double2 (&b)[kR],
+__device__ __forceinline__ void gates(const PassParams &P, double2 (&a)[kR], double2 (&b)[kR],
                                       double (&acc)[12]) {
   constexpr int RB = 9 - 3 * L;
-  const int fb = P.flip_bit;
-  const bool thread_flip = fb < kTileBits && ((tp >> fb) & 1);
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
     const int w = P.gate_wire[RB + j];
     if (w < 0) continue;
-    const double2 cs = __ldg(reinterpret_cast<const double2 *>(&P.coef[P.layer * P.n + w]));
-    const double c = cs.x;
+    const double2 km = __ldg(&P.rot[P.layer * P.n + w]);
+    const double k = km.x;
+    double t = acc[RB + j];
+    if (km.y > 0.0) {
 #pragma unroll
-    for (int r = 0; r < kR; ++r) {
-      if (r & (1 << j)) continue;
-      const int r1 = r | (1 << j);
-      const bool reg_flip = fb < kTileBits && (((r << RB) >> fb) & 1);
-      const double sg = (thread_flip != reg_flip) ? -1.0 : 1.0;
-      const double s = sg * cs.y;
-      const double2 x0 = a[r], x1 = a[r1], y0 = b[r], y1 = b[r1];
-      // theta: Re(conj(lam1) psi0) - Re(conj(lam0) psi1) in the frame with the
-      // layer's RZ removed: the reference's 2 Re<lam_mid|dRY|psi_before>
-      // (cpp/ising_cuda_statevector_grad_kernels.cu:289-307) simplified.
-      acc[RB + j] += sg * (fma(y1.x, x0.x, y1.y * x0.y) - fma(y0.x, x1.x, y0.y * x1.y));
-      a[r] = make_double2(fma(c, x0.x, s * x1.x), fma(c, x0.y, s * x1.y));
-      a[r1] = make_double2(fma(-s, x0.x, c * x1.x), fma(-s, x0.y, c * x1.y));
-      b[r] = make_double2(fma(c, y0.x, s * y1.x), fma(c, y0.y, s * y1.y));
-      b[r1] = make_double2(fma(-s, y0.x, c * y1.x), fma(-s, y0.y, c * y1.y));
+      for (int r = 0; r < kR; ++r) {
+        if (r & (1 << j)) continue;
+        const int r1 = r | (1 << j);
+        const double2 x0 = a[r], x1 = a[r1], y0 = b[r], y1 = b[r1];
+        t = fma(y1.x, x0.x, t);
+        t = fma(y1.y, x0.y, t);
+        t = fma(-y0.x, x1.x, t);
+        t = fma(-y0.y, x1.y, t);
+        a[r] = make_double2(fma(k, x1.x, x0.x), fma(k, x1.y, x0.y));
+        a[r1] = make_double2(fma(-k, x0.x, x1.x), fma(-k, x0.y, x1.y));
+        b[r] = make_double2(fma(k, y1.x, y0.x), fma(k, y1.y, y0.y));
+        b[r1] = make_double2(fma(-k, y0.x, y1.x), fma(-k, y0.y, y1.y));
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < kR; ++r) {
+        if (r & (1 << j)) continue;
+        const int r1 = r | (1 << j);
+        const double2 x0 = a[r], x1 = a[r1], y0 = b[r], y1 = b[r1];
+        t = fma(y1.x, x0.x, t);
+        t = fma(y1.y, x0.y, t);
+        t = fma(-y0.x, x1.x, t);
+        t = fma(-y0.y, x1.y, t);
+        a[r] = make_double2(fma(k, x0.x, x1.x), fma(k, x0.y, x1.y));
+        a[r1] = make_double2(fma(k, x1.x, -x0.x), fma(k, x1.y, -x0.y));
+        b[r] = make_double2(fma(k, y0.x, y1.x), fma(k, y0.y, y1.y));
+        b[r1] = make_double2(fma(k, y1.x, -y0.x), fma(k, y1.y, -y0.y));
+      }
     }
+    acc[RB + j] = t;
   }
 }
 
@@ -416,13 +423,15 @@ __global__ void __launch_bounds__(bw::kT, 1) bwd_pass_kernel(const PassParams P)
     const u32 cbase = deposit(P, tile);
     if (PHASE) {
       // RZ^dagger of the layer on psi and lambda, then the phi sums.
-      apply_phase_gray<3, true, true>(table4(P.ptab, cbase ^ tofff), ratio, a, b);
+      const double2 ph = table4(P.ptab, cbase ^ tofff);
+      const double K = P.lscale[P.layer];
+      apply_phase_gray<3, true, true>(make_double2(K * ph.x, K * ph.y), ratio, a, b);
       phi_sums(P, first, cbase, lane, warp, a, b, red, phi_sm);
     }
 
     int cur = first;
     if (gv[2]) {
-      gates<1>(P, tpart(1, lane, warp), a, b, acc);
+      gates<1>(P, a, b, acc);
       cur = 1;
     }
     if (gv[1]) {
@@ -430,7 +439,7 @@ __global__ void __launch_bounds__(bw::kT, 1) bwd_pass_kernel(const PassParams P)
         transpose(trans, tpart(cur, lane, warp), rshift(cur), tpart(2, lane, warp), 3, a);
         transpose(trans, tpart(cur, lane, warp), rshift(cur), tpart(2, lane, warp), 3, b);
       }
-      gates<2>(P, tpart(2, lane, warp), a, b, acc);
+      gates<2>(P, a, b, acc);
       cur = 2;
     }
     if (gv[0]) {
@@ -438,14 +447,14 @@ __global__ void __launch_bounds__(bw::kT, 1) bwd_pass_kernel(const PassParams P)
         transpose(trans, tpart(cur, lane, warp), rshift(cur), tpart(3, lane, warp), 0, a);
         transpose(trans, tpart(cur, lane, warp), rshift(cur), tpart(3, lane, warp), 0, b);
       }
-      gates<3>(P, tpart(3, lane, warp), a, b, acc);
+      gates<3>(P, a, b, acc);
       cur = 3;
     }
     if (cur != 0) {
       transpose(trans, tpart(cur, lane, warp), rshift(cur), tp0, 9, a);
       transpose(trans, tpart(cur, lane, warp), rshift(cur), tp0, 9, b);
     }
-    if (gv[3]) gates<0>(P, tp0, a, b, acc);
+    if (gv[3]) gates<0>(P, a, b, acc);
 
     if (PDST != kStoreNone || LDST != kStoreNone) {
       const u32 base = cbase ^ toff0;
@@ -490,7 +499,6 @@ __global__ void __launch_bounds__(kThreads, 2) fwd_pass_kernel(const PassParams 
   const u32 toff0 = thread_offset(P, tp0);
   const u32 v8 = P.vec[8], v9 = P.vec[9], v10 = P.vec[10], v11 = P.vec[11];
   const u32 num_tiles = static_cast<u32>(P.num_tiles);
-  double acc[4];
   double2 dummy[kRegs];
   double2 ratio[4];
   if (PHASE) {
@@ -515,11 +523,15 @@ __global__ void __launch_bounds__(kThreads, 2) fwd_pass_kernel(const PassParams 
       const int layout = P.seq_layout[k];
       const int tp = thread_part(layout, lane, warp);
       if (k > 0) transpose(trans, thread_part(prev, lane, warp), reg_shift(prev), tp, reg_shift(layout), a);
-      if (P.seq_apply[k]) apply_gates<false>(P, layout, tp, a, dummy, acc);
+      if (P.seq_apply[k]) apply_gates_fwd(P, layout, a);
       prev = layout;
     }
 
-    if (PHASE) apply_phase_gray<4, false, false>(table4(P.ptab, base), ratio, a, dummy);
+    if (PHASE) {
+      const double2 ph = table4(P.ptab, base);
+      const double K = P.lscale[P.layer];
+      apply_phase_gray<4, false, false>(make_double2(K * ph.x, K * ph.y), ratio, a, dummy);
+    }
 #pragma unroll
     for (int r = 0; r < kRegs; ++r) store_amp<PDST>(P.psi_out, base ^ reg_offset(r, v8, v9, v10, v11), n, a[r]);
   }

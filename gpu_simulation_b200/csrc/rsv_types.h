@@ -47,7 +47,6 @@ struct PassParams {
   int phase;                   // fwd: apply D after gates; bwd: apply D^dagger before gates
   int phi_grad;                // bwd: accumulate the phi-gradient sums of the layer
   int sync_after_load;         // single-tile in-place permutation: all loads before any store
-  int flip_bit;                // tile bit whose direction also flips gated wires (12 = none)
   int nseq;                    // register layouts visited by the pass, in order
   int seq_layout[4];           // layout id (0, 1, 2) of each visit; the last is 0
   int seq_apply[4];            // whether the visit rotates its register tile bits
@@ -56,6 +55,9 @@ struct PassParams {
   const double2 *lam_in;
   double2 *lam_out;
   const double4 *coef;         // [L * n] (cos t/2, sin t/2, cos p/2, sin p/2)
+  const double2 *rot;          // [L * n] tangent form of RY: (k, +1) = [[1,-k],[k,1]] (k = tan t/2)
+                               // or (k, -1) = [[k,-1],[1,k]] (k = cot t/2), RY divided by f
+  const double *lscale;        // [L] product of the divided factors f of each layer
   const double2 *ptab;         // phase byte tables of this layer, [4][256]
   const double2 *prod;         // layer-0 product-state byte tables, [4][256]
   double *partials;            // [gridDim.x][kPartialStride] for this pass
@@ -72,6 +74,7 @@ struct FinalizeParams {
   const int *theta_pass;         // [L*n]
   const int *theta_slot;         // [L*n]
   const int *phi_pass;           // [L]
+  const double *gscale;          // [2 L n] multiplier of every gradient sum
   double *energy_out;
   double *grad_out;              // [2 L n] or null
 };
