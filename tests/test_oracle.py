@@ -95,3 +95,18 @@ def test_hamiltonian_matches_sparse_matrix():
     H = oracle.hamiltonian_sparse(n, h)
     np.testing.assert_allclose(lam, H @ psi, atol=1e-12)
     assert abs(e - np.vdot(psi, H @ psi).real) < 1e-9
+
+
+def test_oracle_matches_reference_golden_vectors():
+    """Golden vectors produced by the reference's own CUDA extension (rebuilt
+    for sm_100a, tests/golden/make_ref_golden.py) pin the oracle at 1e-10."""
+    data = json.loads((GOLDEN / "ref_golden.json").read_text())
+    assert len(data["cases"]) >= 15
+    for case in data["cases"]:
+        n, L, h = case["n"], case["L"], case["h"]
+        if n > 18:
+            continue  # the larger cases are checked on the GPU
+        p = np.random.default_rng(case["seed"]).uniform(0.0, 2.0 * np.pi, 2 * n * L)
+        e, g = oracle.energy_and_grad(n, L, h, p)
+        assert abs(e - case["energy"]) < 1e-10, (n, L, e, case["energy"])
+        np.testing.assert_allclose(g, np.asarray(case["gradient"]), atol=1e-10, rtol=0)

@@ -114,3 +114,17 @@ def test_wrong_parameter_count_raises_value_error():
     eng = Engine(6, 2, 1.0)
     with pytest.raises(ValueError):
         eng.energy_and_grad(np.zeros(5))
+
+
+def test_engine_matches_reference_golden_vectors():
+    """All golden vectors of the reference's own extension (including n=20)."""
+    import json
+    from pathlib import Path
+
+    data = json.loads((Path(__file__).parent / "golden" / "ref_golden.json").read_text())
+    for case in data["cases"]:
+        n, L, h = case["n"], case["L"], case["h"]
+        p = np.random.default_rng(case["seed"]).uniform(0.0, 2.0 * np.pi, 2 * n * L)
+        e, g = Engine(n, L, h).energy_and_grad(p)
+        assert abs(e - case["energy"]) < TOL, (n, L)
+        np.testing.assert_allclose(g, np.asarray(case["gradient"]), atol=TOL, rtol=0)
