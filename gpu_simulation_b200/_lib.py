@@ -38,6 +38,9 @@ _SIGNATURES = {
                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "rsv_benchmark_forward_graph": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t,
                                      _c_double_p, _c_double_p], ctypes.c_int),
+    "rsv_energy_and_grad_noalloc": ([ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_void_p,
+                                     ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+                                    ctypes.c_int),
     "rsv_set_launch_timing": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "rsv_launch_stats": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
                          ctypes.c_int),

@@ -366,16 +366,26 @@ template <typename T>
 struct DevBuf {
   T *p = nullptr;
   size_t count = 0;
+  bool owned = true;
   void alloc(size_t n) {
     release();
     if (n == 0) return;
     check(cudaMalloc(&p, n * sizeof(T)), "cudaMalloc");
     count = n;
+    owned = true;
+  }
+  // Non-owning view of caller-provided device memory (never freed here).
+  void view(T *ptr, size_t n) {
+    release();
+    p = ptr;
+    count = n;
+    owned = false;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p && owned) cudaFree(p);
     p = nullptr;
     count = 0;
+    owned = true;
   }
   ~DevBuf() { release(); }
 };
@@ -671,6 +681,105 @@ rsv_status guarded(F &&f) {
 bool configured = false;
 
 }  // namespace
+}  // namespace rsv
+
+namespace rsv {
+
+void set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
+
+// Energy and gradient of device parameters with every device buffer carved
+// out of a caller-provided workspace (nothing is allocated on the device).
+// Used by the allocation-free entry point (rsv_noalloc.cu).
+rsv_status run_in_workspace(int n, int L, double field, const double *d_params, size_t num_params,
+                            double *d_energy_out, double *d_gradient_out, void *workspace,
+                            size_t workspace_bytes, int max_qubits, int max_layers, void *stream) {
+  return guarded([&] {
+    if (n < 2) invalid("num_qubits must be at least 2.");
+    if (L < 1) invalid("num_layers must be at least 1.");
+    if (n > max_qubits || L > max_layers)
+      invalid("the allocation-free entry point supports num_qubits <= " + std::to_string(max_qubits) +
+              " and num_layers <= " + std::to_string(max_layers) + " (fixed workspace)");
+    if (num_params != static_cast<size_t>(2) * n * L) invalid("num_params does not match the circuit.");
+    if (d_params == nullptr || d_energy_out == nullptr) invalid("null device pointer");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    rsv_backend B;
+    B.n = n;
+    B.L = L;
+    B.field = field;
+    B.num_params = num_params;
+    check(cudaGetDevice(&B.device), "cudaGetDevice");
+    check(cudaDeviceGetAttribute(&B.sms, cudaDevAttrMultiProcessorCount, B.device), "cudaDeviceGetAttribute");
+    B.plan = make_plan(n, L, B.sms);
+    B.num_bwd_passes = static_cast<int>(B.plan.bwd.size());
+    B.state_len = size_t{1} << B.plan.phys;
+    B.energy_grid = static_cast<int>(std::min<u64>(std::max<u64>(1, (u64{1} << n) / 256),
+                                                   static_cast<u64>(B.sms) * 8));
+    const size_t nl = static_cast<size_t>(n) * L;
+    std::vector<int> tab;
+    for (const auto &s : B.plan.bwd) tab.push_back(s.grid);
+    tab.insert(tab.end(), B.plan.theta_pass.begin(), B.plan.theta_pass.end());
+    tab.insert(tab.end(), B.plan.theta_slot.begin(), B.plan.theta_slot.end());
+    tab.insert(tab.end(), B.plan.phi_pass.begin(), B.plan.phi_pass.end());
+    std::vector<int> ord;
+    for (const auto &s : B.plan.bwd) {
+      if (s.layer != L - 1) continue;
+      for (int g : {2, 1, 0, 3})
+        for (int j = 0; j < 3; ++j)
+          if (s.tile.gate_wire[3 * g + j] >= 0) ord.push_back(s.tile.gate_wire[3 * g + j]);
+    }
+    // carve the workspace (256-byte aligned sections)
+    unsigned char *base = static_cast<unsigned char *>(workspace);
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+      unsigned char *q = base + off;
+      off += (bytes + 255) & ~size_t{255};
+      return q;
+    };
+    unsigned char *bufs[3];
+    for (auto &q : bufs) q = take(B.state_len * sizeof(double2));
+    unsigned char *coef = take(nl * sizeof(double4));
+    unsigned char *rot = take(nl * sizeof(double2));
+    unsigned char *lscale = take(L * sizeof(double));
+    unsigned char *gscale = take(2 * nl * sizeof(double));
+    unsigned char *ptab = take(static_cast<size_t>(L) * 1024 * sizeof(double2));
+    unsigned char *prod = take(1024 * sizeof(double2));
+    unsigned char *epart = take(B.energy_grid * sizeof(double));
+    const size_t npart = static_cast<size_t>(std::max(1, B.num_bwd_passes)) * B.plan.max_grid * kPartialStride;
+    unsigned char *ppart = take(npart * sizeof(double));
+    unsigned char *tabs = take(tab.size() * sizeof(int));
+    unsigned char *ords = take(ord.size() * sizeof(int));
+    unsigned char *outs = take((1 + num_params) * sizeof(double));
+    if (off > workspace_bytes)
+      invalid("circuit needs " + std::to_string(off) + " workspace bytes, the fixed workspace has " +
+              std::to_string(workspace_bytes));
+    for (int i = 0; i < 3; ++i) B.buf[i].view(reinterpret_cast<double2 *>(bufs[i]), B.state_len);
+    B.coef.view(reinterpret_cast<double4 *>(coef), nl);
+    B.rot.view(reinterpret_cast<double2 *>(rot), nl);
+    B.lscale.view(reinterpret_cast<double *>(lscale), L);
+    B.gscale.view(reinterpret_cast<double *>(gscale), 2 * nl);
+    B.ptab.view(reinterpret_cast<double2 *>(ptab), static_cast<size_t>(L) * 1024);
+    B.prod.view(reinterpret_cast<double2 *>(prod), 1024);
+    B.energy_partials.view(reinterpret_cast<double *>(epart), B.energy_grid);
+    B.pass_partials.view(reinterpret_cast<double *>(ppart), npart);
+    B.tables.view(reinterpret_cast<int *>(tabs), tab.size());
+    B.order.view(reinterpret_cast<int *>(ords), ord.size());
+    B.outputs.view(reinterpret_cast<double *>(outs), 1 + num_params);
+    check(cudaMemcpyAsync(B.tables.p, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice, st),
+          "plan table upload");
+    check(cudaMemcpyAsync(B.order.p, ord.data(), ord.size() * sizeof(int), cudaMemcpyHostToDevice, st),
+          "order upload");
+    // The workspace keeps the previous call's contents; for n < 12 the padding
+    // amplitudes of the state buffers must start at zero.
+    if (B.plan.phys > n)
+      for (int i = 0; i < 3; ++i)
+        check(cudaMemsetAsync(B.buf[i].p, 0, B.state_len * sizeof(double2), st), "state clear");
+    check(launch_coef(d_params, B.coef.p, static_cast<int>(nl), st), "coef launch");
+    run_all(&B, d_gradient_out != nullptr, d_energy_out, d_gradient_out, st);
+    // the host vectors above are consumed by the time cudaMemcpyAsync from
+    // pageable memory returns; nothing else outlives this call
+  });
+}
+
 }  // namespace rsv
 
 using namespace rsv;

@@ -135,6 +135,31 @@ rsv_status rsv_benchmark_forward_graph(rsv_backend *backend, const double *param
                                        double *graph_ms_out);
 
 /*
+ * Allocation-free energy and gradient: the same computation as
+ * rsv_energy_and_grad_device for one circuit, for callers that cannot call
+ * cudaMalloc -- code whose device memory belongs to another allocator (a
+ * framework's caching pool or a fixed arena it must not fragment) or that
+ * runs where a device allocation and its implicit synchronisation are not
+ * allowed.  No backend object is created: every buffer lives in one fixed
+ * 8 MiB workspace inside this library's device image (held by every GPU that
+ * loads the library until the process exits), so the call issues no
+ * cudaMalloc, cudaFree or other allocating routine.  The caller passes device
+ * pointers: d_params f64[num_params], d_energy_out f64[1], d_gradient_out
+ * f64[num_params] (or NULL for energy only), and a stream used as given.
+ * Limits: num_qubits <= 16, num_layers <= 64; larger circuits return
+ * RSV_ERR_INVALID_ARGUMENT.  The first call on a device looks up the
+ * workspace address (cudaGetSymbolAddress) and should come before any stream
+ * capture.  All calls share the one workspace, which keeps the last call's
+ * contents: calls that overlap on the GPU (other streams, other host threads)
+ * race; serialise them.
+ * No counterpart in the reference.
+ */
+rsv_status rsv_energy_and_grad_noalloc(int num_qubits, int num_layers, double field,
+                                       const double *d_params, size_t num_params,
+                                       double *d_energy_out, double *d_gradient_out,
+                                       void *stream);
+
+/*
  * Per-launch timing over a measured region (for roofline reporting).
  * rsv_set_launch_timing(backend, 1) makes every following call record a CUDA
  * event pair around each of its kernel launches, on the launch stream;
