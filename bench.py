@@ -256,12 +256,12 @@ def main():
     achieved = d["bytes"] / (d["ms"] * 1e-3) / 1e9
     total_ms = sum(v["ms"] for v in kinds.values())
     traffic = None
-    tfile = ROOT / "profiles" / "traffic.json"
+    tfile = ROOT / "profiles" / "traffic_per_launch.md"
     if tfile.exists():
-        tdat = json.loads(tfile.read_text())
-        key = f"{dom}_n{n}"
-        if key in tdat:
-            traffic = tdat[key]["bytes_per_launch"]
+        for row in tfile.read_text().splitlines():
+            cells = [c.strip() for c in row.strip().strip("|").split("|")]
+            if len(cells) == 3 and cells[0] == dom and cells[1] == str(n):
+                traffic = float(cells[2])
     roofline = {
         "bound": "hbm", "kernel": f"pass_kernel ({dom})", "achieved": achieved, "peak": peak,
         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
