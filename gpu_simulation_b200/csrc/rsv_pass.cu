@@ -195,58 +195,82 @@ __device__ __forceinline__ void apply_phase_gray(double2 ph, const double2 (&rat
 
 // ======================================================================
 // Backward pass: 512 threads x 8 amplitudes of psi and lambda each.
-// Register groups of three tile bits: G0 = bits 0..2, G1 = 3..5, G2 = 6..8,
-// G3 = 9..11.  Layout Lk holds group G(3-k) in registers:
-//   L0: lanes -> bits 0..4,        warps -> 5..8,         registers -> 9..11
-//   L1: lanes -> bits 9,10,11,0,1, warps -> 2..5,         registers -> 6..8
-//   L2: lanes -> bits 6..10,       warps -> 11,0,1,2,     registers -> 3..5
-//   L3: lanes -> bits 3..7,        warps -> 8..11,        registers -> 0..2
+// Register groups of three tile bits; two layout families:
+//   family B (warps own tile bits 0..3):
+//     B0: lanes -> 4..8,        registers -> 9..11
+//     B1: lanes -> 9,10,11,4,5, registers -> 6..8
+//   family A (warps own tile bits 8..11):
+//     A1: lanes -> 3..7,        registers -> 0..2
+//     A2: lanes -> 0,1,2,6,7,   registers -> 3..5
+// Moving between the layouts of one family only permutes data inside a warp
+// (a warp-private slice of shared memory and __syncwarp); one CTA-wide
+// transpose per tile moves from family B to family A.  A tile is visited
+// B0 -> B1 -> (A1 ->) A2 and stored from A2, whose lanes 0..2 cover 128-byte
+// segments.
 // ======================================================================
 namespace bw {
 constexpr int kT = 512;
 constexpr int kR = 8;
 
-__device__ __forceinline__ int tpart(int L, int lane, int warp) {
-  if (L == 0) return lane | (warp << 5);
-  if (L == 1) return (lane >> 3) | (warp << 2) | ((lane & 7) << 9);
-  if (L == 2) return (warp >> 1) | (lane << 6) | ((warp & 1) << 11);
-  return (lane << 3) | (warp << 8);
+enum Layout { B0 = 0, B1 = 1, A1 = 2, A2 = 3 };
+
+// tile index of (lane, warp) with register 0, and the tile bit of register bit 0
+template <int LY>
+__device__ __forceinline__ int tpart(int lane, int warp) {
+  if (LY == B0) return warp | (lane << 4);
+  if (LY == B1) return warp | ((lane >> 3) << 4) | ((lane & 7) << 9);
+  if (LY == A1) return (lane << 3) | (warp << 8);
+  return (lane & 7) | ((lane >> 3) << 6) | (warp << 8);
 }
-__device__ __forceinline__ int rshift(int L) { return 9 - 3 * L; }
-__device__ __forceinline__ int lane_bit(int L, int j) {
-  if (L == 0) return j;
-  if (L == 1) return j < 3 ? 9 + j : j - 3;
-  if (L == 2) return 6 + j;
-  return 3 + j;
+template <int LY>
+__host__ __device__ constexpr int rbit() {
+  return LY == B0 ? 9 : LY == B1 ? 6 : LY == A1 ? 0 : 3;
 }
-__device__ __forceinline__ int warp_bit(int L, int j) {
-  if (L == 0) return 5 + j;
-  if (L == 1) return 2 + j;
-  if (L == 2) return j == 0 ? 11 : j - 1;
-  return 8 + j;
+// warp-local index (8 bits) of a tile index: family B keeps tile bits 4..11,
+// family A tile bits 0..7
+template <int LY>
+__device__ __forceinline__ int local(int t) {
+  return (LY == B0 || LY == B1) ? (t >> 4) : (t & 255);
+}
+__device__ __forceinline__ int sw8(int l) { return l ^ (((l >> 3) ^ (l >> 6)) & 7); }
+
+// layout FROM -> TO of the same family, through this warp's 256-entry slice
+template <int FROM, int TO>
+__device__ __forceinline__ void warp_transpose(double2 *wbuf, int lane, int warp, double2 (&a)[kR]) {
+  const int tf = tpart<FROM>(lane, warp), tt = tpart<TO>(lane, warp);
+#pragma unroll
+  for (int r = 0; r < kR; ++r) wbuf[sw8(local<FROM>(tf | (r << rbit<FROM>())))] = a[r];
+  __syncwarp();
+#pragma unroll
+  for (int r = 0; r < kR; ++r) a[r] = wbuf[sw8(local<TO>(tt | (r << rbit<TO>())))];
+  __syncwarp();
 }
 
-__device__ __forceinline__ void transpose(double2 *sm, int tp_from, int rb_from, int tp_to, int rb_to,
-                                          double2 (&a)[kR]) {
-#pragma unroll
-  for (int r = 0; r < kR; ++r) sm[swz(tp_from | (r << rb_from))] = a[r];
+// layout FROM -> TO through the CTA-wide buffer (whole tile).  The leading
+// barrier keeps a fast warp from overwriting a slow warp's private slice.
+template <int FROM, int TO>
+__device__ __forceinline__ void cta_transpose(double2 *sm, int lane, int warp, double2 (&a)[kR]) {
+  const int tf = tpart<FROM>(lane, warp), tt = tpart<TO>(lane, warp);
   __syncthreads();
 #pragma unroll
-  for (int r = 0; r < kR; ++r) a[r] = sm[swz(tp_to | (r << rb_to))];
+  for (int r = 0; r < kR; ++r) sm[swz(tf | (r << rbit<FROM>()))] = a[r];
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kR; ++r) a[r] = sm[swz(tt | (r << rbit<TO>()))];
   __syncthreads();
 }
 
-// Backward rotation of the three register bits of layout L (tile bits
+// Backward rotation of the three register bits of layout LY (tile bits
 // RB..RB+2): RY^dagger / f in tangent form, one FMA per component,
 //   mode +1: [[1,k],[-k,1]]    mode -1: [[k,1],[-1,k]],
 // preceded by the theta sum Re(conj(lam1) psi0) - Re(conj(lam0) psi1) of the
 // pair in the frame with the layer's RZ removed -- the reference's
 // 2 Re<lam_mid|dRY|psi_before> (cpp/ising_cuda_statevector_grad_kernels.cu:289-307)
 // simplified; the factors f still pending are corrected in the final reduction.
-template <int L>
+template <int LY>
 __device__ __forceinline__ void gates(const PassParams &P, double2 (&a)[kR], double2 (&b)[kR],
                                       double (&acc)[12]) {
-  constexpr int RB = 9 - 3 * L;
+  constexpr int RB = rbit<LY>();
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
     const int w = P.gate_wire[RB + j];
@@ -289,9 +313,10 @@ __device__ __forceinline__ void gates(const PassParams &P, double2 (&a)[kR], dou
   }
 }
 
-// phi-gradient sums of one tile in layout L: q = Im(conj(lam) psi) per
-// amplitude, folded into phi_sm[w] (sum of q with bit w set) and phi_sm[32].
-__device__ __forceinline__ void phi_sums(const PassParams &P, int L, u32 cbase, int lane, int warp,
+// phi-gradient sums of one tile in layout B0 (registers -> tile bits 9..11,
+// lanes -> 4..8, warps -> 0..3): q = Im(conj(lam) psi) per amplitude, folded
+// into phi_sm[w] (sum of q with bit w set) and phi_sm[32] (sum of q).
+__device__ __forceinline__ void phi_sums(const PassParams &P, u32 cbase, int lane, int warp,
                                          const double2 (&a)[kR], const double2 (&b)[kR],
                                          double (*red)[12], double *phi_sm) {
   double v[9];
@@ -320,24 +345,16 @@ __device__ __forceinline__ void phi_sums(const PassParams &P, int L, u32 cbase, 
     for (int ww = 0; ww < 16; ++ww) qt += red[ww][0];
     if (w < P.n) {
       const int tb = P.wire_tile_bit[w];
-      const int rb = rshift(L);
       double add = 0.0;
       if (tb < 0) {
         if ((cbase >> w) & 1) add = qt;  // coset bit: set for the whole tile
-      } else if (tb >= rb && tb < rb + 3) {
-        for (int ww = 0; ww < 16; ++ww) add += red[ww][1 + tb - rb];
+      } else if (tb >= 9) {
+        for (int ww = 0; ww < 16; ++ww) add += red[ww][1 + tb - 9];
+      } else if (tb >= 4) {
+        for (int ww = 0; ww < 16; ++ww) add += red[ww][4 + tb - 4];
       } else {
-        int lj = -1, wj = -1;
-        for (int j = 0; j < 5; ++j)
-          if (lane_bit(L, j) == tb) lj = j;
-        for (int j = 0; j < 4; ++j)
-          if (warp_bit(L, j) == tb) wj = j;
-        if (lj >= 0) {
-          for (int ww = 0; ww < 16; ++ww) add += red[ww][4 + lj];
-        } else if (wj >= 0) {
-          for (int ww = 0; ww < 16; ++ww)
-            if ((ww >> wj) & 1) add += red[ww][0];
-        }
+        for (int ww = 0; ww < 16; ++ww)
+          if ((ww >> tb) & 1) add += red[ww][0];
       }
       phi_sm[w] += add;
     }
@@ -348,7 +365,7 @@ __device__ __forceinline__ void phi_sums(const PassParams &P, int L, u32 cbase, 
 }  // namespace bw
 
 // Shared memory of the backward kernel (dynamic): staging psi | staging lam |
-// transpose buffer.
+// transpose buffer (CTA-wide, or 16 warp slices of 256 entries).
 constexpr size_t kBwdSmem = 3 * kTileSize * sizeof(double2);
 constexpr size_t kFwdSmem = kTileSize * sizeof(double2);
 
@@ -366,26 +383,26 @@ __global__ void __launch_bounds__(bw::kT, 1) bwd_pass_kernel(const PassParams P)
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int n = P.n;
+  double2 *wbuf = trans + warp * 256;
 
-  // groups with gates: G3 (bits 9..11, layout 0) .. G0 (bits 0..2, layout 3)
-  bool gv[4];
-#pragma unroll
-  for (int g = 0; g < 4; ++g)
-    gv[g] = P.gate_wire[3 * g] >= 0 || P.gate_wire[3 * g + 1] >= 0 || P.gate_wire[3 * g + 2] >= 0;
-  const int first = gv[2] ? 1 : (gv[1] ? 2 : (gv[0] ? 3 : 0));
+  // gates on tile bits 0..2 need the A1 visit
+  const bool has_lo = P.gate_wire[0] >= 0 || P.gate_wire[1] >= 0 || P.gate_wire[2] >= 0;
 
-  const int tp0 = tpart(0, lane, warp);
-  const u32 toff0 = thread_offset(P, tp0);
+  // global issue layout: lanes -> tile bits 0..4 (coalesced), warps -> 5..8, registers -> 9..11
+  const int tpi = lane | (warp << 5);
+  const u32 toffi = thread_offset(P, tpi);
   const u32 v9 = P.vec[9], v10 = P.vec[10], v11 = P.vec[11];
-  const int tpf = tpart(first, lane, warp);
-  const int rbf = rshift(first);
+  // store layout A2: registers -> tile bits 3..5
+  const int tps = tpart<A2>(lane, warp);
+  const u32 toffs = thread_offset(P, tps);
+  const u32 v3 = P.vec[3], v4 = P.vec[4], v5 = P.vec[5];
 
   double2 ratio[4];
-  u32 tofff = 0;
+  u32 toffp = 0;
   if (PHASE) {
-    tofff = thread_offset(P, tpf);
+    toffp = thread_offset(P, tpart<B0>(lane, warp));
 #pragma unroll
-    for (int j = 0; j < 3; ++j) ratio[j] = phase_ratio(P, unit_bit(P.vec[rbf + j]));
+    for (int j = 0; j < 3; ++j) ratio[j] = phase_ratio(P, unit_bit(P.vec[9 + j]));
     ratio[3] = make_double2(1.0, 0.0);
     if (threadIdx.x < 33) phi_sm[threadIdx.x] = 0.0;
   }
@@ -395,11 +412,11 @@ __global__ void __launch_bounds__(bw::kT, 1) bwd_pass_kernel(const PassParams P)
 
   const u32 num_tiles = static_cast<u32>(P.num_tiles);
   auto issue = [&](u32 tile) {
-    const u32 base = deposit(P, tile) ^ toff0;
+    const u32 base = deposit(P, tile) ^ toffi;
 #pragma unroll
     for (int r = 0; r < kR; ++r) {
       const u32 p = base ^ ((r & 1) ? v9 : 0u) ^ ((r & 2) ? v10 : 0u) ^ ((r & 4) ? v11 : 0u);
-      const int s = swz(tp0 | (r << 9));
+      const int s = swz(tpi | (r << 9));
       cp_async16(&stage_a[s], &P.psi_in[p]);
       cp_async16(&stage_b[s], &P.lam_in[source_index<LSRC>(p, n)]);
     }
@@ -407,13 +424,14 @@ __global__ void __launch_bounds__(bw::kT, 1) bwd_pass_kernel(const PassParams P)
   };
   if (blockIdx.x < num_tiles) issue(blockIdx.x);
 
+  const int tb0 = tpart<B0>(lane, warp);
   for (u32 tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
     cp_async_wait_all();
     __syncthreads();
     double2 a[kR], b[kR];
 #pragma unroll
     for (int r = 0; r < kR; ++r) {
-      const int s = swz(tpf | (r << rbf));
+      const int s = swz(tb0 | (r << 9));
       a[r] = stage_a[s];
       b[r] = stage_b[s];
     }
@@ -422,45 +440,35 @@ __global__ void __launch_bounds__(bw::kT, 1) bwd_pass_kernel(const PassParams P)
 
     const u32 cbase = deposit(P, tile);
     if (PHASE) {
-      // RZ^dagger of the layer on psi and lambda, then the phi sums.
-      const double2 ph = table4(P.ptab, cbase ^ tofff);
+      // RZ^dagger of the layer (with the layer's factor K) on psi and lambda,
+      // then the phi sums.
+      const double2 ph = table4(P.ptab, cbase ^ toffp);
       const double K = P.lscale[P.layer];
       apply_phase_gray<3, true, true>(make_double2(K * ph.x, K * ph.y), ratio, a, b);
-      phi_sums(P, first, cbase, lane, warp, a, b, red, phi_sm);
+      phi_sums(P, cbase, lane, warp, a, b, red, phi_sm);
     }
 
-    int cur = first;
-    if (gv[2]) {
-      gates<1>(P, a, b, acc);
-      cur = 1;
+    gates<B0>(P, a, b, acc);
+    warp_transpose<B0, B1>(wbuf, lane, warp, a);
+    warp_transpose<B0, B1>(wbuf, lane, warp, b);
+    gates<B1>(P, a, b, acc);
+    if (has_lo) {
+      cta_transpose<B1, A1>(trans, lane, warp, a);
+      cta_transpose<B1, A1>(trans, lane, warp, b);
+      gates<A1>(P, a, b, acc);
+      warp_transpose<A1, A2>(wbuf, lane, warp, a);
+      warp_transpose<A1, A2>(wbuf, lane, warp, b);
+    } else {
+      cta_transpose<B1, A2>(trans, lane, warp, a);
+      cta_transpose<B1, A2>(trans, lane, warp, b);
     }
-    if (gv[1]) {
-      if (cur != 2) {
-        transpose(trans, tpart(cur, lane, warp), rshift(cur), tpart(2, lane, warp), 3, a);
-        transpose(trans, tpart(cur, lane, warp), rshift(cur), tpart(2, lane, warp), 3, b);
-      }
-      gates<2>(P, a, b, acc);
-      cur = 2;
-    }
-    if (gv[0]) {
-      if (cur != 3) {
-        transpose(trans, tpart(cur, lane, warp), rshift(cur), tpart(3, lane, warp), 0, a);
-        transpose(trans, tpart(cur, lane, warp), rshift(cur), tpart(3, lane, warp), 0, b);
-      }
-      gates<3>(P, a, b, acc);
-      cur = 3;
-    }
-    if (cur != 0) {
-      transpose(trans, tpart(cur, lane, warp), rshift(cur), tp0, 9, a);
-      transpose(trans, tpart(cur, lane, warp), rshift(cur), tp0, 9, b);
-    }
-    if (gv[3]) gates<0>(P, a, b, acc);
+    gates<A2>(P, a, b, acc);
 
     if (PDST != kStoreNone || LDST != kStoreNone) {
-      const u32 base = cbase ^ toff0;
+      const u32 base = cbase ^ toffs;
 #pragma unroll
       for (int r = 0; r < kR; ++r) {
-        const u32 p = base ^ ((r & 1) ? v9 : 0u) ^ ((r & 2) ? v10 : 0u) ^ ((r & 4) ? v11 : 0u);
+        const u32 p = base ^ ((r & 1) ? v3 : 0u) ^ ((r & 2) ? v4 : 0u) ^ ((r & 4) ? v5 : 0u);
         store_amp<PDST>(P.psi_out, p, n, a[r]);
         store_amp<LDST>(P.lam_out, p, n, b[r]);
       }
