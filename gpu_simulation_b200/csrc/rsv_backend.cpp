@@ -295,6 +295,24 @@ Plan make_plan(int n, int L, int sms) {
   return pl;
 }
 
+// Undo order of the wires within one backward layer, as the backward pass
+// kernel visits them: passes in plan order; inside a pass the register groups
+// of tile bits 9..11, 6..8, 0..2, then 3..5 (layouts B0, B1, A1, A2 of
+// rsv_pass.cu).  Needed for the exact tangent-form gradient correction.
+std::vector<int> undo_order(const Plan &pl) {
+  std::vector<int> ord;
+  for (const auto &s : pl.bwd) {
+    if (s.layer != pl.L - 1) continue;
+    for (int g : {3, 2, 0, 1})
+      for (int j = 0; j < 3; ++j) {
+        const int w = s.tile.gate_wire[3 * g + j];
+        if (w >= 0) ord.push_back(w);
+      }
+  }
+  if (static_cast<int>(ord.size()) != pl.n) throw Error(RSV_ERR_INTERNAL, "undo order incomplete");
+  return ord;
+}
+
 const char *load_name(int m) {
   switch (m) {
     case kLoadNatural: return "load";
@@ -720,13 +738,7 @@ rsv_status run_in_workspace(int n, int L, double field, const double *d_params, 
     tab.insert(tab.end(), B.plan.theta_pass.begin(), B.plan.theta_pass.end());
     tab.insert(tab.end(), B.plan.theta_slot.begin(), B.plan.theta_slot.end());
     tab.insert(tab.end(), B.plan.phi_pass.begin(), B.plan.phi_pass.end());
-    std::vector<int> ord;
-    for (const auto &s : B.plan.bwd) {
-      if (s.layer != L - 1) continue;
-      for (int g : {2, 1, 0, 3})
-        for (int j = 0; j < 3; ++j)
-          if (s.tile.gate_wire[3 * g + j] >= 0) ord.push_back(s.tile.gate_wire[3 * g + j]);
-    }
+    const std::vector<int> ord = undo_order(B.plan);
     // carve the workspace (256-byte aligned sections)
     unsigned char *base = static_cast<unsigned char *>(workspace);
     size_t off = 0;
@@ -878,20 +890,7 @@ rsv_status rsv_create(int num_qubits, int num_layers, double field, const char *
     B->lscale.alloc(num_layers);
     B->gscale.alloc(2 * nl);
     {
-      // Undo order of the wires within one backward layer, as the backward
-      // pass kernel visits them: passes in plan order; inside a pass the
-      // register groups of tile bits 6..8, 3..5, 0..2, then 9..11.
-      std::vector<int> ord;
-      const int L1 = num_layers - 1;
-      for (const auto &s : B->plan.bwd) {
-        if (s.layer != L1) continue;
-        for (int g : {2, 1, 0, 3})
-          for (int j = 0; j < 3; ++j) {
-            const int w = s.tile.gate_wire[3 * g + j];
-            if (w >= 0) ord.push_back(w);
-          }
-      }
-      if (static_cast<int>(ord.size()) != num_qubits) throw Error(RSV_ERR_INTERNAL, "undo order incomplete");
+      const std::vector<int> ord = undo_order(B->plan);
       B->order.alloc(ord.size());
       check(cudaMemcpy(B->order.p, ord.data(), ord.size() * sizeof(int), cudaMemcpyHostToDevice),
             "order upload");
