@@ -7,6 +7,7 @@ Public surface
   * ``ring_ising_energy`` / ``RingIsingEnergy``
                                     torch.autograd.Function (backward = adjoint kernels)
   * ``describe_plan``               launch schedule of one call (host only)
+  * ``BatchEngine``                 thousands of independent circuits per kernel launch
 
 The compiled pieces are built in-tree by ``python -m gpu_simulation_b200.build``.
 """
@@ -14,9 +15,11 @@ The compiled pieces are built in-tree by ``python -m gpu_simulation_b200.build``
 from __future__ import annotations
 
 from .backend import RingIsingAdjointBackend, StandaloneBackendConfig
+from .batch import BatchEngine
 from .engine import Engine, describe_plan
 
 __all__ = [
+    "BatchEngine",
     "Engine",
     "RingIsingAdjointBackend",
     "RingIsingEnergy",

@@ -44,11 +44,24 @@ _SIGNATURES = {
     "rsv_set_launch_timing": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "rsv_launch_stats": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
                          ctypes.c_int),
+    "rsv_set_field": ([ctypes.c_void_p, ctypes.c_double], ctypes.c_int),
     "rsv_backend_info": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                           ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
     "rsv_describe_plan": ([ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t,
                            ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
     "rsv_ring_map": ([ctypes.c_ulonglong, ctypes.c_int, ctypes.c_int], ctypes.c_ulonglong),
+    "rsv_batch_create": ([ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "rsv_batch_destroy": ([ctypes.c_void_p], ctypes.c_int),
+    "rsv_batch_set_circuits": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.c_void_p], ctypes.c_int),
+    "rsv_batch_info": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_size_t),
+                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
+    "rsv_batch_set_active_slots": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "rsv_batch_run_device": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                              ctypes.c_void_p], ctypes.c_int),
+    "rsv_batch_energy_and_grad": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
+                                   ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
 }
 
 _lib = None

@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/rsv.h"
+#include "rsv_batch.h"
 #include "rsv_device.cuh"
 #include "rsv_launch.h"
 #include "rsv_types.h"
@@ -698,6 +699,192 @@ rsv_status guarded(F &&f) {
 
 bool configured = false;
 
+// ------------------------------------------------------------------------
+// Batched circuits: the pass plans of make_plan, flattened into the tables
+// the persistent batch kernel (rsv_batch.cu) walks.
+// ------------------------------------------------------------------------
+
+BatchTile batch_tile(const Tile &t) {
+  BatchTile b{};
+  for (int i = 0; i < 12; ++i) {
+    b.vec[i] = static_cast<unsigned int>(t.vec[i]);
+    b.gate_wire[i] = t.gate_wire[i];
+  }
+  for (int w = 0; w < 32; ++w) b.wire_tile_bit[w] = -1;
+  if (t.unit)
+    for (int i = 0; i < 12; ++i) {
+      int bit = 0;
+      while (!((t.vec[i] >> bit) & 1)) ++bit;
+      b.wire_tile_bit[bit] = i;
+    }
+  b.num_runs = t.num_runs;
+  for (int r = 0; r < 4; ++r) {
+    b.run_start[r] = t.run_start[r];
+    b.run_len[r] = t.run_len[r];
+  }
+  b.num_tiles = static_cast<unsigned int>(t.num_tiles);
+  return b;
+}
+
+BatchStep batch_step(const Step &s, int kind, int tile) {
+  BatchStep b{};
+  b.kind = kind;
+  b.tile = tile;
+  b.layer = s.layer;
+  b.psi_load = s.psi_load;
+  b.lam_load = s.lam_load;
+  b.psi_store = s.psi_store;
+  b.lam_store = s.lam_store;
+  b.phase = s.phase;
+  b.psi_in = s.psi_in;
+  b.psi_out = s.psi_out;
+  b.lam_in = s.lam_in;
+  b.lam_out = s.lam_out;
+  return b;
+}
+
+}  // namespace
+}  // namespace rsv
+
+struct rsv_batch {
+  int device = 0, sms = 0;
+  int max_qubits = 0;
+  int slots = 0, active_slots = 0;
+  size_t state_bytes = 0, slot_bytes = 0;
+  rsv::DevBuf<unsigned char> scratch;
+  // plan tables (grow as new (n, L) pairs appear; uploaded when dirty)
+  std::vector<std::pair<int, int>> plan_keys;
+  std::vector<rsv::BatchPlan> plans;
+  std::vector<rsv::BatchStep> steps;
+  std::vector<rsv::BatchTile> tiles;
+  std::vector<int> undo;
+  std::vector<double> plan_cost;
+  bool dirty = true;
+  rsv::DevBuf<rsv::BatchPlan> d_plans;
+  rsv::DevBuf<rsv::BatchStep> d_steps;
+  rsv::DevBuf<rsv::BatchTile> d_tiles;
+  rsv::DevBuf<int> d_undo;
+  // current circuits
+  int count = 0;
+  size_t num_params = 0;
+  rsv::DevBuf<rsv::BatchCircuit> d_circuits;
+  rsv::DevBuf<int> d_order;
+  rsv::DevBuf<int> d_counter;
+  cudaStream_t stream = nullptr;
+};
+
+namespace rsv {
+namespace {
+
+int batch_plan_index(rsv_batch *Bt, int n, int L) {
+  for (size_t i = 0; i < Bt->plan_keys.size(); ++i)
+    if (Bt->plan_keys[i] == std::make_pair(n, L)) return static_cast<int>(i);
+  const Plan pl = make_plan(n, L, Bt->sms);
+  BatchPlan bp{};
+  bp.first_step = static_cast<int>(Bt->steps.size());
+  bp.undo_off = static_cast<int>(Bt->undo.size());
+  double cost = 0.0;
+  auto add = [&](const Step &s, int kind) {
+    Bt->tiles.push_back(batch_tile(s.tile));
+    Bt->steps.push_back(batch_step(s, kind, static_cast<int>(Bt->tiles.size()) - 1));
+    cost += static_cast<double>(s.tile.num_tiles) * (kind == kBatchBackward ? 2.0 : 1.0);
+  };
+  for (const auto &s : pl.fwd) add(s, kBatchForward);
+  BatchStep e{};
+  e.kind = kBatchEnergy;
+  e.tile = -1;
+  e.psi_in = pl.chi_buf;
+  e.psi_out = pl.mu_buf;
+  e.lam_in = e.lam_out = -1;
+  Bt->steps.push_back(e);
+  cost += 1.0;
+  for (const auto &s : pl.bwd) add(s, kBatchBackward);
+  bp.num_steps = static_cast<int>(Bt->steps.size()) - bp.first_step;
+  for (int w : undo_order(pl)) Bt->undo.push_back(w);
+  Bt->plans.push_back(bp);
+  Bt->plan_keys.emplace_back(n, L);
+  Bt->plan_cost.push_back(cost);
+  Bt->dirty = true;
+  return static_cast<int>(Bt->plans.size()) - 1;
+}
+
+template <typename T>
+void upload(DevBuf<T> &d, const std::vector<T> &h, cudaStream_t st, const char *what) {
+  if (d.count < h.size()) d.alloc(h.size() + h.size() / 2 + 1);
+  if (!h.empty())
+    check(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st), what);
+}
+
+void batch_set_circuits(rsv_batch *Bt, int count, const int *ns, const int *Ls, const double *hs) {
+  if (count < 0) invalid("count must be non-negative");
+  if (count > 0 && (ns == nullptr || Ls == nullptr || hs == nullptr)) invalid("null circuit array");
+  std::vector<BatchCircuit> circ(static_cast<size_t>(count));
+  std::vector<double> cost(static_cast<size_t>(count));
+  size_t off = 0;
+  for (int c = 0; c < count; ++c) {
+    const int n = ns[c], L = Ls[c];
+    if (n < 2 || n > Bt->max_qubits)
+      invalid("circuit " + std::to_string(c) + ": num_qubits must be in [2, " +
+              std::to_string(Bt->max_qubits) + "]");
+    if (L < 1 || L > kBatchMaxLayers)
+      invalid("circuit " + std::to_string(c) + ": num_layers must be in [1, " +
+              std::to_string(kBatchMaxLayers) + "]");
+    if (!std::isfinite(hs[c])) invalid("circuit " + std::to_string(c) + ": field is not finite");
+    BatchCircuit &C = circ[static_cast<size_t>(c)];
+    C.n = n;
+    C.L = L;
+    C.h = hs[c];
+    C.param_off = static_cast<long long>(off);
+    C.plan = batch_plan_index(Bt, n, L);
+    C.index = c;
+    cost[static_cast<size_t>(c)] =
+        Bt->plan_cost[static_cast<size_t>(C.plan)] * static_cast<double>(u64{1} << std::max(n, kTileBits));
+    off += static_cast<size_t>(2) * n * L;
+  }
+  // Longest first (LPT): the persistent CTAs take circuits in this order.
+  std::vector<int> order(static_cast<size_t>(count));
+  for (int c = 0; c < count; ++c) order[static_cast<size_t>(c)] = c;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return cost[static_cast<size_t>(a)] > cost[static_cast<size_t>(b)];
+  });
+  cudaStream_t st = Bt->stream;
+  if (Bt->dirty) {
+    upload(Bt->d_plans, Bt->plans, st, "batch plan upload");
+    upload(Bt->d_steps, Bt->steps, st, "batch step upload");
+    upload(Bt->d_tiles, Bt->tiles, st, "batch tile upload");
+    upload(Bt->d_undo, Bt->undo, st, "batch undo upload");
+    Bt->dirty = false;
+  }
+  upload(Bt->d_circuits, circ, st, "batch circuit upload");
+  upload(Bt->d_order, order, st, "batch order upload");
+  check(cudaStreamSynchronize(st), "batch upload");
+  Bt->count = count;
+  Bt->num_params = off;
+}
+
+void batch_run(rsv_batch *Bt, const double *d_params, double *d_energy, double *d_grad,
+               cudaStream_t st) {
+  if (Bt->count == 0) return;
+  if (d_params == nullptr || d_energy == nullptr) invalid("null device pointer");
+  BatchArgs A{};
+  A.count = Bt->count;
+  A.circuits = Bt->d_circuits.p;
+  A.order = Bt->d_order.p;
+  A.counter = Bt->d_counter.p;
+  A.plans = Bt->d_plans.p;
+  A.steps = Bt->d_steps.p;
+  A.tiles = Bt->d_tiles.p;
+  A.undo = Bt->d_undo.p;
+  A.params = d_params;
+  A.energy_out = d_energy;
+  A.grad_out = d_grad;
+  A.scratch = Bt->scratch.p;
+  A.slot_bytes = Bt->slot_bytes;
+  A.state_bytes = Bt->state_bytes;
+  check(cudaMemsetAsync(Bt->d_counter.p, 0, sizeof(int), st), "batch counter reset");
+  check(launch_batch(A, std::min(Bt->count, Bt->active_slots), st), "batch launch");
+}
+
 }  // namespace
 }  // namespace rsv
 
@@ -1113,6 +1300,14 @@ rsv_status rsv_launch_stats(rsv_backend *B, int *counts, double *total_ms, doubl
   });
 }
 
+rsv_status rsv_set_field(rsv_backend *B, double field) {
+  return guarded([&] {
+    if (B == nullptr) invalid("backend is null");
+    if (!std::isfinite(field)) invalid("field is not finite");
+    B->field = field;
+  });
+}
+
 rsv_status rsv_backend_info(rsv_backend *B, int *num_qubits, int *num_layers, size_t *num_params,
                             size_t *device_bytes) {
   return guarded([&] {
@@ -1123,6 +1318,105 @@ rsv_status rsv_backend_info(rsv_backend *B, int *num_qubits, int *num_layers, si
     if (device_bytes)
       *device_bytes = 3 * B->state_len * sizeof(double2) + B->pass_partials.count * sizeof(double) +
                       B->energy_partials.count * sizeof(double);
+  });
+}
+
+rsv_status rsv_batch_create(int max_qubits, int slots, rsv_batch **out) {
+  return guarded([&] {
+    if (out == nullptr) invalid("out is null");
+    *out = nullptr;
+    if (max_qubits < 2 || max_qubits > kBatchMaxQubits)
+      invalid("max_qubits must be in [2, " + std::to_string(kBatchMaxQubits) + "]");
+    if (slots < 0) invalid("slots must be non-negative");
+    auto Bt = std::make_unique<rsv_batch>();
+    check(cudaGetDevice(&Bt->device), "cudaGetDevice");
+    check(cudaDeviceGetAttribute(&Bt->sms, cudaDevAttrMultiProcessorCount, Bt->device),
+          "cudaDeviceGetAttribute");
+    check(configure_batch_kernel(), "configure batch kernel");
+    Bt->max_qubits = max_qubits;
+    Bt->slots = slots > 0 ? slots : Bt->sms;
+    Bt->active_slots = Bt->slots;
+    Bt->state_bytes = sizeof(double2) << std::max(max_qubits, kTileBits);
+    Bt->slot_bytes = (3 * Bt->state_bytes + batch_slot_table_bytes() + 255) & ~size_t{255};
+    Bt->scratch.alloc(Bt->slot_bytes * static_cast<size_t>(Bt->slots));
+    Bt->d_counter.alloc(1);
+    check(cudaStreamCreateWithFlags(&Bt->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    *out = Bt.release();
+  });
+}
+
+rsv_status rsv_batch_destroy(rsv_batch *batch) {
+  return guarded([&] {
+    if (batch == nullptr) return;
+    cudaStreamSynchronize(batch->stream);
+    cudaStreamDestroy(batch->stream);
+    delete batch;
+  });
+}
+
+rsv_status rsv_batch_set_circuits(rsv_batch *batch, int count, const int *num_qubits,
+                                  const int *num_layers, const double *fields) {
+  return guarded([&] {
+    if (batch == nullptr) invalid("batch is null");
+    batch_set_circuits(batch, count, num_qubits, num_layers, fields);
+  });
+}
+
+rsv_status rsv_batch_info(rsv_batch *batch, int *count, size_t *num_params, int *slots,
+                          size_t *device_bytes) {
+  return guarded([&] {
+    if (batch == nullptr) invalid("batch is null");
+    if (count) *count = batch->count;
+    if (num_params) *num_params = batch->num_params;
+    if (slots) *slots = batch->active_slots;
+    if (device_bytes) *device_bytes = batch->slot_bytes * static_cast<size_t>(batch->slots);
+  });
+}
+
+rsv_status rsv_batch_set_active_slots(rsv_batch *batch, int slots) {
+  return guarded([&] {
+    if (batch == nullptr) invalid("batch is null");
+    if (slots < 1 || slots > batch->slots)
+      invalid("slots must be in [1, " + std::to_string(batch->slots) + "]");
+    batch->active_slots = slots;
+  });
+}
+
+rsv_status rsv_batch_run_device(rsv_batch *batch, const double *d_params, double *d_energy_out,
+                                double *d_gradient_out, void *stream) {
+  return guarded([&] {
+    if (batch == nullptr) invalid("batch is null");
+    batch_run(batch, d_params, d_energy_out, d_gradient_out, static_cast<cudaStream_t>(stream));
+  });
+}
+
+rsv_status rsv_batch_energy_and_grad(rsv_batch *batch, int count, const int *num_qubits,
+                                     const int *num_layers, const double *fields,
+                                     const double *params, size_t num_params,
+                                     double *energy_out, double *gradient_out, void *stream) {
+  return guarded([&] {
+    if (batch == nullptr) invalid("batch is null");
+    batch_set_circuits(batch, count, num_qubits, num_layers, fields);
+    if (num_params != batch->num_params)
+      invalid("num_params does not match the circuits (" + std::to_string(batch->num_params) +
+              " expected)");
+    if (count == 0) return;
+    if (params == nullptr || energy_out == nullptr) invalid("null host pointer");
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : batch->stream;
+    DevBuf<double> d_params, d_out;
+    d_params.alloc(num_params);
+    d_out.alloc(static_cast<size_t>(count) + (gradient_out ? num_params : 0));
+    check(cudaMemcpyAsync(d_params.p, params, num_params * sizeof(double), cudaMemcpyHostToDevice, st),
+          "params upload");
+    batch_run(batch, d_params.p, d_out.p, gradient_out ? d_out.p + count : nullptr, st);
+    check(cudaMemcpyAsync(energy_out, d_out.p, static_cast<size_t>(count) * sizeof(double),
+                          cudaMemcpyDeviceToHost, st),
+          "energy download");
+    if (gradient_out)
+      check(cudaMemcpyAsync(gradient_out, d_out.p + count, num_params * sizeof(double),
+                            cudaMemcpyDeviceToHost, st),
+            "gradient download");
+    check(cudaStreamSynchronize(st), "batch synchronize");
   });
 }
 

@@ -1,0 +1,415 @@
+// Batched energy and gradient of many independent ring-Ising circuits in one
+// persistent kernel launch (uneven qubit counts and depths).
+//
+// The reference has no batched mode (it is only proposed in its design notes,
+// SURVEY 2.5); this kernel runs thousands of circuits per launch:
+//   * one CTA (512 threads) per circuit at a time; CTAs take circuits from an
+//     atomic work counter over a list sorted by decreasing cost;
+//   * every circuit runs the same pass plan the single-circuit engine uses for
+//     its (n, L) (built on the host, uploaded once), tile by tile on the
+//     CTA's own scratch slot, which stays in L2 for small circuits;
+//   * a tile is 4096 amplitudes, 8 per thread, in the layout families of the
+//     backward pass kernel (rsv_tile.cuh); the next tile of the same pass is
+//     prefetched with cp.async;
+//   * the circuit's coefficient, tangent-form and RZ-phase tables are built
+//     by the CTA itself; gradient sums are reduced on chip and written once
+//     per circuit, so no cross-CTA reduction is needed and results are
+//     deterministic.
+#include "rsv_batch.h"
+
+// the per-circuit tables are written by this kernel, in the slot it reuses
+#define RSV_TABLES_WRITTEN_IN_KERNEL 1
+#include "rsv_tile.cuh"
+
+namespace rsv {
+namespace {
+
+using namespace bw;
+
+constexpr int kBatchThreads = bw::kT;
+
+// Forward rotation of the three register bits of layout LY: RY / f in
+// tangent form (mode +1: [[1,-k],[k,1]], mode -1: [[k,-1],[1,k]]).
+template <int LY>
+__device__ __forceinline__ void fgates(const PassParams &P, double2 (&a)[kR]) {
+  constexpr int RB = rbit<LY>();
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const int w = P.gate_wire[RB + j];
+    if (w < 0) continue;
+    const double2 km = P.rot[P.layer * P.n + w];
+    const double k = km.x;
+    if (km.y > 0.0) {
+#pragma unroll
+      for (int r = 0; r < kR; ++r) {
+        if (r & (1 << j)) continue;
+        const int r1 = r | (1 << j);
+        const double2 x0 = a[r], x1 = a[r1];
+        a[r] = make_double2(fma(-k, x1.x, x0.x), fma(-k, x1.y, x0.y));
+        a[r1] = make_double2(fma(k, x0.x, x1.x), fma(k, x0.y, x1.y));
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < kR; ++r) {
+        if (r & (1 << j)) continue;
+        const int r1 = r | (1 << j);
+        const double2 x0 = a[r], x1 = a[r1];
+        a[r] = make_double2(fma(k, x0.x, -x1.x), fma(k, x0.y, -x1.y));
+        a[r1] = make_double2(fma(k, x1.x, x0.x), fma(k, x1.y, x0.y));
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ double2 load_src(int mode, const double2 *buf, u32 p, int n,
+                                            const double2 *prod) {
+  if (mode == kLoadNatural) return buf[p];
+  if (mode == kLoadGatherP) return buf[static_cast<u32>(ring_p(p, n))];
+  if (mode == kLoadProduct) return table4(prod, static_cast<u32>(ring_pinv(p, n)));
+  return table4(prod, p);
+}
+
+__device__ __forceinline__ void store_dst(int mode, double2 *buf, u32 p, int n, double2 v) {
+  if (mode == kStoreNatural) buf[p] = v;
+  else if (mode == kStoreScatterP) buf[static_cast<u32>(ring_p(p, n))] = v;
+  else if (mode == kStoreScatterPinv) buf[static_cast<u32>(ring_pinv(p, n))] = v;
+}
+
+struct Shared {
+  PassParams P;  // the current pass (uniform over the CTA; kept off the thread stacks)
+  double2 stage_a[kTileSize];
+  double2 stage_b[kTileSize];
+  double2 trans[kTileSize];
+  double red[16][12];
+  double phi_sm[33];
+  double theta[kBatchMaxLayers * kBatchMaxQubits];
+  double phi_b[kBatchMaxLayers * kBatchMaxQubits];
+  double phi_tot[kBatchMaxLayers];
+  double energy;
+  int next;
+};
+
+// One pass (forward or backward) of one circuit, all of its tiles.
+template <bool BWD>
+__device__ void run_pass(const PassParams &P, Shared &S, int lane, int warp, double (&acc)[12]) {
+  const int n = P.n;
+  double2 *wbuf = S.trans + warp * 256;
+  const bool has_lo = P.gate_wire[0] >= 0 || P.gate_wire[1] >= 0 || P.gate_wire[2] >= 0;
+  const bool staged = P.psi_load == kLoadNatural || P.psi_load == kLoadGatherP;
+  const int tpi = lane | (warp << 5);
+  const u32 toffi = thread_offset(P, tpi);
+  const u32 v9 = P.vec[9], v10 = P.vec[10], v11 = P.vec[11];
+  const int tb0 = tpart<B0>(lane, warp);
+  const u32 toffb0 = thread_offset(P, tb0);
+  const int tps = tpart<A2>(lane, warp);
+  const u32 toffs = thread_offset(P, tps);
+  const u32 v3 = P.vec[3], v4 = P.vec[4], v5 = P.vec[5];
+  const u32 num_tiles = static_cast<u32>(P.num_tiles);
+
+  double2 ratio[4];
+  if (P.phase) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) ratio[j] = phase_ratio(P, unit_bit(BWD ? P.vec[9 + j] : P.vec[3 + j]));
+    ratio[3] = make_double2(1.0, 0.0);
+  }
+  if (BWD && P.phi_grad && threadIdx.x < 33) S.phi_sm[threadIdx.x] = 0.0;
+
+  auto issue = [&](u32 tile) {
+    const u32 base = deposit(P, tile) ^ toffi;
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+      const u32 p = base ^ ((r & 1) ? v9 : 0u) ^ ((r & 2) ? v10 : 0u) ^ ((r & 4) ? v11 : 0u);
+      const int s = swz(tpi | (r << 9));
+      const u32 ps = P.psi_load == kLoadGatherP ? static_cast<u32>(ring_p(p, n)) : p;
+      cp_async16(&S.stage_a[s], &P.psi_in[ps]);
+      if (BWD) {
+        const u32 ls = P.lam_load == kLoadGatherP ? static_cast<u32>(ring_p(p, n)) : p;
+        cp_async16(&S.stage_b[s], &P.lam_in[ls]);
+      }
+    }
+    cp_async_commit();
+  };
+  if (staged) issue(0);
+
+  for (u32 tile = 0; tile < num_tiles; ++tile) {
+    const u32 cbase = deposit(P, tile);
+    double2 a[kR], b[kR];
+    if (staged) {
+      cp_async_wait_all();
+      __syncthreads();
+#pragma unroll
+      for (int r = 0; r < kR; ++r) {
+        const int s = swz(tb0 | (r << 9));
+        a[r] = S.stage_a[s];
+        if (BWD) b[r] = S.stage_b[s];
+      }
+      __syncthreads();
+      if (tile + 1 < num_tiles) issue(tile + 1);
+    } else {
+      const u32 base = cbase ^ toffb0;
+#pragma unroll
+      for (int r = 0; r < kR; ++r) {
+        const u32 p = base ^ ((r & 1) ? v9 : 0u) ^ ((r & 2) ? v10 : 0u) ^ ((r & 4) ? v11 : 0u);
+        a[r] = load_src(P.psi_load, P.psi_in, p, n, P.prod);
+      }
+    }
+    if (BWD && P.phase) {
+      const double2 ph = table4(P.ptab, cbase ^ toffb0);
+      const double K = P.lscale[P.layer];
+      apply_phase_gray<3, true, true>(make_double2(K * ph.x, K * ph.y), ratio, a, b);
+      phi_sums(P, cbase, lane, warp, a, b, S.red, S.phi_sm);
+    }
+
+    if (BWD) gates<B0>(P, a, b, acc); else fgates<B0>(P, a);
+    warp_transpose<B0, B1>(wbuf, lane, warp, a);
+    if (BWD) warp_transpose<B0, B1>(wbuf, lane, warp, b);
+    if (BWD) gates<B1>(P, a, b, acc); else fgates<B1>(P, a);
+    if (has_lo) {
+      cta_transpose<B1, A1>(S.trans, lane, warp, a);
+      if (BWD) cta_transpose<B1, A1>(S.trans, lane, warp, b);
+      if (BWD) gates<A1>(P, a, b, acc); else fgates<A1>(P, a);
+      warp_transpose<A1, A2>(wbuf, lane, warp, a);
+      if (BWD) warp_transpose<A1, A2>(wbuf, lane, warp, b);
+    } else {
+      cta_transpose<B1, A2>(S.trans, lane, warp, a);
+      if (BWD) cta_transpose<B1, A2>(S.trans, lane, warp, b);
+    }
+    if (BWD) gates<A2>(P, a, b, acc); else fgates<A2>(P, a);
+
+    const u32 base = cbase ^ toffs;
+    if (!BWD && P.phase) {
+      const double2 ph = table4(P.ptab, base);
+      const double K = P.lscale[P.layer];
+      apply_phase_gray<3, false, false>(make_double2(K * ph.x, K * ph.y), ratio, a, b);
+    }
+    // single-tile in-place permutation: every load of the tile precedes every store
+    if (P.sync_after_load) __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+      const u32 p = base ^ ((r & 1) ? v3 : 0u) ^ ((r & 2) ? v4 : 0u) ^ ((r & 4) ? v5 : 0u);
+      store_dst(P.psi_store, P.psi_out, p, n, a[r]);
+      if (BWD) store_dst(P.lam_store, P.lam_out, p, n, b[r]);
+    }
+  }
+  __syncthreads();  // the pass's global writes are visible to the next pass
+}
+
+// lambda = P^T H P chi and the energy, one CTA (rsv_kernels.cu energy_kernel).
+__device__ double run_energy(const double2 *chi, double2 *mu, int n, double field, Shared &S) {
+  u64 masks[kBatchMaxQubits];
+#pragma unroll
+  for (int w = 0; w < kBatchMaxQubits; ++w) masks[w] = (w < n) ? ring_pinv(u64{1} << w, n) : 0;
+  double e = 0.0;
+  const u32 size = 1u << n;
+  for (u32 i = threadIdx.x; i < size; i += blockDim.x) {
+    const double2 c = chi[i];
+    const double d = diag_after_ring(i, n);
+    double2 x = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int w = 0; w < kBatchMaxQubits; ++w) {
+      if (w < n) {
+        const double2 t = chi[i ^ static_cast<u32>(masks[w])];
+        x.x += t.x;
+        x.y += t.y;
+      }
+    }
+    const double2 m = make_double2(fma(d, c.x, -field * x.x), fma(d, c.y, -field * x.y));
+    mu[i] = m;
+    e += fma(c.x, m.x, c.y * m.y);
+  }
+  e = warp_sum(e);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) S.red[warp][0] = e;
+  __syncthreads();
+  double s = 0.0;
+  for (int ww = 0; ww < 16; ++ww) s += S.red[ww][0];
+  __syncthreads();
+  return s;
+}
+
+__global__ void __launch_bounds__(kBatchThreads, 1) batch_kernel(const BatchArgs A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Shared &S = *reinterpret_cast<Shared *>(smem_raw);
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  unsigned char *slot = A.scratch + static_cast<size_t>(blockIdx.x) * A.slot_bytes;
+  double2 *bufs[3];
+  for (int i = 0; i < 3; ++i) bufs[i] = reinterpret_cast<double2 *>(slot + i * A.state_bytes);
+  double4 *coef = reinterpret_cast<double4 *>(slot + 3 * A.state_bytes);
+  double2 *rot = reinterpret_cast<double2 *>(coef + kBatchMaxLayers * kBatchMaxQubits);
+  double *lscale = reinterpret_cast<double *>(rot + kBatchMaxLayers * kBatchMaxQubits);
+  double *gscale = lscale + kBatchMaxLayers;
+  double2 *ptab = reinterpret_cast<double2 *>(gscale + 2 * kBatchMaxLayers * kBatchMaxQubits);
+  double2 *prod = ptab + kBatchMaxLayers * 1024;
+
+  for (;;) {
+    if (threadIdx.x == 0) S.next = atomicAdd(A.counter, 1);
+    __syncthreads();
+    const int idx = S.next;
+    __syncthreads();
+    if (idx >= A.count) break;
+    const BatchCircuit C = A.circuits[A.order[idx]];
+    const BatchPlan &PL = A.plans[C.plan];
+    const int n = C.n, L = C.L;
+    const double *params = A.params + C.param_off;
+    const int nl = n * L;
+
+    // ---- per-circuit tables (coef_kernel, tables_kernel, rot_kernel) ----
+    for (int k = threadIdx.x; k < nl; k += blockDim.x) {
+      double st, ct, sp, cp;
+      sincos(params[2 * k] * 0.5, &st, &ct);
+      sincos(params[2 * k + 1] * 0.5, &sp, &cp);
+      coef[k] = make_double4(ct, st, cp, sp);
+      rot[k] = (fabs(ct) >= fabs(st)) ? make_double2(st / ct, 1.0) : make_double2(ct / st, -1.0);
+    }
+    for (int k = threadIdx.x; k < nl; k += blockDim.x) S.theta[k] = 0.0, S.phi_b[k] = 0.0;
+    // zero-padded layout below 12 qubits: the slot holds another circuit's
+    // data, and the padding amplitudes must read as zero
+    if (n < kTileBits)
+      for (int i = threadIdx.x; i < 3 * kTileSize; i += blockDim.x)
+        bufs[i / kTileSize][i % kTileSize] = make_double2(0.0, 0.0);
+    if (threadIdx.x < kBatchMaxLayers) S.phi_tot[threadIdx.x] = 0.0;
+    __syncthreads();
+    // phase tables (tables_kernel): only the entries an index of the
+    // (zero-padded, max(n,12)-bit) state can reach; wires >= n contribute 1 to
+    // the RZ phase and the factor of |0> to the product state
+    const int phys = n > kTileBits ? n : kTileBits;
+    for (int e = threadIdx.x; e < (L + 1) * 1024; e += blockDim.x) {
+      const int layer = e / 1024, byte = (e / 256) % 4, v = e % 256;
+      if ((v >> max(0, phys - byte * 8)) != 0) continue;  // table4 reads entry 0 of every byte
+      double2 accv = make_double2(1.0, 0.0);
+      for (int j = 0; j < 8; ++j) {
+        const int w = byte * 8 + j;
+        const bool one = (v >> j) & 1;
+        double2 f;
+        if (w >= n) {
+          f = (layer < L || !one) ? make_double2(1.0, 0.0) : make_double2(0.0, 0.0);
+        } else {
+          const double4 k = coef[(layer < L ? layer : 0) * n + w];
+          if (layer < L) f = one ? make_double2(k.z, k.w) : make_double2(k.z, -k.w);
+          else f = one ? make_double2(k.y * k.z, k.y * k.w) : make_double2(k.x * k.z, -k.x * k.w);
+        }
+        accv = cmul(accv, f);
+      }
+      if (layer < L) ptab[layer * 1024 + byte * 256 + v] = accv;
+      else prod[byte * 256 + v] = accv;
+    }
+    if (threadIdx.x < L) {
+      const int layer = threadIdx.x;
+      auto factor = [&](int w) {
+        const double4 k = coef[layer * n + w];
+        return (fabs(k.x) >= fabs(k.y)) ? k.x : k.y;
+      };
+      double K = 1.0;
+      for (int w = 0; w < n; ++w) K *= factor(w);
+      lscale[layer] = K;
+      double pending = K;
+      for (int i = 0; i < n; ++i) {
+        const int w = A.undo[PL.undo_off + i];
+        gscale[2 * (layer * n + w)] = 1.0 / (pending * pending);
+        gscale[2 * (layer * n + w) + 1] = 1.0 / (K * K);
+        pending /= factor(w);
+      }
+    }
+    __syncthreads();
+
+    // ---- the plan ----
+    double energy = 0.0;
+    for (int si = 0; si < PL.num_steps; ++si) {
+      const BatchStep &st = A.steps[PL.first_step + si];
+      if (st.kind == kBatchEnergy) {
+        energy = run_energy(bufs[st.psi_in], bufs[st.psi_out], n, C.h, S);
+        if (A.grad_out == nullptr) break;  // energies only: skip the backward sweep
+        continue;
+      }
+      const BatchTile &T = A.tiles[st.tile];
+      if (threadIdx.x == 0) {
+        PassParams &P = S.P;
+        P.n = n;
+        P.layer = st.layer;
+        P.num_runs = T.num_runs;
+        for (int r = 0; r < 4; ++r) P.run_start[r] = T.run_start[r], P.run_len[r] = T.run_len[r];
+        P.num_tiles = T.num_tiles;
+        for (int b = 0; b < 12; ++b) P.vec[b] = T.vec[b], P.gate_wire[b] = T.gate_wire[b];
+        for (int w = 0; w < 32; ++w) P.wire_tile_bit[w] = T.wire_tile_bit[w];
+        P.psi_load = st.psi_load;
+        P.lam_load = st.lam_load;
+        P.psi_store = st.psi_store;
+        P.lam_store = st.lam_store;
+        P.phase = st.phase;
+        P.phi_grad = st.phase;
+        P.sync_after_load = T.num_tiles == 1;
+        P.psi_in = st.psi_in >= 0 ? bufs[st.psi_in] : nullptr;
+        P.psi_out = st.psi_out >= 0 ? bufs[st.psi_out] : nullptr;
+        P.lam_in = st.lam_in >= 0 ? bufs[st.lam_in] : nullptr;
+        P.lam_out = st.lam_out >= 0 ? bufs[st.lam_out] : nullptr;
+        P.coef = coef;
+        P.rot = rot;
+        P.lscale = lscale;
+        P.ptab = ptab + st.layer * 1024;
+        P.prod = prod;
+        P.partials = nullptr;
+      }
+      __syncthreads();
+      const PassParams &P = S.P;
+      double acc[12];
+#pragma unroll
+      for (int i = 0; i < 12; ++i) acc[i] = 0.0;
+      if (st.kind == kBatchForward) {
+        run_pass<false>(P, S, lane, warp, acc);
+      } else {
+        run_pass<true>(P, S, lane, warp, acc);
+        // theta sums of this pass into the circuit's accumulators
+#pragma unroll
+        for (int i = 0; i < 12; ++i) {
+          const double s = warp_sum(acc[i]);
+          if (lane == 0) S.red[warp][i] = s;
+        }
+        __syncthreads();
+        if (threadIdx.x < 12 && T.gate_wire[threadIdx.x] >= 0) {
+          double s = 0.0;
+          for (int ww = 0; ww < 16; ++ww) s += S.red[ww][threadIdx.x];
+          S.theta[st.layer * n + T.gate_wire[threadIdx.x]] += s;
+        }
+        if (st.phase) {
+          if (threadIdx.x < n) S.phi_b[st.layer * n + threadIdx.x] = S.phi_sm[threadIdx.x];
+          if (threadIdx.x == 32) S.phi_tot[st.layer] = S.phi_sm[32];
+        }
+        __syncthreads();
+      }
+    }
+
+    // ---- outputs ----
+    if (threadIdx.x == 0) A.energy_out[C.index] = energy;
+    if (A.grad_out != nullptr) {
+      double *g = A.grad_out + C.param_off;
+      for (int k = threadIdx.x; k < nl; k += blockDim.x) {
+        const int layer = k / n, w = k % n;
+        g[2 * k] = S.theta[k] * gscale[2 * k];
+        g[2 * k + 1] = (S.phi_tot[layer] - 2.0 * S.phi_b[k]) * gscale[2 * k + 1];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+size_t batch_smem_bytes() { return sizeof(Shared); }
+
+size_t batch_slot_table_bytes() {
+  return kBatchMaxLayers * kBatchMaxQubits * (sizeof(double4) + sizeof(double2) + 2 * sizeof(double)) +
+         kBatchMaxLayers * sizeof(double) + (kBatchMaxLayers + 1) * 1024 * sizeof(double2);
+}
+
+cudaError_t configure_batch_kernel() {
+  return cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              static_cast<int>(sizeof(Shared)));
+}
+
+cudaError_t launch_batch(const BatchArgs &A, int grid, cudaStream_t s) {
+  batch_kernel<<<grid, kBatchThreads, sizeof(Shared), s>>>(A);
+  return cudaGetLastError();
+}
+
+}  // namespace rsv

@@ -120,6 +120,11 @@ class Engine:
         return {name: {"launches": int(counts[i]), "ms": float(ms[i]), "bytes": float(by[i])}
                 for i, name in enumerate(self.KINDS)}
 
+    def set_field(self, field: float) -> None:
+        """Change the transverse field h (same circuit shape and buffers)."""
+        check(self._lib.rsv_set_field(self._h, float(field)))
+        self.field = float(field)
+
     def device_bytes(self) -> int:
         v = ctypes.c_size_t()
         check(self._lib.rsv_backend_info(self._h, None, None, None, ctypes.byref(v)))

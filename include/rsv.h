@@ -175,6 +175,11 @@ rsv_status rsv_set_launch_timing(rsv_backend *backend, int enable);
 rsv_status rsv_launch_stats(rsv_backend *backend, int *counts, double *total_ms,
                             double *total_bytes);
 
+/* Change the transverse field h of an existing backend (the circuit shape and
+ * buffers stay).  No reference counterpart (its field is fixed at
+ * construction, cpp/ising_cuda_backend.hpp:26-29). */
+rsv_status rsv_set_field(rsv_backend *backend, double field);
+
 /* Geometry of a backend: qubits, layers, parameter count and device bytes held. */
 rsv_status rsv_backend_info(rsv_backend *backend, int *num_qubits, int *num_layers,
                             size_t *num_params, size_t *device_bytes);
@@ -197,6 +202,56 @@ rsv_status rsv_describe_plan(int num_qubits, int num_layers, char *buf, size_t b
  * ring_cnot_layer_transformed_index (reference cpp/ising_cuda_kernels.cu:178-205).
  */
 unsigned long long rsv_ring_map(unsigned long long index, int num_qubits, int inverse);
+
+/*
+ * Batched circuits: many independent ring-Ising circuits of uneven size
+ * (2 <= num_qubits <= RSV_BATCH_MAX_QUBITS, 1 <= num_layers <=
+ * RSV_BATCH_MAX_LAYERS, own field each) evaluated by ONE persistent kernel
+ * launch.  No counterpart in the reference, which evaluates one circuit per
+ * backend object; a batch of circuits there is a loop over
+ * RingIsingCudaBackend::energy_and_grad (reference cpp/ising_cuda_backend.hpp:38-41).
+ *
+ * Packed layout: circuit c owns params[off_c, off_c + 2*n_c*L_c) with
+ * off_c = sum_{j<c} 2*n_j*L_j, in the per-circuit layout above; gradients
+ * use the same packing; energies are one f64 per circuit.
+ *
+ * rsv_batch_set_circuits builds (or reuses) the pass plan of every distinct
+ * (num_qubits, num_layers), sorts the circuits by decreasing cost and uploads
+ * the descriptors; it is synchronous.  rsv_batch_run_device enqueues the
+ * whole batch on `stream` (used as given; 0 = legacy default stream): a
+ * counter reset and one kernel launch, no allocation and no host
+ * synchronisation, so it can be captured into a CUDA graph.  d_gradient_out
+ * NULL computes energies only.  A handle is not re-entrant.
+ */
+#define RSV_BATCH_MAX_QUBITS 16
+#define RSV_BATCH_MAX_LAYERS 64
+typedef struct rsv_batch rsv_batch;
+
+/* Handle whose scratch holds circuits of up to max_qubits qubits; slots = the
+ * number of circuits in flight (0 = one per SM). */
+rsv_status rsv_batch_create(int max_qubits, int slots, rsv_batch **out);
+rsv_status rsv_batch_destroy(rsv_batch *batch);
+
+rsv_status rsv_batch_set_circuits(rsv_batch *batch, int count, const int *num_qubits,
+                                  const int *num_layers, const double *fields);
+
+/* Circuits and packed parameter count of the current description. */
+rsv_status rsv_batch_info(rsv_batch *batch, int *count, size_t *num_params, int *slots,
+                          size_t *device_bytes);
+
+/* Circuits in flight for the following runs (1..the slots given at creation);
+ * used by the autotuner (gpu_simulation_b200.batch). */
+rsv_status rsv_batch_set_active_slots(rsv_batch *batch, int slots);
+
+rsv_status rsv_batch_run_device(rsv_batch *batch, const double *d_params, double *d_energy_out,
+                                double *d_gradient_out, void *stream);
+
+/* Host-memory convenience: set_circuits + copies + run + copies back,
+ * synchronous.  gradient_out may be NULL. */
+rsv_status rsv_batch_energy_and_grad(rsv_batch *batch, int count, const int *num_qubits,
+                                     const int *num_layers, const double *fields,
+                                     const double *params, size_t num_params,
+                                     double *energy_out, double *gradient_out, void *stream);
 
 #ifdef __cplusplus
 }

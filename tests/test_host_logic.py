@@ -118,3 +118,22 @@ def test_null_backend_calls_are_rejected():
     rc = lib.rsv_energy_and_grad(None, None, 0, 1, ctypes.byref(e), None, None)
     assert rc == _lib.RSV_ERR_INVALID_ARGUMENT
     assert lib.rsv_destroy(None) == 0
+
+
+def test_batch_sharding_and_synthetic_batch():
+    from gpu_simulation_b200.batch import circuit_cost, param_offsets, shard_circuits, synthetic_batch
+
+    ns, ls, hs, params = synthetic_batch(count=300, seed=7)
+    assert ns.min() >= 6 and ns.max() <= 16 and ls.min() >= 1 and ls.max() <= 16
+    assert np.all((hs >= 0.2) & (hs < 2.0))
+    assert params.size == param_offsets(ns, ls)[-1]
+    ns2, ls2, hs2, params2 = synthetic_batch(count=300, seed=7)
+    assert np.array_equal(ns, ns2) and np.array_equal(params, params2)
+    cost = circuit_cost(ns, ls)
+    for world in (1, 2, 3, 8):
+        parts = shard_circuits(ns, ls, world)
+        assert len(parts) == world
+        assert np.array_equal(np.concatenate(parts), np.arange(ns.size))
+        if world > 1:
+            loads = np.array([cost[p].sum() for p in parts])
+            assert loads.max() - loads.min() <= 2 * cost.max()
