@@ -18,6 +18,13 @@ arm runs the repository's CPU restatement of it (oracle/, OpenMP, every host
 thread) on a bounded sample of the same workload.  With --gpus N > 1 (under
 torchrun) every rank evaluates its own independent circuit (replicas, weak
 scaling; the path has no exchange step).
+
+Two further sections ride on the same JSON line: ``batch`` -- 4096 circuits
+of uneven size per step through the persistent batched kernel (one CUDA
+graph replay; with N ranks a cost-balanced shard per rank plus a final
+all-gather), against a per-circuit loop of the single-circuit entry point;
+``warm_start`` -- plain VQE from seeded random angles vs from the warm-start
+network's prediction at n=16, L=6 on 128 held-out fields (N=1 only).
 """
 
 from __future__ import annotations
@@ -53,6 +60,8 @@ def parse_args():
     ap.add_argument("--field", type=float, default=1.0)
     ap.add_argument("--no-sweep", action="store_true", help="skip the n=20/24/30 device-timed sweep")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 4096-circuit batched section")
+    ap.add_argument("--no-warmstart", action="store_true", help="skip the warm-start section")
     return ap.parse_args()
 
 
@@ -163,6 +172,140 @@ def run_reference_arm(args, rank, world):
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+# ------------------------------------------------------- batched circuits
+def fp64_peak_tflops():
+    """FP64 throughput of a cuBLAS DGEMM (8192^3, best of 5) on this GPU."""
+    import torch
+
+    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = float("inf")
+    for _ in range(5):
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e))
+    return 2.0 * 8192 ** 3 / (best * 1e-3) / 1e12
+
+
+def batch_flops(ns, ls):
+    """Algorithmic FP64 flops of energy_and_grad over a batch (FMA = 2):
+    per circuit 2^(n-1) n L (24 forward + 80 backward) + 2^n (2n + 8)."""
+    n = ns.astype(np.float64)
+    L = ls.astype(np.float64)
+    return float(np.sum(2.0 ** (n - 1) * n * L * 104.0 + 2.0 ** n * (2.0 * n + 8.0)))
+
+
+def batch_section(args, rank, world, dist, barrier, max_over_ranks):
+    """4096 circuits (n ~ U{6..16}, L ~ U{1..16}, h ~ U[0.2, 2)) per step, one
+    CUDA-graph replay of the persistent batched kernel; with N ranks every
+    rank runs its cost-balanced shard and the results are all-gathered."""
+    import torch
+
+    from gpu_simulation_b200 import BatchEngine, Engine
+    from gpu_simulation_b200.batch import gather_sharded, param_offsets, shard_circuits, synthetic_batch
+
+    count = 4096
+    ns, ls, hs, params = synthetic_batch(count, seed=7)
+    off = param_offsets(ns, ls)
+    shards = shard_circuits(ns, ls, world)
+    mine = shards[rank]
+    lo, hi = int(off[mine[0]]), int(off[mine[-1] + 1])
+    eng = BatchEngine()
+    eng.set_circuits(ns[mine], ls[mine], hs[mine])
+    p = torch.from_numpy(params[lo:hi]).cuda()
+    e = torch.empty(len(mine), dtype=torch.float64, device="cuda")
+    g = torch.empty_like(p)
+    tune = eng.autotune(p, e, g)
+    graph = eng.capture_graph(p, e, g)
+
+    def step():
+        graph.replay()
+        if world > 1:
+            gather_sharded(e, g, shards, off)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    barrier()
+    s, t = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(args.steps):
+        step()
+    t.record()
+    t.synchronize()
+    ms = max_over_ranks(s.elapsed_time(t) / args.steps)
+
+    # end to end through the host API (descriptors, parameters in; energies, gradients out)
+    eng.energy_and_grad(ns[mine], ls[mine], hs[mine], params[lo:hi])
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        eng.energy_and_grad(ns[mine], ls[mine], hs[mine], params[lo:hi])
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps)
+
+    flops = batch_flops(ns, ls)
+    out = {
+        "workload": f"{count} circuits per step: n~U{{6..16}}, L~U{{1..16}}, h~U[0.2,2), seed 7",
+        "value": count * 1000.0 / ms, "unit": "circuits/s (energy+gradient)", "ms_per_step": ms,
+        "gpu_launches_per_step": 1, "active_slots": eng.slots, "autotune_ms": tune,
+        "l2": "no flush: every replay recomputes all states from the parameters; the scratch slots are "
+              "meant to stay on chip / in L2",
+        "flops_per_step": flops, "achieved_tflops": flops / (ms * 1e-3) / 1e12,
+        "e2e": {"value": count * 1000.0 / e2e_ms, "unit": "circuits/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": int(8 * params.size + 16 * count),
+                "d2h_bytes_per_step": int(8 * (params.size + count))},
+    }
+    if world == 1:
+        peak = fp64_peak_tflops()
+        out["fp64_peak_tflops"] = peak
+        out["fp64_peak_source"] = "measured: cuBLAS DGEMM 8192^3, best of 5"
+        out["frac_of_fp64_peak"] = out["achieved_tflops"] / peak
+        # the per-circuit loop through the single-circuit device entry point
+        engines = {}
+        for c in range(count):
+            k = (int(ns[c]), int(ls[c]))
+            if k not in engines:
+                engines[k] = Engine(k[0], k[1], 1.0)
+        ee = torch.empty(count, dtype=torch.float64, device="cuda")
+        gg = torch.empty_like(p)
+
+        def loop():
+            for c in range(count):
+                en = engines[(int(ns[c]), int(ls[c]))]
+                en.set_field(float(hs[c]))
+                en.energy_and_grad_device(p[off[c]:off[c + 1]], ee[c:c + 1], gg[off[c]:off[c + 1]])
+
+        loop()
+        torch.cuda.synchronize()
+        s.record()
+        loop()
+        t.record()
+        t.synchronize()
+        loop_ms = s.elapsed_time(t)
+        out["per_circuit_loop_ms"] = loop_ms
+        out["speedup_vs_per_circuit_loop"] = loop_ms / ms
+        out["max_abs_diff_vs_loop"] = float(max((ee - e).abs().max().item(), (gg - g).abs().max().item()))
+        for en in engines.values():
+            en.close()
+    del graph
+    eng.close()
+    return out
+
+
+def warmstart_section():
+    """Warm start (n=16, L=6): plain VQE (Adam lr 0.05, 300 steps) from seeded
+    random angles vs from the network's prediction, on 128 held-out fields."""
+    from gpu_simulation_b200.warmstart import warm_start_experiment
+
+    r = warm_start_experiment()
+    r.pop("steps_plain")
+    r.pop("steps_warm")
+    return r
 
 
 # ---------------------------------------------------------------- GPU arm
@@ -319,6 +462,10 @@ def main():
                       f"{t:.2f} s, scaled by 2^{n - n_s} to n={n}",
         }
     eng.close()
+    if not args.no_batch:
+        line["batch"] = batch_section(args, rank, world, dist, barrier, max_over_ranks)
+    if world == 1 and not args.no_warmstart:
+        line["warm_start"] = warmstart_section()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -62,6 +62,22 @@ _SIGNATURES = {
     "rsv_batch_energy_and_grad": ([ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
                                    ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "rsv_mlp_num_weights": ([ctypes.c_int, ctypes.c_void_p], ctypes.c_size_t),
+    "rsv_mlp_work_floats": ([ctypes.c_int, ctypes.c_void_p, ctypes.c_int], ctypes.c_size_t),
+    "rsv_mlp_scratch_floats": ([ctypes.c_int, ctypes.c_void_p, ctypes.c_int], ctypes.c_size_t),
+    "rsv_mlp_forward": ([ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "rsv_mlp_backward": ([ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                          ctypes.c_void_p], ctypes.c_int),
+    "rsv_mlp_mse": ([ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                     ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "rsv_adam_f32": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                      ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                      ctypes.c_void_p], ctypes.c_int),
+    "rsv_adam_f64": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                      ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                      ctypes.c_void_p], ctypes.c_int),
 }
 
 _lib = None

@@ -73,6 +73,35 @@ def shard_circuits(num_qubits, num_layers, world_size: int) -> list[np.ndarray]:
     return [np.arange(bounds[r], bounds[r + 1]) for r in range(world_size)]
 
 
+def gather_sharded(local_energy, local_grad, shards, offsets, group=None):
+    """All-gather every rank's results for its shard (``shard_circuits``) into
+    the full energies [count] and packed gradients [num_params], in circuit
+    order.  Shards are contiguous ranges in rank order, so the gathered pieces
+    only need their padding trimmed.  Works on any torch.distributed backend
+    whose device holds the tensors (NCCL on GPUs, gloo on CPU)."""
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    counts = [len(s) for s in shards]
+    sizes = [int(offsets[s[-1] + 1] - offsets[s[0]]) if len(s) else 0 for s in shards]
+    pad_e, pad_g = max(1, max(counts)), max(1, max(sizes))
+    dev = local_energy.device
+
+    def padded(x, n):
+        out = torch.zeros(n, dtype=torch.float64, device=dev)
+        out[: x.numel()] = x
+        return out
+
+    e_parts = [torch.empty(pad_e, dtype=torch.float64, device=dev) for _ in range(world)]
+    g_parts = [torch.empty(pad_g, dtype=torch.float64, device=dev) for _ in range(world)]
+    dist.all_gather(e_parts, padded(local_energy, pad_e), group=group)
+    dist.all_gather(g_parts, padded(local_grad, pad_g), group=group)
+    energy = torch.cat([e_parts[r][: counts[r]] for r in range(world)])
+    grad = torch.cat([g_parts[r][: sizes[r]] for r in range(world)])
+    return energy, grad
+
+
 class BatchEngine:
     """Owns one ``rsv_batch`` (scratch for ``slots`` circuits in flight on the current GPU)."""
 

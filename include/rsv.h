@@ -253,6 +253,43 @@ rsv_status rsv_batch_energy_and_grad(rsv_batch *batch, int count, const int *num
                                      const double *params, size_t num_params,
                                      double *energy_out, double *gradient_out, void *stream);
 
+/*
+ * Warm-start network: a fully connected network in FP32 with FP32
+ * accumulation, widths[0] inputs -> widths[1] -> ... -> widths[num_layers]
+ * outputs, GELU (erf form) after every layer but the last.  It maps circuit
+ * descriptors (h, n, L) to initial angles for the VQE; every reported energy
+ * still comes from the simulator.  No counterpart in the reference (its VQE
+ * starts from seeded random angles, ring_ising/runner.py).
+ *
+ * Weights are packed layer by layer: W_l (widths[l] x widths[l-1], row-major)
+ * then b_l (widths[l]); gradients use the same packing.  All pointers are
+ * device pointers; calls are asynchronous on `stream` (used as given).
+ *   rsv_mlp_forward: x (batch x widths[0]) -> out (batch x widths[num_layers]);
+ *     d_work (rsv_mlp_work_floats) receives the pre- and post-activations of
+ *     the hidden layers for the backward pass.
+ *   rsv_mlp_backward: d_dout = dLoss/dout -> d_grad = dLoss/dweights, using
+ *     the d_work of the matching forward; d_scratch has
+ *     rsv_mlp_scratch_floats entries.
+ *   rsv_mlp_mse: loss = mean((out - target)^2) into d_loss (one float) and
+ *     d_dout = 2 (out - target) / count; d_partials holds 256 floats.
+ *   rsv_adam_f32 / rsv_adam_f64: one bias-corrected Adam step (step >= 1).
+ */
+size_t rsv_mlp_num_weights(int num_layers, const int *widths);
+size_t rsv_mlp_work_floats(int num_layers, const int *widths, int batch);
+size_t rsv_mlp_scratch_floats(int num_layers, const int *widths, int batch);
+rsv_status rsv_mlp_forward(int num_layers, const int *widths, const float *d_weights, int batch,
+                           const float *d_x, float *d_out, float *d_work, void *stream);
+rsv_status rsv_mlp_backward(int num_layers, const int *widths, const float *d_weights, int batch,
+                            const float *d_x, const float *d_work, const float *d_dout,
+                            float *d_grad, float *d_scratch, void *stream);
+rsv_status rsv_mlp_mse(size_t count, const float *d_out, const float *d_target, float *d_dout,
+                       float *d_loss, float *d_partials, void *stream);
+rsv_status rsv_adam_f32(float *d_params, const float *d_grad, float *d_m, float *d_v, size_t count,
+                        float lr, float beta1, float beta2, float eps, int step, void *stream);
+rsv_status rsv_adam_f64(double *d_params, const double *d_grad, double *d_m, double *d_v,
+                        size_t count, double lr, double beta1, double beta2, double eps, int step,
+                        void *stream);
+
 #ifdef __cplusplus
 }
 #endif
