@@ -45,6 +45,11 @@ _SIGNATURES = {
     "rsv_launch_stats": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
                          ctypes.c_int),
     "rsv_set_field": ([ctypes.c_void_p, ctypes.c_double], ctypes.c_int),
+    "rsv_set_backward_mode": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "rsv_backward_mode": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                           ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "rsv_describe_plan_mode": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t,
+                                ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
     "rsv_backend_info": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                           ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
     "rsv_describe_plan": ([ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t,

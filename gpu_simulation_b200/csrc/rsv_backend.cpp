@@ -152,23 +152,167 @@ struct Step {
   int phase = 0, phi_grad = 0;
   int psi_in = -1, psi_out = -1, lam_in = -1, lam_out = -1;
   int pass_index = -1;  // backward partial record
+  int prod_table = 0;   // analytic psi: 0 = full layer-0 state, j >= 1 = partial table j
   int grid = 1;
 };
 
 struct Plan {
   int n = 0, L = 0, phys = 0;
+  bool checkpoint = false;  // backward reads forward checkpoints of psi (see make_plan)
+  int num_bufs = 3;
   std::vector<Step> fwd, bwd;
   int chi_buf = 0, mu_buf = 1;
   std::vector<int> theta_pass, theta_slot, phi_pass;
+  // checkpoint mode: wire masks of the partial layer-0 product tables 1..
+  std::vector<unsigned int> partial_masks;
   int max_grid = 1;
 };
 
-Plan make_plan(int n, int L, int sms) {
+// Checkpoint-mode plans keep max((L-1) * passes + 1, 2) state buffers; they
+// are chosen automatically while those fit this budget.
+constexpr double kCheckpointBudgetBytes = 96.0 * (1ull << 30);
+
+int passes_per_layer(int n) {
+  if (n <= kTileBits) return 1;
+  return 1 + static_cast<int>(high_tiles(n, 12).size());
+}
+
+bool checkpoint_fits(int n, int L) {
+  if (n <= kTileBits) return false;
+  const double bufs = static_cast<double>(std::max((L - 1) * passes_per_layer(n) + 1, 2));
+  return bufs * 16.0 * static_cast<double>(u64{1} << n) <= kCheckpointBudgetBytes;
+}
+
+void record_theta(Plan &pl, const Step &s) {
+  for (int b = 0; b < 12; ++b) {
+    const int w = s.tile.gate_wire[b];
+    if (w < 0) continue;
+    const size_t k = static_cast<size_t>(s.layer) * pl.n + w;
+    if (pl.theta_pass[k] >= 0) throw Error(RSV_ERR_INTERNAL, "wire planned twice");
+    pl.theta_pass[k] = s.pass_index;
+    pl.theta_slot[k] = b;
+  }
+}
+
+Plan make_checkpoint_plan(Plan pl, const std::vector<Tile> &fwd_tiles, int fwd_ctas, int bwd_ctas) {
+  const int n = pl.n, L = pl.L;
+  const int P = static_cast<int>(fwd_tiles.size());
+  auto grid_for = [](const Tile &t, int ctas) {
+    return static_cast<int>(std::min<u64>(t.num_tiles, static_cast<u64>(ctas)));
+  };
+  std::vector<int> all_bits(12);
+  for (int b = 0; b < 12; ++b) all_bits[b] = b;
+  int next = 0;
+  std::vector<std::vector<int>> ck(L);  // ck[l][j]: buffer written by forward pass j of layer l
+  int cur = -1;                          // input of the next layer (after its CNOT ring)
+  if (L == 1) {
+    Step s;
+    s.tile = unit_tile(pl.phys, all_bits, {});
+    s.psi_load = kLoadProductPlain;
+    s.psi_out = next++;
+    s.psi_store = kStoreNatural;
+    s.grid = grid_for(s.tile, fwd_ctas);
+    pl.fwd.push_back(s);
+    cur = s.psi_out;
+  }
+  for (int layer = 1; layer < L; ++layer) {
+    for (int j = 0; j < P; ++j) {
+      const bool first = j == 0, last = j + 1 == P;
+      Step s;
+      s.layer = layer;
+      s.tile = fwd_tiles[static_cast<size_t>(j)];
+      s.psi_load = (first && layer == 1) ? kLoadProduct : kLoadNatural;
+      s.psi_in = s.psi_load == kLoadNatural ? (first ? cur : ck[layer].back()) : -1;
+      s.phase = last ? 1 : 0;
+      s.psi_out = next++;
+      s.psi_store = (last && layer + 1 < L) ? kStoreScatterP : kStoreNatural;
+      s.grid = grid_for(s.tile, fwd_ctas);
+      ck[layer].push_back(s.psi_out);
+      if (last) cur = s.psi_out;
+      pl.fwd.push_back(s);
+    }
+  }
+  pl.chi_buf = cur;
+  pl.mu_buf = next++;
+  pl.num_bufs = next;
+
+  // partial product tables of layer 0: table j+1 = wires of forward passes 0..j
+  // applied (RY / f on |0>, no RZ), every other wire still |0>
+  for (int j = 0; j + 1 < P; ++j) {
+    unsigned int m = 0;
+    for (int jj = 0; jj <= j; ++jj)
+      for (int b = 0; b < 12; ++b)
+        if (fwd_tiles[static_cast<size_t>(jj)].gate_wire[b] >= 0)
+          m |= 1u << fwd_tiles[static_cast<size_t>(jj)].gate_wire[b];
+    pl.partial_masks.push_back(m);
+  }
+
+  pl.theta_pass.assign(static_cast<size_t>(n) * L, -1);
+  pl.theta_slot.assign(static_cast<size_t>(n) * L, -1);
+  pl.phi_pass.assign(L, -1);
+  int lam = pl.mu_buf;
+  int pass_index = 0;
+  for (int layer = L - 1; layer >= 0; --layer) {
+    for (int gi = 0; gi < P; ++gi) {
+      const int j = P - 1 - gi;  // the forward pass this backward pass undoes
+      const bool first = gi == 0, final_pass = layer == 0 && gi + 1 == P;
+      Step s;
+      s.bwd = true;
+      s.layer = layer;
+      s.tile = fwd_tiles[static_cast<size_t>(j)];
+      s.phase = first ? 1 : 0;
+      s.phi_grad = first ? 1 : 0;
+      if (s.phi_grad && !s.tile.unit) throw Error(RSV_ERR_INTERNAL, "phi pass needs a unit tile");
+      if (layer == 0) {
+        s.psi_load = kLoadProductPlain;
+        s.prod_table = first ? 0 : j + 1;
+      } else {
+        s.psi_in = ck[layer][static_cast<size_t>(j)];
+        s.psi_load = (first && layer + 1 < L) ? kLoadGatherP : kLoadNatural;
+      }
+      s.psi_store = kStoreNone;
+      s.lam_in = lam;
+      s.lam_load = (first && layer + 1 < L) ? kLoadGatherP : kLoadNatural;
+      if (s.lam_load == kLoadGatherP) {
+        // the checkpoints of layer + 1 are dead: take one for lambda
+        s.lam_out = ck[layer + 1][0];
+        lam = s.lam_out;
+      } else {
+        s.lam_out = lam;
+      }
+      s.lam_store = final_pass ? kStoreNone : kStoreNatural;
+      s.pass_index = pass_index++;
+      s.grid = grid_for(s.tile, bwd_ctas);
+      record_theta(pl, s);
+      if (first) pl.phi_pass[layer] = s.pass_index;
+      pl.max_grid = std::max(pl.max_grid, s.grid);
+      pl.bwd.push_back(s);
+    }
+  }
+  for (size_t k = 0; k < pl.theta_pass.size(); ++k)
+    if (pl.theta_pass[k] < 0) throw Error(RSV_ERR_INTERNAL, "wire without a backward pass");
+  return pl;
+}
+
+// Two backward schedules share the forward tiles and the kernels:
+//   uncompute (checkpoint = false): three state buffers; the backward
+//     un-computes psi alongside lambda (reads and writes both), and its last
+//     pass per layer scatters psi through P^-1 (antipodal tile);
+//   checkpoint: every forward pass writes a fresh buffer; backward pass j of a
+//     layer undoes exactly the wires of forward pass P-1-j, reads psi from the
+//     checkpoint after that forward pass (gathered through P for the layer's
+//     last pass, analytic product tables for layer 0) and writes only lambda.
+//     Reference counterpart: run_structured_backward_sweep
+//     (cpp/ising_cuda_structured_adjoint_modes.inc:188-307), which always
+//     un-computes psi.
+Plan make_plan(int n, int L, int sms, bool checkpoint = false) {
   Plan pl;
   pl.n = n;
   pl.L = L;
   pl.phys = std::max(n, kTileBits);
   const bool single = (pl.phys == kTileBits);
+  if (single) checkpoint = false;  // one tile: every permutation in place, three buffers
+  pl.checkpoint = checkpoint;
   const int fwd_ctas = std::max(1, 2 * sms), bwd_ctas = std::max(1, sms);
 
   std::vector<int> all_bits(12), real_wires;
@@ -189,6 +333,7 @@ Plan make_plan(int n, int L, int sms) {
   auto grid_for = [](const Tile &t, int ctas) {
     return static_cast<int>(std::min<u64>(t.num_tiles, static_cast<u64>(ctas)));
   };
+  if (checkpoint) return make_checkpoint_plan(pl, fwd_tiles, fwd_ctas, bwd_ctas);
 
   // Forward.  Layer 0 is the analytic product state; layers 1..L-1 run
   // their passes; the last pass of each layer applies the RZ phase and, except
@@ -299,16 +444,22 @@ Plan make_plan(int n, int L, int sms) {
 // Undo order of the wires within one backward layer, as the backward pass
 // kernel visits them: passes in plan order; inside a pass the register groups
 // of tile bits 9..11, 6..8, 0..2, then 3..5 (layouts B0, B1, A1, A2 of
-// rsv_pass.cu).  Needed for the exact tangent-form gradient correction.
+// rsv_pass.cu and of the batched kernel).  Needed for the exact tangent-form
+// gradient correction.  In checkpoint mode the first wire of every pass
+// carries kUndoPassStart (the gradient correction restarts there, see
+// rot_kernel).
 std::vector<int> undo_order(const Plan &pl) {
+  static const int kBits[12] = {9, 10, 11, 6, 7, 8, 0, 1, 2, 3, 4, 5};
   std::vector<int> ord;
   for (const auto &s : pl.bwd) {
     if (s.layer != pl.L - 1) continue;
-    for (int g : {3, 2, 0, 1})
-      for (int j = 0; j < 3; ++j) {
-        const int w = s.tile.gate_wire[3 * g + j];
-        if (w >= 0) ord.push_back(w);
-      }
+    bool start = pl.checkpoint;
+    for (int i = 0; i < 12; ++i) {
+      const int w = s.tile.gate_wire[kBits[i]];
+      if (w < 0) continue;
+      ord.push_back(start ? (w | kUndoPassStart) : w);
+      start = false;
+    }
   }
   if (static_cast<int>(ord.size()) != pl.n) throw Error(RSV_ERR_INTERNAL, "undo order incomplete");
   return ord;
@@ -361,15 +512,24 @@ std::string describe(const Plan &pl) {
     ts << "] tiles=" << t.num_tiles;
     return ts.str();
   };
-  os << "n=" << pl.n << " L=" << pl.L << " phys=" << pl.phys << "\n";
+  os << "n=" << pl.n << " L=" << pl.L << " phys=" << pl.phys << " bufs=" << pl.num_bufs
+     << " mode=" << (pl.checkpoint ? "checkpoint" : "uncompute") << "\n";
   for (const auto &s : pl.fwd)
     os << "fwd layer=" << s.layer << " " << tile_str(s.tile) << " psi:" << load_name(s.psi_load)
        << "(" << s.psi_in << ")->" << store_name(s.psi_store) << "(" << s.psi_out << ")"
        << (s.phase ? " phase" : "") << " grid=" << s.grid << "\n";
   os << "energy chi=" << pl.chi_buf << " mu=" << pl.mu_buf << "\n";
+  auto psi_src = [&](const Step &s) -> std::string {
+    if (s.psi_load == kLoadProductPlain && s.prod_table > 0) {
+      std::ostringstream ps;
+      ps << "partial(0x" << std::hex << pl.partial_masks[static_cast<size_t>(s.prod_table - 1)] << ")";
+      return ps.str();
+    }
+    return load_name(s.psi_load);
+  };
   for (const auto &s : pl.bwd)
     os << "bwd layer=" << s.layer << " pass=" << s.pass_index << " " << tile_str(s.tile)
-       << " psi:" << load_name(s.psi_load) << "(" << s.psi_in << ")->" << store_name(s.psi_store)
+       << " psi:" << psi_src(s) << "(" << s.psi_in << ")->" << store_name(s.psi_store)
        << "(" << s.psi_out << ") lam:" << load_name(s.lam_load) << "(" << s.lam_in << ")->"
        << store_name(s.lam_store) << "(" << s.lam_out << ")" << (s.phase ? " phase" : "")
        << (s.phi_grad ? " phi" : "") << " grid=" << s.grid << "\n";
@@ -438,7 +598,8 @@ struct rsv_backend {
   int device = 0, sms = 0;
   cudaStream_t stream = nullptr;
   rsv::Plan plan;
-  rsv::DevBuf<double2> buf[3];
+  rsv::DevBuf<double2> states;  // plan.num_bufs state buffers of state_len amplitudes each
+  int backward_mode = RSV_BACKWARD_AUTO;
   rsv::DevBuf<double4> coef;
   rsv::DevBuf<double2> ptab, prod;
   rsv::DevBuf<double> energy_partials, pass_partials, outputs;  // outputs: [1 + num_params]
@@ -467,6 +628,8 @@ struct rsv_backend {
 
 namespace rsv {
 namespace {
+
+double2 *state_buf(const rsv_backend *B, int i) { return B->states.p + static_cast<size_t>(i) * B->state_len; }
 
 void fill_pass_params(rsv_backend *B, const Step &s, PassParams &P) {
   std::memset(&P, 0, sizeof(P));
@@ -534,15 +697,15 @@ void fill_pass_params(rsv_backend *B, const Step &s, PassParams &P) {
       if (w >= 0 && ((v >> w) & 1)) throw Error(RSV_ERR_INTERNAL, "multi-bit direction overlaps a gated wire");
     }
   }
-  P.psi_in = s.psi_in >= 0 ? B->buf[s.psi_in].p : nullptr;
-  P.psi_out = s.psi_out >= 0 ? B->buf[s.psi_out].p : nullptr;
-  P.lam_in = s.lam_in >= 0 ? B->buf[s.lam_in].p : nullptr;
-  P.lam_out = s.lam_out >= 0 ? B->buf[s.lam_out].p : nullptr;
+  P.psi_in = s.psi_in >= 0 ? state_buf(B, s.psi_in) : nullptr;
+  P.psi_out = s.psi_out >= 0 ? state_buf(B, s.psi_out) : nullptr;
+  P.lam_in = s.lam_in >= 0 ? state_buf(B, s.lam_in) : nullptr;
+  P.lam_out = s.lam_out >= 0 ? state_buf(B, s.lam_out) : nullptr;
   P.coef = B->coef.p;
   P.rot = B->rot.p;
   P.lscale = B->lscale.p;
   P.ptab = B->ptab.p + static_cast<size_t>(s.layer) * 1024;
-  P.prod = B->prod.p;
+  P.prod = B->prod.p + static_cast<size_t>(s.prod_table) * 1024;
   P.partials = s.bwd ? B->pass_partials.p + static_cast<size_t>(s.pass_index) * B->plan.max_grid *
                                                  kPartialStride
                      : nullptr;
@@ -599,7 +762,7 @@ void run_forward(rsv_backend *B, cudaStream_t st) {
 void run_energy(rsv_backend *B, cudaStream_t st) {
   const double bytes = 2.0 * 16.0 * static_cast<double>(u64{1} << B->n);
   timed(B, st, 2, bytes, [&] {
-    check(launch_energy(B->buf[B->plan.chi_buf].p, B->buf[B->plan.mu_buf].p, B->n, B->field,
+    check(launch_energy(state_buf(B, B->plan.chi_buf), state_buf(B, B->plan.mu_buf), B->n, B->field,
                         u64{1} << B->n, B->energy_partials.p, B->energy_grid, st),
           "energy launch");
   });
@@ -648,16 +811,31 @@ void upload_host_coefs(rsv_backend *B, const double *params, cudaStream_t st) {
         "coefficient upload");
 }
 
+PartialMasks partial_masks(const Plan &pl) {
+  PartialMasks m{};
+  m.count = static_cast<int>(pl.partial_masks.size());
+  if (m.count > kMaxPartialTables) throw Error(RSV_ERR_INTERNAL, "too many partial product tables");
+  for (int i = 0; i < m.count; ++i) m.mask[i] = pl.partial_masks[static_cast<size_t>(i)];
+  return m;
+}
+
+// Per-call tables (RZ phases, product states, tangent forms, gradient corrections).
+void launch_prep(rsv_backend *B, cudaStream_t st) {
+  timed(B, st, 0, 0.0, [&] {
+    check(launch_tables(B->coef.p, B->n, B->L, B->ptab.p, B->prod.p, partial_masks(B->plan), st),
+          "tables launch");
+  });
+  timed(B, st, 0, 0.0, [&] {
+    check(launch_rot(B->coef.p, B->n, B->L, B->order.p, B->plan.checkpoint, B->rot.p, B->lscale.p,
+                     B->gscale.p, st),
+          "rot launch");
+  });
+}
+
 void run_all(rsv_backend *B, bool grad, double *energy_out, double *grad_out, cudaStream_t st) {
   ++B->generation;
   B->forward_only_state = false;
-  timed(B, st, 0, 0.0, [&] {
-    check(launch_tables(B->coef.p, B->n, B->L, B->ptab.p, B->prod.p, st), "tables launch");
-  });
-  timed(B, st, 0, 0.0, [&] {
-    check(launch_rot(B->coef.p, B->n, B->L, B->order.p, B->rot.p, B->lscale.p, B->gscale.p, st),
-          "rot launch");
-  });
+  launch_prep(B, st);
   run_forward(B, st);
   run_energy(B, st);
   if (grad) run_backward(B, st);
@@ -951,7 +1129,8 @@ rsv_status run_in_workspace(int n, int L, double field, const double *d_params, 
     if (off > workspace_bytes)
       invalid("circuit needs " + std::to_string(off) + " workspace bytes, the fixed workspace has " +
               std::to_string(workspace_bytes));
-    for (int i = 0; i < 3; ++i) B.buf[i].view(reinterpret_cast<double2 *>(bufs[i]), B.state_len);
+    // the three buffers were carved back to back (each a multiple of 256 bytes)
+    B.states.view(reinterpret_cast<double2 *>(bufs[0]), 3 * B.state_len);
     B.coef.view(reinterpret_cast<double4 *>(coef), nl);
     B.rot.view(reinterpret_cast<double2 *>(rot), nl);
     B.lscale.view(reinterpret_cast<double *>(lscale), L);
@@ -970,13 +1149,61 @@ rsv_status run_in_workspace(int n, int L, double field, const double *d_params, 
     // The workspace keeps the previous call's contents; for n < 12 the padding
     // amplitudes of the state buffers must start at zero.
     if (B.plan.phys > n)
-      for (int i = 0; i < 3; ++i)
-        check(cudaMemsetAsync(B.buf[i].p, 0, B.state_len * sizeof(double2), st), "state clear");
+      check(cudaMemsetAsync(B.states.p, 0, 3 * B.state_len * sizeof(double2), st), "state clear");
     check(launch_coef(d_params, B.coef.p, static_cast<int>(nl), st), "coef launch");
     run_all(&B, d_gradient_out != nullptr, d_energy_out, d_gradient_out, st);
     // the host vectors above are consumed by the time cudaMemcpyAsync from
     // pageable memory returns; nothing else outlives this call
   });
+}
+
+// (Re)plan a backend for a backward schedule and allocate what depends on the
+// plan: the state buffers, the product tables, the partial records and the
+// plan tables.  A failed allocation of the checkpoint schedule falls back to
+// the three-buffer schedule when the mode is automatic.
+void setup_plan(rsv_backend *B, int mode) {
+  if (mode != RSV_BACKWARD_AUTO && mode != RSV_BACKWARD_UNCOMPUTE && mode != RSV_BACKWARD_CHECKPOINT)
+    invalid("backward mode must be RSV_BACKWARD_AUTO, _UNCOMPUTE or _CHECKPOINT");
+  const bool want = mode == RSV_BACKWARD_CHECKPOINT || (mode == RSV_BACKWARD_AUTO && checkpoint_fits(B->n, B->L));
+  B->states.release();
+  Plan pl = make_plan(B->n, B->L, B->sms, want);
+  B->state_len = size_t{1} << pl.phys;
+  try {
+    B->states.alloc(static_cast<size_t>(pl.num_bufs) * B->state_len);
+  } catch (const Error &e) {
+    if (mode != RSV_BACKWARD_AUTO || !pl.checkpoint || e.status != RSV_ERR_OUT_OF_MEMORY) throw;
+    cudaGetLastError();  // clear the allocation failure
+    pl = make_plan(B->n, B->L, B->sms, false);
+    B->states.alloc(static_cast<size_t>(pl.num_bufs) * B->state_len);
+  }
+  check(cudaMemset(B->states.p, 0, B->states.count * sizeof(double2)), "state memset");
+  B->plan = pl;
+  B->backward_mode = mode;
+  B->num_bwd_passes = static_cast<int>(B->plan.bwd.size());
+  B->prod.alloc(1024 * (1 + B->plan.partial_masks.size()));
+  B->pass_partials.alloc(static_cast<size_t>(std::max(1, B->num_bwd_passes)) * B->plan.max_grid *
+                         kPartialStride);
+  std::vector<int> tab;
+  for (const auto &s : B->plan.bwd) tab.push_back(s.grid);
+  tab.insert(tab.end(), B->plan.theta_pass.begin(), B->plan.theta_pass.end());
+  tab.insert(tab.end(), B->plan.theta_slot.begin(), B->plan.theta_slot.end());
+  tab.insert(tab.end(), B->plan.phi_pass.begin(), B->plan.phi_pass.end());
+  B->tables.alloc(tab.size());
+  check(cudaMemcpy(B->tables.p, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice),
+        "plan table upload");
+  const std::vector<int> ord = undo_order(B->plan);
+  B->order.alloc(ord.size());
+  check(cudaMemcpy(B->order.p, ord.data(), ord.size() * sizeof(int), cudaMemcpyHostToDevice),
+        "order upload");
+  ++B->generation;  // any state kept for a deferred backward is gone
+  B->forward_only_state = false;
+}
+
+Plan plan_for_mode(int n, int L, int mode) {
+  if (mode == RSV_BACKWARD_AUTO) return make_plan(n, L, 148, checkpoint_fits(n, L));
+  if (mode == RSV_BACKWARD_UNCOMPUTE) return make_plan(n, L, 148, false);
+  if (mode == RSV_BACKWARD_CHECKPOINT) return make_plan(n, L, 148, true);
+  invalid("backward mode must be RSV_BACKWARD_AUTO, _UNCOMPUTE or _CHECKPOINT");
 }
 
 }  // namespace rsv
@@ -1000,10 +1227,15 @@ unsigned long long rsv_ring_map(unsigned long long index, int num_qubits, int in
 
 rsv_status rsv_describe_plan(int num_qubits, int num_layers, char *buf, size_t buf_size,
                              size_t *length_out) {
+  return rsv_describe_plan_mode(num_qubits, num_layers, RSV_BACKWARD_AUTO, buf, buf_size, length_out);
+}
+
+rsv_status rsv_describe_plan_mode(int num_qubits, int num_layers, int backward_mode, char *buf,
+                                  size_t buf_size, size_t *length_out) {
   return guarded([&] {
     if (num_qubits < 2 || num_qubits > kMaxQubits) invalid("num_qubits out of range");
     if (num_layers < 1) invalid("num_layers must be at least 1");
-    const Plan pl = make_plan(num_qubits, num_layers, 148);
+    const Plan pl = plan_for_mode(num_qubits, num_layers, backward_mode);
     const std::string s = describe(pl);
     if (length_out) *length_out = s.size();
     if (buf && buf_size) {
@@ -1048,40 +1280,17 @@ rsv_status rsv_create(int num_qubits, int num_layers, double field, const char *
       check(configure_pass_kernels(), "configure pass kernels");
       configured = true;
     }
-    B->plan = make_plan(num_qubits, num_layers, B->sms);
-    B->num_bwd_passes = static_cast<int>(B->plan.bwd.size());
-    B->state_len = size_t{1} << B->plan.phys;
-    for (auto &b : B->buf) {
-      b.alloc(B->state_len);
-      check(cudaMemset(b.p, 0, B->state_len * sizeof(double2)), "state memset");
-    }
+    setup_plan(B.get(), RSV_BACKWARD_AUTO);
     const size_t nl = static_cast<size_t>(num_qubits) * num_layers;
     B->coef.alloc(nl);
     B->ptab.alloc(static_cast<size_t>(num_layers) * 1024);
-    B->prod.alloc(1024);
     B->energy_grid = static_cast<int>(std::min<u64>(
         std::max<u64>(1, (u64{1} << num_qubits) / 256), static_cast<u64>(B->sms) * 8));
     B->energy_partials.alloc(B->energy_grid);
-    B->pass_partials.alloc(static_cast<size_t>(std::max(1, B->num_bwd_passes)) * B->plan.max_grid *
-                           kPartialStride);
     B->outputs.alloc(1 + B->num_params);
-    std::vector<int> tab;
-    for (const auto &s : B->plan.bwd) tab.push_back(s.grid);
-    tab.insert(tab.end(), B->plan.theta_pass.begin(), B->plan.theta_pass.end());
-    tab.insert(tab.end(), B->plan.theta_slot.begin(), B->plan.theta_slot.end());
-    tab.insert(tab.end(), B->plan.phi_pass.begin(), B->plan.phi_pass.end());
-    B->tables.alloc(tab.size());
-    check(cudaMemcpy(B->tables.p, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice),
-          "plan table upload");
     B->rot.alloc(nl);
     B->lscale.alloc(num_layers);
     B->gscale.alloc(2 * nl);
-    {
-      const std::vector<int> ord = undo_order(B->plan);
-      B->order.alloc(ord.size());
-      check(cudaMemcpy(B->order.p, ord.data(), ord.size() * sizeof(int), cudaMemcpyHostToDevice),
-            "order upload");
-    }
     B->coef_host.alloc(nl);
     B->out_host.alloc(1 + B->num_params);
     check(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -1187,9 +1396,7 @@ rsv_status rsv_profile_energy_and_grad(rsv_backend *B, const double *params, siz
     ++B->generation;
     B->forward_only_state = false;
     cudaEventRecord(ev[0], st);
-    check(launch_tables(B->coef.p, B->n, B->L, B->ptab.p, B->prod.p, st), "tables launch");
-    check(launch_rot(B->coef.p, B->n, B->L, B->order.p, B->rot.p, B->lscale.p, B->gscale.p, st),
-          "rot launch");
+    launch_prep(B, st);
     cudaEventRecord(ev[1], st);
     run_forward(B, st);
     cudaEventRecord(ev[2], st);
@@ -1233,9 +1440,7 @@ rsv_status rsv_benchmark_forward_graph(rsv_backend *B, const double *params, siz
     B->forward_only_state = false;
     upload_host_coefs(B, params, st);
     auto forward = [&] {
-      check(launch_tables(B->coef.p, B->n, B->L, B->ptab.p, B->prod.p, st), "tables launch");
-      check(launch_rot(B->coef.p, B->n, B->L, B->order.p, B->rot.p, B->lscale.p, B->gscale.p, st),
-            "rot launch");
+      launch_prep(B, st);
       run_forward(B, st);
     };
     cudaEvent_t a, b;
@@ -1300,6 +1505,23 @@ rsv_status rsv_launch_stats(rsv_backend *B, int *counts, double *total_ms, doubl
   });
 }
 
+rsv_status rsv_set_backward_mode(rsv_backend *B, int mode) {
+  return guarded([&] {
+    if (B == nullptr) invalid("backend is null");
+    check(cudaStreamSynchronize(B->stream), "backend synchronize");
+    setup_plan(B, mode);
+  });
+}
+
+rsv_status rsv_backward_mode(rsv_backend *B, int *mode_out, int *checkpoint_out, int *num_buffers_out) {
+  return guarded([&] {
+    if (B == nullptr) invalid("backend is null");
+    if (mode_out) *mode_out = B->backward_mode;
+    if (checkpoint_out) *checkpoint_out = B->plan.checkpoint ? 1 : 0;
+    if (num_buffers_out) *num_buffers_out = B->plan.num_bufs;
+  });
+}
+
 rsv_status rsv_set_field(rsv_backend *B, double field) {
   return guarded([&] {
     if (B == nullptr) invalid("backend is null");
@@ -1316,7 +1538,7 @@ rsv_status rsv_backend_info(rsv_backend *B, int *num_qubits, int *num_layers, si
     if (num_layers) *num_layers = B->L;
     if (num_params) *num_params = B->num_params;
     if (device_bytes)
-      *device_bytes = 3 * B->state_len * sizeof(double2) + B->pass_partials.count * sizeof(double) +
+      *device_bytes = B->states.count * sizeof(double2) + B->pass_partials.count * sizeof(double) +
                       B->energy_partials.count * sizeof(double);
   });
 }

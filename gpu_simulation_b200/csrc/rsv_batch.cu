@@ -31,13 +31,13 @@ constexpr int kBatchThreads = bw::kT;
 // Forward rotation of the three register bits of layout LY: RY / f in
 // tangent form (mode +1: [[1,-k],[k,1]], mode -1: [[k,-1],[1,k]]).
 template <int LY>
-__device__ __forceinline__ void fgates(const PassParams &P, double2 (&a)[kR]) {
+__device__ __forceinline__ void fgates(const PassParams &P, const double2 *km_tb, double2 (&a)[kR]) {
   constexpr int RB = rbit<LY>();
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
     const int w = P.gate_wire[RB + j];
     if (w < 0) continue;
-    const double2 km = P.rot[P.layer * P.n + w];
+    const double2 km = km_tb[RB + j];
     const double k = km.x;
     if (km.y > 0.0) {
 #pragma unroll
@@ -77,6 +77,7 @@ __device__ __forceinline__ void store_dst(int mode, double2 *buf, u32 p, int n, 
 
 struct Shared {
   PassParams P;  // the current pass (uniform over the CTA; kept off the thread stacks)
+  double2 km[12];  // tangent form of the wire gated on each tile bit of the pass
   double2 stage_a[kTileSize];
   double2 stage_b[kTileSize];
   double2 trans[kTileSize];
@@ -160,21 +161,21 @@ __device__ void run_pass(const PassParams &P, Shared &S, int lane, int warp, dou
       phi_sums(P, cbase, lane, warp, a, b, S.red, S.phi_sm);
     }
 
-    if (BWD) gates<B0>(P, a, b, acc); else fgates<B0>(P, a);
+    if (BWD) gates<B0>(P, S.km, a, b, acc); else fgates<B0>(P, S.km, a);
     warp_transpose<B0, B1>(wbuf, lane, warp, a);
     if (BWD) warp_transpose<B0, B1>(wbuf, lane, warp, b);
-    if (BWD) gates<B1>(P, a, b, acc); else fgates<B1>(P, a);
+    if (BWD) gates<B1>(P, S.km, a, b, acc); else fgates<B1>(P, S.km, a);
     if (has_lo) {
       cta_transpose<B1, A1>(S.trans, lane, warp, a);
       if (BWD) cta_transpose<B1, A1>(S.trans, lane, warp, b);
-      if (BWD) gates<A1>(P, a, b, acc); else fgates<A1>(P, a);
+      if (BWD) gates<A1>(P, S.km, a, b, acc); else fgates<A1>(P, S.km, a);
       warp_transpose<A1, A2>(wbuf, lane, warp, a);
       if (BWD) warp_transpose<A1, A2>(wbuf, lane, warp, b);
     } else {
       cta_transpose<B1, A2>(S.trans, lane, warp, a);
       if (BWD) cta_transpose<B1, A2>(S.trans, lane, warp, b);
     }
-    if (BWD) gates<A2>(P, a, b, acc); else fgates<A2>(P, a);
+    if (BWD) gates<A2>(P, S.km, a, b, acc); else fgates<A2>(P, S.km, a);
 
     const u32 base = cbase ^ toffs;
     if (!BWD && P.phase) {
@@ -349,6 +350,8 @@ __global__ void __launch_bounds__(kBatchThreads, 1) batch_kernel(const BatchArgs
         P.ptab = ptab + st.layer * 1024;
         P.prod = prod;
         P.partials = nullptr;
+        for (int b = 0; b < 12; ++b)
+          S.km[b] = T.gate_wire[b] >= 0 ? rot[st.layer * n + T.gate_wire[b]] : make_double2(0.0, 1.0);
       }
       __syncthreads();
       const PassParams &P = S.P;

@@ -29,12 +29,32 @@ __global__ void coef_kernel(const double *__restrict__ params, double4 *__restri
 // factor of |0> (1 for bit 0, 0 for bit 1).
 // grid: (L + 1) * 4 blocks of 256 threads; block L*4.. builds prod.
 __global__ void tables_kernel(const double4 *__restrict__ coef, int n, int L,
-                              double2 *__restrict__ ptab, double2 *__restrict__ prod) {
+                              double2 *__restrict__ ptab, double2 *__restrict__ prod,
+                              const PartialMasks partial) {
   const int tbl = blockIdx.x;
   const int layer = tbl / 4;
   const int byte = tbl % 4;
   const int v = threadIdx.x;
   double2 acc = make_double2(1.0, 0.0);
+  if (layer > L) {
+    // partial product table (layer > L): wires in the mask carry RY / f |0>
+    // of layer 0 (tangent form, no RZ), the others |0>
+    const int j = layer - L - 1;
+    const unsigned int m = partial.mask[j];
+    for (int b = 0; b < 8; ++b) {
+      const int w = byte * 8 + b;
+      const bool one = (v >> b) & 1;
+      double f = one ? 0.0 : 1.0;
+      if (w < n && ((m >> w) & 1)) {
+        const double4 k = coef[w];
+        const double fac = (fabs(k.x) >= fabs(k.y)) ? k.x : k.y;
+        f = (one ? k.y : k.x) / fac;
+      }
+      acc = make_double2(acc.x * f, acc.y * f);
+    }
+    prod[(1 + j) * 1024 + byte * 256 + v] = acc;
+    return;
+  }
   if (layer < L) {
     for (int j = 0; j < 8; ++j) {
       const int w = byte * 8 + j;
@@ -71,10 +91,15 @@ __global__ void tables_kernel(const double4 *__restrict__ coef, int n, int L,
 //   theta of wire w: 1 / (prod of f over the wires of its layer still pending
 //                         when w is undone, w included)^2,
 //   phi of the layer: 1 / K_l^2.
-// order[n] is the undo order of the wires within a backward layer.
+// order[n] is the undo order of the wires within a backward layer.  In the
+// checkpoint schedule psi is re-read from the forward pass's checkpoint at
+// every backward pass, so the correction restarts at each pass (entries with
+// kUndoPassStart):
+//   theta of wire w: (prod of f over the wires undone before w in its pass)^2,
+//                    divided by K_l^2 in the layer's first (phase) pass.
 // grid: L blocks of 32 threads.
 __global__ void rot_kernel(const double4 *__restrict__ coef, int n, int L, const int *__restrict__ order,
-                           double2 *__restrict__ rot, double *__restrict__ lscale,
+                           int checkpoint, double2 *__restrict__ rot, double *__restrict__ lscale,
                            double *__restrict__ gscale) {
   const int layer = blockIdx.x;
   if (layer >= L) return;
@@ -91,12 +116,31 @@ __global__ void rot_kernel(const double4 *__restrict__ coef, int n, int L, const
   double K = 1.0;
   for (int w = 0; w < n; ++w) K *= factor(w);
   lscale[layer] = K;
-  double pending = K;
-  for (int i = 0; i < n; ++i) {
-    const int w = order[i];
-    gscale[2 * (layer * n + w)] = 1.0 / (pending * pending);
-    gscale[2 * (layer * n + w) + 1] = 1.0 / (K * K);
-    pending /= factor(w);
+  if (!checkpoint) {
+    double pending = K;
+    for (int i = 0; i < n; ++i) {
+      const int w = order[i] & (kUndoPassStart - 1);
+      gscale[2 * (layer * n + w)] = 1.0 / (pending * pending);
+      gscale[2 * (layer * n + w) + 1] = 1.0 / (K * K);
+      pending /= factor(w);
+    }
+  } else {
+    // psi from a checkpoint: at the start of the layer's first backward pass
+    // psi and lambda both carry K (the phase pass), at the start of every
+    // later pass their factors cancel; inside a pass each undone wire divides
+    // both by its f.
+    double undone = 1.0;
+    bool first = true;
+    for (int i = 0; i < n; ++i) {
+      const int w = order[i] & (kUndoPassStart - 1);
+      if (i > 0 && (order[i] & kUndoPassStart)) {
+        undone = 1.0;
+        first = false;
+      }
+      gscale[2 * (layer * n + w)] = undone * undone / (first ? K * K : 1.0);
+      gscale[2 * (layer * n + w) + 1] = 1.0 / (K * K);
+      undone *= factor(w);
+    }
   }
 }
 
@@ -201,14 +245,15 @@ cudaError_t launch_coef(const double *params, double4 *coef, int count, cudaStre
 }
 
 cudaError_t launch_tables(const double4 *coef, int n, int L, double2 *ptab, double2 *prod,
-                          cudaStream_t s) {
-  tables_kernel<<<(L + 1) * 4, 256, 0, s>>>(coef, n, L, ptab, prod);
+                          const PartialMasks &partial, cudaStream_t s) {
+  if (partial.count < 0 || partial.count > kMaxPartialTables) return cudaErrorInvalidValue;
+  tables_kernel<<<(L + 1 + partial.count) * 4, 256, 0, s>>>(coef, n, L, ptab, prod, partial);
   return cudaGetLastError();
 }
 
-cudaError_t launch_rot(const double4 *coef, int n, int L, const int *order, double2 *rot,
-                       double *lscale, double *gscale, cudaStream_t s) {
-  rot_kernel<<<L, 32, 0, s>>>(coef, n, L, order, rot, lscale, gscale);
+cudaError_t launch_rot(const double4 *coef, int n, int L, const int *order, bool checkpoint,
+                       double2 *rot, double *lscale, double *gscale, cudaStream_t s) {
+  rot_kernel<<<L, 32, 0, s>>>(coef, n, L, order, checkpoint ? 1 : 0, rot, lscale, gscale);
   return cudaGetLastError();
 }
 

@@ -9,10 +9,11 @@
 namespace rsv {
 
 cudaError_t launch_coef(const double *params, double4 *coef, int count, cudaStream_t s);
+// prod holds 1 + partial.count tables of [4][256]
 cudaError_t launch_tables(const double4 *coef, int n, int L, double2 *ptab, double2 *prod,
-                          cudaStream_t s);
-cudaError_t launch_rot(const double4 *coef, int n, int L, const int *order, double2 *rot,
-                       double *lscale, double *gscale, cudaStream_t s);
+                          const PartialMasks &partial, cudaStream_t s);
+cudaError_t launch_rot(const double4 *coef, int n, int L, const int *order, bool checkpoint,
+                       double2 *rot, double *lscale, double *gscale, cudaStream_t s);
 cudaError_t configure_pass_kernels();
 size_t pass_smem_bytes(bool bwd);
 cudaError_t launch_pass(const PassParams &P, bool bwd, int grid, cudaStream_t s);

@@ -101,7 +101,76 @@ constexpr size_t kBwdSmem = 3 * kTileSize * sizeof(double2);
 constexpr size_t kFwdSmem = kTileSize * sizeof(double2);
 
 // ---------------------------------------------------------------- backward
-template <int LSRC, int PDST, int LDST, bool PHASE>
+// phi-gradient sums of the first backward pass of a layer without a CTA
+// barrier per tile.  In layout B0 (registers -> tile bits 9..11, lanes ->
+// 4..8, warps -> 0..3) every thread keeps, across its tiles, the sum of
+// q = Im(conj(lam) psi) and the sums over its registers with tile bit 9, 10,
+// 11 set (phi_thr, one column per thread); the coset bits of a tile are the
+// same for the whole tile, so each warp adds its tile sum to a warp-private
+// accumulator of every coset wire whose bit is set.  phi_reduce folds them
+// into phi_sm[w] (sum of q with wire-w bit 1) and phi_sm[32] (sum of q) once
+// per CTA.
+constexpr int kPhiThr = 4;  // per-thread accumulators: total, tile bits 9, 10, 11
+
+__device__ __forceinline__ void phi_accumulate(const PassParams &P, u32 cbase, int lane, int warp,
+                                               const double2 (&a)[bw::kR], const double2 (&b)[bw::kR],
+                                               double *phi_thr, double (*phi_cos)[32]) {
+  double v[kPhiThr] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int r = 0; r < bw::kR; ++r) {
+    const double q = fma(b[r].x, a[r].y, -b[r].y * a[r].x);
+    v[0] += q;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      if ((r >> j) & 1) v[1 + j] += q;
+  }
+#pragma unroll
+  for (int j = 0; j < kPhiThr; ++j) phi_thr[j * bw::kT] += v[j];
+  const double s = warp_sum(v[0]);  // every lane holds the warp's tile sum
+  if (lane < P.n && P.wire_tile_bit[lane] < 0 && ((cbase >> lane) & 1)) phi_cos[warp][lane] += s;
+}
+
+__device__ __forceinline__ void phi_reduce(const PassParams &P, int lane, int warp, const double *phi_thr,
+                                           double (*phi_cos)[32], double (*red)[12], double *phi_sm) {
+  double v[9];
+#pragma unroll
+  for (int j = 0; j < kPhiThr; ++j) v[j] = phi_thr[j * bw::kT];
+#pragma unroll
+  for (int j = 0; j < 5; ++j) v[4 + j] = ((lane >> j) & 1) ? v[0] : 0.0;
+#pragma unroll
+  for (int j = 0; j < 9; ++j) v[j] = warp_sum(v[j]);
+  if (lane == 0) {
+#pragma unroll
+    for (int j = 0; j < 9; ++j) red[warp][j] = v[j];
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int w = threadIdx.x;
+    double qt = 0.0;
+    for (int ww = 0; ww < 16; ++ww) qt += red[ww][0];
+    if (w < P.n) {
+      const int tb = P.wire_tile_bit[w];
+      double add = 0.0;
+      if (tb < 0) {
+        for (int ww = 0; ww < 16; ++ww) add += phi_cos[ww][w];
+      } else if (tb >= 9) {
+        for (int ww = 0; ww < 16; ++ww) add += red[ww][1 + tb - 9];
+      } else if (tb >= 4) {
+        for (int ww = 0; ww < 16; ++ww) add += red[ww][4 + tb - 4];
+      } else {
+        for (int ww = 0; ww < 16; ++ww)
+          if ((ww >> tb) & 1) add += red[ww][0];
+      }
+      phi_sm[w] = add;
+    }
+    if (w == 31) phi_sm[32] = qt;
+  }
+  __syncthreads();
+}
+
+// PSRC: kLoadNatural / kLoadGatherP (staged with lambda) or kLoadProductPlain
+// (analytic layer-0 psi from P.prod, computed in registers).
+template <int PSRC, int LSRC, int PDST, int LDST, bool PHASE>
 __global__ void __launch_bounds__(bw::kT, 1) bwd_pass_kernel(const PassParams P) {
   using namespace bw;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -110,6 +179,9 @@ __global__ void __launch_bounds__(bw::kT, 1) bwd_pass_kernel(const PassParams P)
   double2 *trans = stage_b + kTileSize;
   __shared__ double red[16][12];
   __shared__ double phi_sm[33];
+  __shared__ double2 km_sm[12];
+  __shared__ double phi_thr_sm[PHASE ? kPhiThr * bw::kT : 1];
+  __shared__ double phi_cos[PHASE ? 16 : 1][32];
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -129,14 +201,20 @@ __global__ void __launch_bounds__(bw::kT, 1) bwd_pass_kernel(const PassParams P)
   const u32 v3 = P.vec[3], v4 = P.vec[4], v5 = P.vec[5];
 
   double2 ratio[4];
-  u32 toffp = 0;
+  const u32 toffp = thread_offset(P, tpart<B0>(lane, warp));
   if (PHASE) {
-    toffp = thread_offset(P, tpart<B0>(lane, warp));
 #pragma unroll
     for (int j = 0; j < 3; ++j) ratio[j] = phase_ratio(P, unit_bit(P.vec[9 + j]));
     ratio[3] = make_double2(1.0, 0.0);
-    if (threadIdx.x < 33) phi_sm[threadIdx.x] = 0.0;
+#pragma unroll
+    for (int j = 0; j < kPhiThr; ++j) phi_thr_sm[j * kT + threadIdx.x] = 0.0;
+    phi_cos[warp][lane] = 0.0;
   }
+  if (threadIdx.x < 12) {
+    const int w = P.gate_wire[threadIdx.x];
+    km_sm[threadIdx.x] = w >= 0 ? RSV_TABLE_LOAD(&P.rot[P.layer * n + w]) : make_double2(0.0, 1.0);
+  }
+  __syncthreads();
   double acc[12];
 #pragma unroll
   for (int i = 0; i < 12; ++i) acc[i] = 0.0;
@@ -148,7 +226,7 @@ __global__ void __launch_bounds__(bw::kT, 1) bwd_pass_kernel(const PassParams P)
     for (int r = 0; r < kR; ++r) {
       const u32 p = base ^ ((r & 1) ? v9 : 0u) ^ ((r & 2) ? v10 : 0u) ^ ((r & 4) ? v11 : 0u);
       const int s = swz(tpi | (r << 9));
-      cp_async16(&stage_a[s], &P.psi_in[p]);
+      if (PSRC != kLoadProductPlain) cp_async16(&stage_a[s], &P.psi_in[source_index<PSRC>(p, n)]);
       cp_async16(&stage_b[s], &P.lam_in[source_index<LSRC>(p, n)]);
     }
     cp_async_commit();
@@ -163,37 +241,44 @@ __global__ void __launch_bounds__(bw::kT, 1) bwd_pass_kernel(const PassParams P)
 #pragma unroll
     for (int r = 0; r < kR; ++r) {
       const int s = swz(tb0 | (r << 9));
-      a[r] = stage_a[s];
+      if (PSRC != kLoadProductPlain) a[r] = stage_a[s];
       b[r] = stage_b[s];
     }
     __syncthreads();
     if (tile + gridDim.x < num_tiles) issue(tile + gridDim.x);
 
     const u32 cbase = deposit(P, tile);
+    if (PSRC == kLoadProductPlain) {
+      // layout B0: registers -> tile bits 9..11
+      const u32 base = cbase ^ toffp;
+#pragma unroll
+      for (int r = 0; r < kR; ++r)
+        a[r] = table4(P.prod, base ^ ((r & 1) ? v9 : 0u) ^ ((r & 2) ? v10 : 0u) ^ ((r & 4) ? v11 : 0u));
+    }
     if (PHASE) {
       // RZ^dagger of the layer (with the layer's factor K) on psi and lambda,
       // then the phi sums.
       const double2 ph = table4(P.ptab, cbase ^ toffp);
       const double K = P.lscale[P.layer];
       apply_phase_gray<3, true, true>(make_double2(K * ph.x, K * ph.y), ratio, a, b);
-      phi_sums(P, cbase, lane, warp, a, b, red, phi_sm);
+      phi_accumulate(P, cbase, lane, warp, a, b, phi_thr_sm + threadIdx.x, phi_cos);
     }
 
-    gates<B0>(P, a, b, acc);
+    gates<B0>(P, km_sm, a, b, acc);
     warp_transpose<B0, B1>(wbuf, lane, warp, a);
     warp_transpose<B0, B1>(wbuf, lane, warp, b);
-    gates<B1>(P, a, b, acc);
+    gates<B1>(P, km_sm, a, b, acc);
     if (has_lo) {
-      cta_transpose<B1, A1>(trans, lane, warp, a);
-      cta_transpose<B1, A1>(trans, lane, warp, b);
-      gates<A1>(P, a, b, acc);
+      cta_transpose2<B1, A1, true>(trans, lane, warp, a, b);
+      gates<A1>(P, km_sm, a, b, acc);
       warp_transpose<A1, A2>(wbuf, lane, warp, a);
       warp_transpose<A1, A2>(wbuf, lane, warp, b);
     } else {
-      cta_transpose<B1, A2>(trans, lane, warp, a);
-      cta_transpose<B1, A2>(trans, lane, warp, b);
+      // the next writer of the buffer (the next tile's warp transpose) comes
+      // after the staging barriers
+      cta_transpose2<B1, A2, false>(trans, lane, warp, a, b);
     }
-    gates<A2>(P, a, b, acc);
+    gates<A2>(P, km_sm, a, b, acc);
 
     if (PDST != kStoreNone || LDST != kStoreNone) {
       const u32 base = cbase ^ toffs;
@@ -221,6 +306,8 @@ __global__ void __launch_bounds__(bw::kT, 1) bwd_pass_kernel(const PassParams P)
     rec[threadIdx.x] = s;
   }
   if (PHASE) {
+    __syncthreads();  // red is reused
+    phi_reduce(P, lane, warp, phi_thr_sm + threadIdx.x, phi_cos, red, phi_sm);
     if (threadIdx.x < 31) rec[kPartialPhi + threadIdx.x] = phi_sm[threadIdx.x];
     if (threadIdx.x == 31) rec[kPartialTot] = phi_sm[32];
   }
@@ -276,9 +363,9 @@ __global__ void __launch_bounds__(kThreads, 2) fwd_pass_kernel(const PassParams 
   }
 }
 
-template <int LSRC, int PDST, int LDST, bool PHASE>
+template <int PSRC, int LSRC, int PDST, int LDST, bool PHASE>
 cudaError_t launch_bwd(const PassParams &P, int grid, cudaStream_t s) {
-  auto k = bwd_pass_kernel<LSRC, PDST, LDST, PHASE>;
+  auto k = bwd_pass_kernel<PSRC, LSRC, PDST, LDST, PHASE>;
   static bool configured = false;
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -308,27 +395,29 @@ cudaError_t launch_fwd(const PassParams &P, int grid, cudaStream_t s) {
 
 cudaError_t launch_pass(const PassParams &P, bool bwd, int grid, cudaStream_t s) {
   if (bwd) {
-    if (P.psi_load != kLoadNatural) return cudaErrorInvalidValue;
     const bool phase = P.phase != 0;
-    const bool gather = P.lam_load == kLoadGatherP;
-    if (P.lam_load != kLoadNatural && !gather) return cudaErrorInvalidValue;
     if (P.phi_grad != P.phase) return cudaErrorInvalidValue;
-    const int ps = P.psi_store, ls = P.lam_store;
-    // (psi, lambda) stores used by the planner: (natural, natural),
-    // (scatter P^-1, natural), (none, none)
-    if (ps == kStoreNatural && ls == kStoreNatural) {
-      if (phase) return gather ? launch_bwd<kLoadGatherP, kStoreNatural, kStoreNatural, true>(P, grid, s)
-                               : launch_bwd<kLoadNatural, kStoreNatural, kStoreNatural, true>(P, grid, s);
-      if (!gather) return launch_bwd<kLoadNatural, kStoreNatural, kStoreNatural, false>(P, grid, s);
-    } else if (ps == kStoreScatterPinv && ls == kStoreNatural) {
-      if (phase) return gather ? launch_bwd<kLoadGatherP, kStoreScatterPinv, kStoreNatural, true>(P, grid, s)
-                               : launch_bwd<kLoadNatural, kStoreScatterPinv, kStoreNatural, true>(P, grid, s);
-      if (!gather) return launch_bwd<kLoadNatural, kStoreScatterPinv, kStoreNatural, false>(P, grid, s);
-    } else if (ps == kStoreNone && ls == kStoreNone) {
-      if (phase) return gather ? launch_bwd<kLoadGatherP, kStoreNone, kStoreNone, true>(P, grid, s)
-                               : launch_bwd<kLoadNatural, kStoreNone, kStoreNone, true>(P, grid, s);
-      if (!gather) return launch_bwd<kLoadNatural, kStoreNone, kStoreNone, false>(P, grid, s);
-    }
+    const int pl = P.psi_load, ll = P.lam_load, ps = P.psi_store, ls = P.lam_store;
+    // The (psi source, lambda source, psi store, lambda store, phase) variants
+    // the two backward schedules use.
+#define RSV_BWD(PL, LL, PS, LS)                                                      \
+  if (pl == PL && ll == LL && ps == PS && ls == LS)                                  \
+    return phase ? launch_bwd<PL, LL, PS, LS, true>(P, grid, s)                      \
+                 : launch_bwd<PL, LL, PS, LS, false>(P, grid, s);
+    // uncompute schedule: psi streamed in and out
+    RSV_BWD(kLoadNatural, kLoadNatural, kStoreNatural, kStoreNatural)
+    RSV_BWD(kLoadNatural, kLoadGatherP, kStoreNatural, kStoreNatural)
+    RSV_BWD(kLoadNatural, kLoadNatural, kStoreScatterPinv, kStoreNatural)
+    RSV_BWD(kLoadNatural, kLoadGatherP, kStoreScatterPinv, kStoreNatural)
+    RSV_BWD(kLoadNatural, kLoadNatural, kStoreNone, kStoreNone)
+    RSV_BWD(kLoadNatural, kLoadGatherP, kStoreNone, kStoreNone)
+    // checkpoint schedule: psi read from a checkpoint (or analytic), only lambda written
+    RSV_BWD(kLoadNatural, kLoadNatural, kStoreNone, kStoreNatural)
+    RSV_BWD(kLoadGatherP, kLoadGatherP, kStoreNone, kStoreNatural)
+    RSV_BWD(kLoadProductPlain, kLoadGatherP, kStoreNone, kStoreNatural)
+    RSV_BWD(kLoadProductPlain, kLoadNatural, kStoreNone, kStoreNatural)
+    RSV_BWD(kLoadProductPlain, kLoadNatural, kStoreNone, kStoreNone)
+#undef RSV_BWD
     return cudaErrorInvalidValue;
   }
   const bool phase = P.phase != 0;

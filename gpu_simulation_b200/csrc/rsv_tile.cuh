@@ -186,6 +186,28 @@ __device__ __forceinline__ void cta_transpose(double2 *sm, int lane, int warp, d
   __syncthreads();
 }
 
+// Both vectors FROM -> TO through the CTA-wide buffer: one buffer, so the
+// second vector waits for every read of the first.  TRAIL = false drops the
+// closing barrier when the next writer of the buffer synchronises first.
+template <int FROM, int TO, bool TRAIL>
+__device__ __forceinline__ void cta_transpose2(double2 *sm, int lane, int warp, double2 (&a)[kR],
+                                               double2 (&b)[kR]) {
+  const int tf = tpart<FROM>(lane, warp), tt = tpart<TO>(lane, warp);
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kR; ++r) sm[swz(tf | (r << rbit<FROM>()))] = a[r];
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kR; ++r) a[r] = sm[swz(tt | (r << rbit<TO>()))];
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kR; ++r) sm[swz(tf | (r << rbit<FROM>()))] = b[r];
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kR; ++r) b[r] = sm[swz(tt | (r << rbit<TO>()))];
+  if (TRAIL) __syncthreads();
+}
+
 // Backward rotation of the three register bits of layout LY (tile bits
 // RB..RB+2): RY^dagger / f in tangent form, one FMA per component,
 //   mode +1: [[1,k],[-k,1]]    mode -1: [[k,1],[-1,k]],
@@ -193,15 +215,17 @@ __device__ __forceinline__ void cta_transpose(double2 *sm, int lane, int warp, d
 // pair in the frame with the layer's RZ removed -- the reference's
 // 2 Re<lam_mid|dRY|psi_before> (cpp/ising_cuda_statevector_grad_kernels.cu:289-307)
 // simplified; the factors f still pending are corrected in the final reduction.
+// km[tb]: the tangent form (k, mode) of the wire gated on tile bit tb, staged
+// in shared memory once per pass.
 template <int LY>
-__device__ __forceinline__ void gates(const PassParams &P, double2 (&a)[kR], double2 (&b)[kR],
-                                      double (&acc)[12]) {
+__device__ __forceinline__ void gates(const PassParams &P, const double2 *km_tb, double2 (&a)[kR],
+                                      double2 (&b)[kR], double (&acc)[12]) {
   constexpr int RB = rbit<LY>();
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
     const int w = P.gate_wire[RB + j];
     if (w < 0) continue;
-    const double2 km = RSV_TABLE_LOAD(&P.rot[P.layer * P.n + w]);
+    const double2 km = km_tb[RB + j];
     const double k = km.x;
     double t = acc[RB + j];
     if (km.y > 0.0) {

@@ -22,6 +22,19 @@ enum StoreMode : int {
   kStoreNone = 3,
 };
 
+// Undo-order entries (rot_kernel): wire id, plus this flag on the first wire of
+// a backward pass when the gradient correction restarts at every pass
+// (checkpoint schedule).
+constexpr int kUndoPassStart = 1 << 16;
+
+// Partial product tables of layer 0 (checkpoint schedule): at most this many,
+// each [4][256] after the full product table.
+constexpr int kMaxPartialTables = 4;
+struct PartialMasks {
+  int count;
+  unsigned int mask[kMaxPartialTables];  // wires whose RY / f is applied; the rest stay |0>
+};
+
 // Per-CTA partial record written by every backward pass (doubles):
 //   [0, 12)   theta partial sums per tile bit
 //   [16, 47)  phi: sum of Im(conj(lambda) psi) over amplitudes whose wire-w bit is 1
@@ -59,7 +72,7 @@ struct PassParams {
                                // or (k, -1) = [[k,-1],[1,k]] (k = cot t/2), RY divided by f
   const double *lscale;        // [L] product of the divided factors f of each layer
   const double2 *ptab;         // phase byte tables of this layer, [4][256]
-  const double2 *prod;         // layer-0 product-state byte tables, [4][256]
+  const double2 *prod;         // layer-0 product-state byte tables, [4][256] (full or partial)
   double *partials;            // [gridDim.x][kPartialStride] for this pass
 };
 

@@ -120,6 +120,22 @@ class Engine:
         return {name: {"launches": int(counts[i]), "ms": float(ms[i]), "bytes": float(by[i])}
                 for i, name in enumerate(self.KINDS)}
 
+    BACKWARD_MODES = {"auto": 0, "uncompute": 1, "checkpoint": 2}
+
+    def set_backward_mode(self, mode: str) -> None:
+        """Backward schedule: "uncompute" (three state buffers, psi un-computed
+        alongside lambda), "checkpoint" (psi read from forward checkpoints,
+        only lambda written) or "auto" (checkpoint while it fits)."""
+        if mode not in self.BACKWARD_MODES:
+            raise ValueError(f"backward mode must be one of {sorted(self.BACKWARD_MODES)}")
+        check(self._lib.rsv_set_backward_mode(self._h, self.BACKWARD_MODES[mode]))
+
+    def backward_mode(self) -> dict:
+        m, ck, nb = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(self._lib.rsv_backward_mode(self._h, ctypes.byref(m), ctypes.byref(ck), ctypes.byref(nb)))
+        names = {v: k for k, v in self.BACKWARD_MODES.items()}
+        return {"mode": names[m.value], "checkpoint": bool(ck.value), "state_buffers": nb.value}
+
     def set_field(self, field: float) -> None:
         """Change the transverse field h (same circuit shape and buffers)."""
         check(self._lib.rsv_set_field(self._h, float(field)))
@@ -131,10 +147,11 @@ class Engine:
         return int(v.value)
 
 
-def describe_plan(num_qubits: int, num_layers: int) -> str:
+def describe_plan(num_qubits: int, num_layers: int, backward_mode: str = "auto") -> str:
     """Launch schedule of one energy_and_grad call (host only, no GPU needed)."""
     lib = load_library()
     buf = ctypes.create_string_buffer(1 << 20)
     ln = ctypes.c_size_t()
-    check(lib.rsv_describe_plan(int(num_qubits), int(num_layers), buf, len(buf), ctypes.byref(ln)))
+    check(lib.rsv_describe_plan_mode(int(num_qubits), int(num_layers), Engine.BACKWARD_MODES[backward_mode],
+                                     buf, len(buf), ctypes.byref(ln)))
     return buf.value.decode()

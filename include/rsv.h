@@ -175,6 +175,26 @@ rsv_status rsv_set_launch_timing(rsv_backend *backend, int enable);
 rsv_status rsv_launch_stats(rsv_backend *backend, int *counts, double *total_ms,
                             double *total_bytes);
 
+/*
+ * Backward schedule.  RSV_BACKWARD_UNCOMPUTE keeps three state buffers and
+ * un-computes psi alongside lambda (the reference's schedule,
+ * cpp/ising_cuda_structured_adjoint_modes.inc:188-307).  RSV_BACKWARD_CHECKPOINT
+ * keeps the state after every forward pass (max((L-1) * passes + 1, 2)
+ * buffers of 16 * 2^n bytes; passes = 3 for 20 <= n <= 31) so that the
+ * backward reads psi and writes only lambda.
+ * RSV_BACKWARD_AUTO (the default of rsv_create) picks the checkpoint schedule
+ * for n >= 13 while its buffers fit 96 GiB (and its allocation succeeds).
+ * rsv_set_backward_mode re-plans and reallocates (synchronises the backend's
+ * stream); rsv_backward_mode reports the mode, whether the checkpoint schedule
+ * is in use and the number of state buffers.  No reference counterpart.
+ */
+#define RSV_BACKWARD_AUTO 0
+#define RSV_BACKWARD_UNCOMPUTE 1
+#define RSV_BACKWARD_CHECKPOINT 2
+rsv_status rsv_set_backward_mode(rsv_backend *backend, int mode);
+rsv_status rsv_backward_mode(rsv_backend *backend, int *mode_out, int *checkpoint_out,
+                             int *num_buffers_out);
+
 /* Change the transverse field h of an existing backend (the circuit shape and
  * buffers stay).  No reference counterpart (its field is fixed at
  * construction, cpp/ising_cuda_backend.hpp:26-29). */
@@ -195,6 +215,9 @@ rsv_status rsv_backend_info(rsv_backend *backend, int *num_qubits, int *num_laye
  */
 rsv_status rsv_describe_plan(int num_qubits, int num_layers, char *buf, size_t buf_size,
                              size_t *length_out);
+/* The same for a given backward schedule (RSV_BACKWARD_*). */
+rsv_status rsv_describe_plan_mode(int num_qubits, int num_layers, int backward_mode, char *buf,
+                                  size_t buf_size, size_t *length_out);
 
 /*
  * Host-only reference of the engine's ring-CNOT index maps (P and P^-1),

@@ -22,11 +22,14 @@ import numpy as np
 from gpu_simulation_b200._lib import load_library
 
 
-def describe_plan(n: int, layers: int) -> str:
+AUTO, UNCOMPUTE, CHECKPOINT = 0, 1, 2  # RSV_BACKWARD_* of include/rsv.h
+
+
+def describe_plan(n: int, layers: int, mode: int = AUTO) -> str:
     lib = load_library()
     buf = ctypes.create_string_buffer(1 << 20)
     ln = ctypes.c_size_t()
-    rc = lib.rsv_describe_plan(n, layers, buf, len(buf), ctypes.byref(ln))
+    rc = lib.rsv_describe_plan_mode(n, layers, mode, buf, len(buf), ctypes.byref(ln))
     if rc != 0:
         raise ValueError(lib.rsv_last_error().decode())
     return buf.value.decode()
@@ -71,7 +74,7 @@ def parse_plan(text: str) -> dict:
             phase=" phase" in m["flags"], phi=" phi" in m["flags"], grid=int(m["grid"]),
         ))
     return dict(n=int(head["n"]), L=int(head["L"]), phys=int(head["phys"]), steps=steps,
-                energy=energy)
+                energy=energy, bufs=int(head["bufs"]), mode=head["mode"])
 
 
 def ring_p(i: np.ndarray, n: int) -> np.ndarray:
@@ -135,9 +138,10 @@ def check_pair_roles(step: dict, n: int) -> None:
             raise AssertionError(f"pair roles of wire {w} disagree with the kernel rule: {step}")
 
 
-def simulate(n: int, layers: int, field: float, params: np.ndarray, check_indices: bool = True):
+def simulate(n: int, layers: int, field: float, params: np.ndarray, check_indices: bool = True,
+             mode: int = AUTO):
     """Run the plan with numpy.  Returns (energy, gradient flat f64[2nL])."""
-    plan = parse_plan(describe_plan(n, layers))
+    plan = parse_plan(describe_plan(n, layers, mode))
     phys = plan["phys"]
     size = 1 << phys
     p = np.asarray(params, dtype=np.float64).reshape(layers, n, 2)
@@ -164,9 +168,22 @@ def simulate(n: int, layers: int, field: float, params: np.ndarray, check_indice
                 amp *= np.where(b == 1, 0.0, 1.0)
         return amp
 
-    bufs = [np.zeros(size, dtype=np.complex128) for _ in range(3)]
+    def partial(j, mask):
+        # layer-0 product state with only the wires in `mask` rotated (RY, no RZ)
+        amp = np.ones(j.shape, dtype=np.complex128)
+        for w in range(n):
+            b = (j >> w) & 1
+            if (mask >> w) & 1:
+                amp *= np.where(b == 1, s[0, w], c[0, w])
+            else:
+                amp *= np.where(b == 1, 0.0, 1.0)
+        return amp
+
+    bufs = [np.zeros(size, dtype=np.complex128) for _ in range(plan["bufs"])]
 
     def load(mode, bid):
+        if mode.startswith("partial("):
+            return partial(idx, int(mode[len("partial("):-1], 16))
         if mode == "load":
             return bufs[bid].copy()
         if mode == "gatherP":

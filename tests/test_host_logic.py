@@ -61,19 +61,33 @@ def test_ring_map_matches_oracle_closed_form():
 def test_plan_executed_in_numpy_matches_oracle(n, L, h):
     rng = np.random.default_rng(100 + n * 10 + L)
     p = rng.uniform(0, 2 * np.pi, 2 * n * L)
-    e_sim, g_sim = plan_sim.simulate(n, L, h, p)
     e_ref, g_ref = oracle.energy_and_grad(n, L, h, p)
-    assert abs(e_sim - e_ref) < 1e-11
-    np.testing.assert_allclose(g_sim, g_ref, atol=1e-11, rtol=0)
+    for mode in (plan_sim.UNCOMPUTE, plan_sim.CHECKPOINT):
+        e_sim, g_sim = plan_sim.simulate(n, L, h, p, mode=mode)
+        assert abs(e_sim - e_ref) < 1e-11
+        np.testing.assert_allclose(g_sim, g_ref, atol=1e-11, rtol=0)
 
 
-@pytest.mark.parametrize("n,L", [(20, 4), (24, 4), (28, 4), (30, 4), (31, 2)])
-def test_large_plans_cover_every_wire_once_with_three_buffers(n, L):
-    plan = plan_sim.parse_plan(describe_plan(n, L))
+@pytest.mark.parametrize("n,L", [(20, 4), (24, 4), (28, 4), (30, 4), (31, 2), (28, 9)])
+def test_large_plans_cover_every_wire_once(n, L):
+    for mode in (plan_sim.AUTO, plan_sim.UNCOMPUTE, plan_sim.CHECKPOINT):
+        plan = plan_sim.parse_plan(plan_sim.describe_plan(n, L, mode))
+        check_large_plan(plan, n, L)
+    # automatic choice: the checkpoint schedule while its buffers fit 96 GiB
+    auto = plan_sim.parse_plan(describe_plan(n, L))
+    ck = plan_sim.parse_plan(plan_sim.describe_plan(n, L, plan_sim.CHECKPOINT))
+    fits = ck["bufs"] * 16 * 2 ** n <= 96 * 2 ** 30
+    assert auto["mode"] == ("checkpoint" if fits else "uncompute")
+    assert plan_sim.parse_plan(plan_sim.describe_plan(n, L, plan_sim.UNCOMPUTE))["bufs"] == 3
+
+
+def check_large_plan(plan, n, L):
     seen = {}
     for st in plan["steps"]:
         for b in ("psi_in", "psi_out", "lam_in", "lam_out"):
-            assert st[b] in (-1, 0, 1, 2)
+            assert -1 <= st[b] < plan["bufs"]
+        if plan["mode"] == "checkpoint" and st["bwd"]:
+            assert st["psi_store"] == "none"
         if st["bwd"]:
             for w in st["gates"]:
                 key = (st["layer"], w)
