@@ -8,6 +8,8 @@ Public surface
                                     torch.autograd.Function (backward = adjoint kernels)
   * ``describe_plan``               launch schedule of one call (host only)
   * ``BatchEngine``                 thousands of independent circuits per kernel launch
+  * ``training.run_standalone``     device-resident gradient-descent loop (CUDA-graph steps)
+  * ``warmstart``                   learned warm start (FP32 network, own kernels)
 
 The compiled pieces are built in-tree by ``python -m gpu_simulation_b200.build``.
 """

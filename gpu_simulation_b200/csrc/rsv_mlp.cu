@@ -150,6 +150,40 @@ __global__ void adam_kernel(long long count, T *__restrict__ p, const T *__restr
   }
 }
 
+// One plain gradient-descent step of the VQE loop, device resident (the
+// reference's apply_gradient_step, ring_ising/workflows/common.py:23-25, and
+// the per-step metrics of run_gradient_descent_loop,
+// ring_ising/training/loop.py:93-115): p -= stepsize * g; the step's energy
+// and |g| are appended to the histories at *counter, which is then
+// incremented (so one captured step can be replayed).  One CTA: the norm is
+// reduced in a fixed order.
+constexpr int kGdThreads = 256;
+__global__ void __launch_bounds__(kGdThreads) gd_step_kernel(long long count, double *__restrict__ p,
+                                                            const double *__restrict__ g, double stepsize,
+                                                            const double *__restrict__ energy,
+                                                            double *__restrict__ energy_hist,
+                                                            double *__restrict__ gnorm_hist, int *counter) {
+  __shared__ double red[kGdThreads];
+  double s = 0.0;
+  for (long long i = threadIdx.x; i < count; i += kGdThreads) {
+    const double gi = g[i];
+    s = fma(gi, gi, s);
+    p[i] = __dsub_rn(p[i], __dmul_rn(stepsize, gi));  // params - stepsize * grad, no contraction
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = kGdThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const int k = *counter;
+    if (energy_hist) energy_hist[k] = *energy;
+    if (gnorm_hist) gnorm_hist[k] = sqrt(red[0]);
+    *counter = k + 1;
+  }
+}
+
 int elementwise_grid(long long count) {
   const long long b = (count + 255) / 256;
   return static_cast<int>(b < 1 ? 1 : (b > 4096 ? 4096 : b));
@@ -203,6 +237,12 @@ cudaError_t adam_step(long long count, T *p, const T *g, T *m, T *v, T lr, T bet
   const T corr2 = T(1) - pow(beta2, static_cast<T>(step));
   adam_kernel<T><<<elementwise_grid(count), 256, 0, s>>>(count, p, g, m, v, lr, beta1, beta2, eps,
                                                          corr1, corr2);
+  return cudaGetLastError();
+}
+
+cudaError_t gd_step(long long count, double *p, const double *g, double stepsize, const double *energy,
+                    double *energy_hist, double *gnorm_hist, int *counter, cudaStream_t s) {
+  gd_step_kernel<<<1, kGdThreads, 0, s>>>(count, p, g, stepsize, energy, energy_hist, gnorm_hist, counter);
   return cudaGetLastError();
 }
 

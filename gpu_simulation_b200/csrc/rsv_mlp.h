@@ -17,6 +17,8 @@ cudaError_t mlp_colsum(int M, int N, const float *dZ, float *db, cudaStream_t s)
 int mlp_loss_blocks(long long count);
 cudaError_t mlp_mse(long long count, const float *out, const float *target, float *dout,
                     float *partials, float *loss, cudaStream_t s);
+cudaError_t gd_step(long long count, double *p, const double *g, double stepsize, const double *energy,
+                    double *energy_hist, double *gnorm_hist, int *counter, cudaStream_t s);
 template <typename T>
 cudaError_t adam_step(long long count, T *p, const T *g, T *m, T *v, T lr, T beta1, T beta2, T eps,
                       int step, cudaStream_t s);

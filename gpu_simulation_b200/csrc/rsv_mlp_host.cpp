@@ -195,4 +195,16 @@ rsv_status rsv_adam_f64(double *d_p, const double *d_g, double *d_m, double *d_v
   });
 }
 
+rsv_status rsv_gd_step_f64(double *d_params, const double *d_grad, size_t count, double stepsize,
+                           const double *d_energy, double *d_energy_hist, double *d_gnorm_hist,
+                           int *d_step_counter, void *stream) {
+  return mlp_guarded([&] {
+    if (!d_params || !d_grad || !d_energy || !d_step_counter) throw ArgError("null device pointer");
+    if (!std::isfinite(stepsize)) throw ArgError("stepsize is not finite");
+    cuda_check(gd_step(static_cast<long long>(count), d_params, d_grad, stepsize, d_energy, d_energy_hist,
+                       d_gnorm_hist, d_step_counter, static_cast<cudaStream_t>(stream)),
+               "gradient step");
+  });
+}
+
 }  // extern "C"

@@ -313,6 +313,19 @@ rsv_status rsv_adam_f64(double *d_params, const double *d_grad, double *d_m, dou
                         size_t count, double lr, double beta1, double beta2, double eps, int step,
                         void *stream);
 
+/*
+ * One plain gradient-descent step of a device-resident VQE loop: d_params -=
+ * stepsize * d_grad (count values); the step's energy (*d_energy) and gradient
+ * norm are stored at index *d_step_counter of d_energy_hist / d_gnorm_hist
+ * (either may be NULL), then *d_step_counter is incremented, so one captured
+ * (energy_and_grad, gd_step) pair can be replayed as a CUDA graph.  Replaces
+ * the host-side update of the reference's training loop
+ * (ring_ising/workflows/common.py:23-25, ring_ising/training/loop.py:93-115).
+ */
+rsv_status rsv_gd_step_f64(double *d_params, const double *d_grad, size_t count, double stepsize,
+                           const double *d_energy, double *d_energy_hist, double *d_gnorm_hist,
+                           int *d_step_counter, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

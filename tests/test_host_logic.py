@@ -151,3 +151,11 @@ def test_batch_sharding_and_synthetic_batch():
         if world > 1:
             loads = np.array([cost[p].sum() for p in parts])
             assert loads.max() - loads.min() <= 2 * cost.max()
+
+
+def test_initial_params_follow_the_reference_recipe():
+    from gpu_simulation_b200.training import make_initial_params
+
+    p = make_initial_params(8, 2, 7, 0.3)
+    assert p.shape == (2, 8, 2) and p.dtype == np.float64
+    np.testing.assert_array_equal(p, 0.3 * np.random.default_rng(7).standard_normal((2, 8, 2)))
