@@ -25,6 +25,7 @@
 
 #include "../../include/rsv.h"
 #include "rsv_batch.h"
+#include "rsv_gate.h"
 #include "rsv_device.cuh"
 #include "rsv_launch.h"
 #include "rsv_types.h"
@@ -600,6 +601,10 @@ struct rsv_backend {
   rsv::Plan plan;
   rsv::DevBuf<double2> states;  // plan.num_bufs state buffers of state_len amplitudes each
   int backward_mode = RSV_BACKWARD_AUTO;
+  // gradient_strategy "inverse_walk_cuQuantum": gate-level kernels (rsv_gate.cu)
+  bool gate_level = false;
+  int gate_grid = 1;
+  rsv::DevBuf<double> gate_partials;  // [1 + 2 n L][gate_grid]
   rsv::DevBuf<double4> coef;
   rsv::DevBuf<double2> ptab, prod;
   rsv::DevBuf<double> energy_partials, pass_partials, outputs;  // outputs: [1 + num_params]
@@ -832,9 +837,31 @@ void launch_prep(rsv_backend *B, cudaStream_t st) {
   });
 }
 
+// Gate-level path: RY, RZ and CNOT as separate kernels and the inverse walk
+// (the reference's inverse_walk_cuQuantum schedule without cuStateVec).
+void run_gate_level(rsv_backend *B, bool grad, double *energy_out, double *grad_out, cudaStream_t st) {
+  GateLevelArgs A{};
+  A.n = B->n;
+  A.L = B->L;
+  A.field = B->field;
+  A.coef = B->coef.p;
+  A.psi = state_buf(B, 0);
+  A.lam = state_buf(B, 1);
+  A.grid = B->gate_grid;
+  A.energy_partials = B->gate_partials.p;
+  A.grad_partials = B->gate_partials.p + B->gate_grid;
+  A.energy_out = energy_out;
+  A.grad_out = grad ? grad_out : nullptr;
+  check(rsv::run_gate_level(A, st), "gate-level launch");
+}
+
 void run_all(rsv_backend *B, bool grad, double *energy_out, double *grad_out, cudaStream_t st) {
   ++B->generation;
   B->forward_only_state = false;
+  if (B->gate_level) {
+    run_gate_level(B, grad, energy_out, grad_out, st);
+    return;
+  }
   launch_prep(B, st);
   run_forward(B, st);
   run_energy(B, st);
@@ -1282,6 +1309,11 @@ rsv_status rsv_create(int num_qubits, int num_layers, double field, const char *
     }
     setup_plan(B.get(), RSV_BACKWARD_AUTO);
     const size_t nl = static_cast<size_t>(num_qubits) * num_layers;
+    if (strat == "inverse_walk_cuQuantum" || strat == "inverse_walk_cuquantum") {
+      B->gate_level = true;
+      B->gate_grid = gate_grid(num_qubits, B->sms);
+      B->gate_partials.alloc(static_cast<size_t>(B->gate_grid) * (1 + 2 * nl));
+    }
     B->coef.alloc(nl);
     B->ptab.alloc(static_cast<size_t>(num_layers) * 1024);
     B->energy_grid = static_cast<int>(std::min<u64>(
@@ -1396,15 +1428,24 @@ rsv_status rsv_profile_energy_and_grad(rsv_backend *B, const double *params, siz
     ++B->generation;
     B->forward_only_state = false;
     cudaEventRecord(ev[0], st);
-    launch_prep(B, st);
-    cudaEventRecord(ev[1], st);
-    run_forward(B, st);
-    cudaEventRecord(ev[2], st);
-    run_energy(B, st);
-    cudaEventRecord(ev[3], st);
-    if (grad) run_backward(B, st);
-    cudaEventRecord(ev[4], st);
-    run_finalize(B, grad, B->outputs.p, B->outputs.p + 1, st);
+    if (B->gate_level) {
+      // one stage: the gate-level walk is not split into these phases
+      cudaEventRecord(ev[1], st);
+      run_gate_level(B, grad, B->outputs.p, B->outputs.p + 1, st);
+      cudaEventRecord(ev[2], st);
+      cudaEventRecord(ev[3], st);
+      cudaEventRecord(ev[4], st);
+    } else {
+      launch_prep(B, st);
+      cudaEventRecord(ev[1], st);
+      run_forward(B, st);
+      cudaEventRecord(ev[2], st);
+      run_energy(B, st);
+      cudaEventRecord(ev[3], st);
+      if (grad) run_backward(B, st);
+      cudaEventRecord(ev[4], st);
+      run_finalize(B, grad, B->outputs.p, B->outputs.p + 1, st);
+    }
     const size_t count = grad ? 1 + B->num_params : 1;
     check(cudaMemcpyAsync(B->out_host.p, B->outputs.p, count * sizeof(double),
                           cudaMemcpyDeviceToHost, st),

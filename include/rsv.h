@@ -58,9 +58,12 @@ const char *rsv_stage_name(int i);
  * Replaces RingIsingCudaBackend::RingIsingCudaBackend
  * (reference cpp/ising_cuda_backend.hpp:26-29, cpp/ising_cuda_backend.cu:388-404,
  *  bound at cpp/ising_cuda_bindings.cpp:74-80).
- * gradient_strategy: "structured_adjoint", "inverse_walk_cuQuantum" (alias
- * "inverse_walk_cuquantum") or "dense_scan"; all run the structured engine
- * (their results agree to rounding).  structured_rotation_chunk_width must be
+ * gradient_strategy: "structured_adjoint" (tile-pass engine),
+ * "inverse_walk_cuQuantum" (alias "inverse_walk_cuquantum": RY, RZ and CNOT as
+ * separate kernels and the gate-level adjoint walk, without cuStateVec) or
+ * "dense_scan" (runs the structured engine); results agree to rounding.  The
+ * split device entry points (rsv_forward_device / rsv_backward_device) and
+ * rsv_benchmark_forward_graph always run the tile-pass engine.  structured_rotation_chunk_width must be
  * in [1, 8] and double_buffer is accepted; both are validated as the
  * reference does and otherwise ignored (the engine plans its own tiles).
  * Allocates three state buffers of 16 * 2^max(n,12) bytes.
