@@ -45,6 +45,8 @@ _SIGNATURES = {
     "rsv_launch_stats": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
                          ctypes.c_int),
     "rsv_set_field": ([ctypes.c_void_p, ctypes.c_double], ctypes.c_int),
+    "rsv_zgemm_batched": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                           ctypes.c_void_p], ctypes.c_int),
     "rsv_set_backward_mode": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "rsv_backward_mode": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                            ctypes.POINTER(ctypes.c_int)], ctypes.c_int),

@@ -25,6 +25,7 @@
 
 #include "../../include/rsv.h"
 #include "rsv_batch.h"
+#include "rsv_dense.h"
 #include "rsv_gate.h"
 #include "rsv_device.cuh"
 #include "rsv_launch.h"
@@ -605,6 +606,9 @@ struct rsv_backend {
   bool gate_level = false;
   int gate_grid = 1;
   rsv::DevBuf<double> gate_partials;  // [1 + 2 n L][gate_grid]
+  // gradient_strategy "dense_scan" (n <= 8): dense layer products (rsv_dense.cu)
+  bool dense = false;
+  rsv::DevBuf<double2> dense_work;
   rsv::DevBuf<double4> coef;
   rsv::DevBuf<double2> ptab, prod;
   rsv::DevBuf<double> energy_partials, pass_partials, outputs;  // outputs: [1 + num_params]
@@ -860,6 +864,18 @@ void run_all(rsv_backend *B, bool grad, double *energy_out, double *grad_out, cu
   B->forward_only_state = false;
   if (B->gate_level) {
     run_gate_level(B, grad, energy_out, grad_out, st);
+    return;
+  }
+  if (B->dense) {
+    DenseArgs D{};
+    D.n = B->n;
+    D.L = B->L;
+    D.field = B->field;
+    D.coef = B->coef.p;
+    D.work = B->dense_work.p;
+    D.energy_out = energy_out;
+    D.grad_out = grad ? grad_out : nullptr;
+    check(run_dense_scan(D, st), "dense_scan launch");
     return;
   }
   launch_prep(B, st);
@@ -1309,6 +1325,10 @@ rsv_status rsv_create(int num_qubits, int num_layers, double field, const char *
     }
     setup_plan(B.get(), RSV_BACKWARD_AUTO);
     const size_t nl = static_cast<size_t>(num_qubits) * num_layers;
+    if (strat == "dense_scan") {
+      B->dense = true;
+      B->dense_work.alloc(dense_workspace_bytes(num_qubits, num_layers) / sizeof(double2));
+    }
     if (strat == "inverse_walk_cuQuantum" || strat == "inverse_walk_cuquantum") {
       B->gate_level = true;
       B->gate_grid = gate_grid(num_qubits, B->sms);
@@ -1428,10 +1448,11 @@ rsv_status rsv_profile_energy_and_grad(rsv_backend *B, const double *params, siz
     ++B->generation;
     B->forward_only_state = false;
     cudaEventRecord(ev[0], st);
-    if (B->gate_level) {
-      // one stage: the gate-level walk is not split into these phases
+    if (B->gate_level || B->dense) {
+      // one stage: these schedules are not split into the phases below
       cudaEventRecord(ev[1], st);
-      run_gate_level(B, grad, B->outputs.p, B->outputs.p + 1, st);
+      --B->generation;  // run_all counts the call
+      run_all(B, grad, B->outputs.p, B->outputs.p + 1, st);
       cudaEventRecord(ev[2], st);
       cudaEventRecord(ev[3], st);
       cudaEventRecord(ev[4], st);
@@ -1560,6 +1581,18 @@ rsv_status rsv_backward_mode(rsv_backend *B, int *mode_out, int *checkpoint_out,
     if (mode_out) *mode_out = B->backward_mode;
     if (checkpoint_out) *checkpoint_out = B->plan.checkpoint ? 1 : 0;
     if (num_buffers_out) *num_buffers_out = B->plan.num_bufs;
+  });
+}
+
+rsv_status rsv_zgemm_batched(const void *d_a, const void *d_b, void *d_c, int dim, int batch, void *stream) {
+  return guarded([&] {
+    if (dim < 1 || dim > 4096 || batch < 1) invalid("dim must be in [1, 4096] and batch positive");
+    if (dim >= 32 && dim % 32 != 0) invalid("dim >= 32 must be a multiple of 32");
+    if (!d_a || !d_b || !d_c) invalid("null device pointer");
+    const long long mat = static_cast<long long>(dim) * dim;
+    check(zgemm_batched(static_cast<const double2 *>(d_a), static_cast<const double2 *>(d_b),
+                        static_cast<double2 *>(d_c), dim, batch, mat, mat, mat, static_cast<cudaStream_t>(stream)),
+          "zgemm launch");
   });
 }
 

@@ -61,11 +61,12 @@ const char *rsv_stage_name(int i);
  * gradient_strategy: "structured_adjoint" (tile-pass engine),
  * "inverse_walk_cuQuantum" (alias "inverse_walk_cuquantum": RY, RZ and CNOT as
  * separate kernels and the gate-level adjoint walk, without cuStateVec) or
- * "dense_scan" (runs the structured engine); results agree to rounding.  The
- * split device entry points (rsv_forward_device / rsv_backward_device) and
- * rsv_benchmark_forward_graph always run the tile-pass engine.  structured_rotation_chunk_width must be
- * in [1, 8] and double_buffer is accepted; both are validated as the
- * reference does and otherwise ignored (the engine plans its own tiles).
+ * "dense_scan" (n <= 8: dense layer matrices, product tree on FP64 tensor
+ * cores); results agree to rounding.  The split device entry points
+ * (rsv_forward_device / rsv_backward_device) and rsv_benchmark_forward_graph
+ * always run the tile-pass engine.  structured_rotation_chunk_width must be in
+ * [1, 8] and double_buffer is accepted; both are validated as the reference
+ * does and otherwise ignored (the engine plans its own tiles).
  * Allocates three state buffers of 16 * 2^max(n,12) bytes.
  */
 rsv_status rsv_create(int num_qubits, int num_layers, double field,
@@ -197,6 +198,15 @@ rsv_status rsv_launch_stats(rsv_backend *backend, int *counts, double *total_ms,
 rsv_status rsv_set_backward_mode(rsv_backend *backend, int mode);
 rsv_status rsv_backward_mode(rsv_backend *backend, int *mode_out, int *checkpoint_out,
                              int *num_buffers_out);
+
+/*
+ * Batched complex128 GEMM on FP64 tensor cores (mma.sync f64; the dense_scan
+ * product tree uses it): C[b] = A[b] B[b] for b < batch, every matrix dim x dim
+ * row-major and the batches contiguous; dim < 32 or a multiple of 32.  Device
+ * pointers, asynchronous on `stream`.  Replaces the reference's
+ * cublasZgemmStridedBatched calls (cpp/ising_cuda_dense_modes.inc:124-138).
+ */
+rsv_status rsv_zgemm_batched(const void *d_a, const void *d_b, void *d_c, int dim, int batch, void *stream);
 
 /* Change the transverse field h of an existing backend (the circuit shape and
  * buffers stay).  No reference counterpart (its field is fixed at
