@@ -244,8 +244,8 @@ __global__ void __launch_bounds__(bw::kT, 1) bwd_pass_kernel(const PassParams P)
       if (PSRC != kLoadProductPlain) a[r] = stage_a[s];
       b[r] = stage_b[s];
     }
-    __syncthreads();
-    if (tile + gridDim.x < num_tiles) issue(tile + gridDim.x);
+    // the staging buffers stay free until the CTA-wide transpose below has
+    // used them; the next tile is prefetched right after it
 
     const u32 cbase = deposit(P, tile);
     if (PSRC == kLoadProductPlain) {
@@ -269,14 +269,14 @@ __global__ void __launch_bounds__(bw::kT, 1) bwd_pass_kernel(const PassParams P)
     warp_transpose<B0, B1>(wbuf, lane, warp, b);
     gates<B1>(P, km_sm, a, b, acc);
     if (has_lo) {
-      cta_transpose2<B1, A1, true>(trans, lane, warp, a, b);
+      cta_transpose_pair<B1, A1>(stage_a, stage_b, lane, warp, a, b);
+      if (tile + gridDim.x < num_tiles) issue(tile + gridDim.x);
       gates<A1>(P, km_sm, a, b, acc);
       warp_transpose<A1, A2>(wbuf, lane, warp, a);
       warp_transpose<A1, A2>(wbuf, lane, warp, b);
     } else {
-      // the next writer of the buffer (the next tile's warp transpose) comes
-      // after the staging barriers
-      cta_transpose2<B1, A2, false>(trans, lane, warp, a, b);
+      cta_transpose_pair<B1, A2>(stage_a, stage_b, lane, warp, a, b);
+      if (tile + gridDim.x < num_tiles) issue(tile + gridDim.x);
     }
     gates<A2>(P, km_sm, a, b, acc);
 

@@ -208,6 +208,30 @@ __device__ __forceinline__ void cta_transpose2(double2 *sm, int lane, int warp, 
   if (TRAIL) __syncthreads();
 }
 
+// Both vectors FROM -> TO at once through two CTA-wide buffers (the staging
+// buffers of the backward pass, free between reading a tile and prefetching
+// the next): three barriers for the pair.
+template <int FROM, int TO>
+__device__ __forceinline__ void cta_transpose_pair(double2 *sa, double2 *sb, int lane, int warp,
+                                                   double2 (&a)[kR], double2 (&b)[kR]) {
+  const int tf = tpart<FROM>(lane, warp), tt = tpart<TO>(lane, warp);
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kR; ++r) {
+    const int s = swz(tf | (r << rbit<FROM>()));
+    sa[s] = a[r];
+    sb[s] = b[r];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kR; ++r) {
+    const int s = swz(tt | (r << rbit<TO>()));
+    a[r] = sa[s];
+    b[r] = sb[s];
+  }
+  __syncthreads();
+}
+
 // Backward rotation of the three register bits of layout LY (tile bits
 // RB..RB+2): RY^dagger / f in tangent form, one FMA per component,
 //   mode +1: [[1,k],[-k,1]]    mode -1: [[k,1],[-1,k]],
