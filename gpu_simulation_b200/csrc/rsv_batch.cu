@@ -144,8 +144,8 @@ __device__ void run_pass(const PassParams &P, Shared &S, int lane, int warp, dou
         a[r] = S.stage_a[s];
         if (BWD) b[r] = S.stage_b[s];
       }
-      __syncthreads();
-      if (tile + 1 < num_tiles) issue(tile + 1);
+      // the staging buffers now serve the CTA-wide transpose below; the next
+      // tile is prefetched right after it
     } else {
       const u32 base = cbase ^ toffb0;
 #pragma unroll
@@ -166,14 +166,16 @@ __device__ void run_pass(const PassParams &P, Shared &S, int lane, int warp, dou
     if (BWD) warp_transpose<B0, B1>(wbuf, lane, warp, b);
     if (BWD) gates<B1>(P, S.km, a, b, acc); else fgates<B1>(P, S.km, a);
     if (has_lo) {
-      cta_transpose<B1, A1>(S.trans, lane, warp, a);
-      if (BWD) cta_transpose<B1, A1>(S.trans, lane, warp, b);
+      if (BWD) cta_transpose_pair<B1, A1>(S.stage_a, S.stage_b, lane, warp, a, b);
+      else cta_transpose<B1, A1>(S.stage_a, lane, warp, a);
+      if (staged && tile + 1 < num_tiles) issue(tile + 1);
       if (BWD) gates<A1>(P, S.km, a, b, acc); else fgates<A1>(P, S.km, a);
       warp_transpose<A1, A2>(wbuf, lane, warp, a);
       if (BWD) warp_transpose<A1, A2>(wbuf, lane, warp, b);
     } else {
-      cta_transpose<B1, A2>(S.trans, lane, warp, a);
-      if (BWD) cta_transpose<B1, A2>(S.trans, lane, warp, b);
+      if (BWD) cta_transpose_pair<B1, A2>(S.stage_a, S.stage_b, lane, warp, a, b);
+      else cta_transpose<B1, A2>(S.stage_a, lane, warp, a);
+      if (staged && tile + 1 < num_tiles) issue(tile + 1);
     }
     if (BWD) gates<A2>(P, S.km, a, b, acc); else fgates<A2>(P, S.km, a);
 

@@ -186,28 +186,6 @@ __device__ __forceinline__ void cta_transpose(double2 *sm, int lane, int warp, d
   __syncthreads();
 }
 
-// Both vectors FROM -> TO through the CTA-wide buffer: one buffer, so the
-// second vector waits for every read of the first.  TRAIL = false drops the
-// closing barrier when the next writer of the buffer synchronises first.
-template <int FROM, int TO, bool TRAIL>
-__device__ __forceinline__ void cta_transpose2(double2 *sm, int lane, int warp, double2 (&a)[kR],
-                                               double2 (&b)[kR]) {
-  const int tf = tpart<FROM>(lane, warp), tt = tpart<TO>(lane, warp);
-  __syncthreads();
-#pragma unroll
-  for (int r = 0; r < kR; ++r) sm[swz(tf | (r << rbit<FROM>()))] = a[r];
-  __syncthreads();
-#pragma unroll
-  for (int r = 0; r < kR; ++r) a[r] = sm[swz(tt | (r << rbit<TO>()))];
-  __syncthreads();
-#pragma unroll
-  for (int r = 0; r < kR; ++r) sm[swz(tf | (r << rbit<FROM>()))] = b[r];
-  __syncthreads();
-#pragma unroll
-  for (int r = 0; r < kR; ++r) b[r] = sm[swz(tt | (r << rbit<TO>()))];
-  if (TRAIL) __syncthreads();
-}
-
 // Both vectors FROM -> TO at once through two CTA-wide buffers (the staging
 // buffers of the backward pass, free between reading a tile and prefetching
 // the next): three barriers for the pair.
