@@ -24,7 +24,10 @@ of uneven size per step through the persistent batched kernel (one CUDA
 graph replay; with N ranks a cost-balanced shard per rank plus a final
 all-gather), against a per-circuit loop of the single-circuit entry point;
 ``warm_start`` -- plain VQE from seeded random angles vs from the warm-start
-network's prediction at n=16, L=6 on 128 held-out fields (N=1 only).
+network's prediction at n=16, L=6 on 128 held-out fields (N=1 only);
+``adam_n12_l3`` and ``autograd_n20_l8`` -- torch Adam loops through the
+autograd Function at n=12, L=3 (20 steps) and n=20, L=8 (100 steps), with the
+bare device entry point and the CPU oracle beside them (N=1 only).
 """
 
 from __future__ import annotations
@@ -62,6 +65,7 @@ def parse_args():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-batch", action="store_true", help="skip the 4096-circuit batched section")
     ap.add_argument("--no-warmstart", action="store_true", help="skip the warm-start section")
+    ap.add_argument("--no-small", action="store_true", help="skip the n=12 Adam and n=20 autograd sections")
     return ap.parse_args()
 
 
@@ -297,6 +301,73 @@ def batch_section(args, rank, world, dist, barrier, max_over_ranks):
     return out
 
 
+def adam_section(n, L, steps, seed, field=1.0):
+    """``steps`` torch Adam steps (lr 0.05) on the autograd Function (forward
+    sweep + energy, then the adjoint sweep as backward), angles U[0, 2 pi) from
+    default_rng(seed).  Reports gradient evaluations/s of the loop and of the
+    bare device entry point, and the CPU oracle on the same circuit."""
+    import torch
+
+    import oracle
+    from gpu_simulation_b200 import Engine, ring_ising_energy
+
+    eng = Engine(n, L, field)
+    p0 = np.random.default_rng(seed).uniform(0.0, 2.0 * np.pi, (L, n, 2))
+    x = torch.tensor(p0, device="cuda", requires_grad=True)
+    opt = torch.optim.Adam([x], lr=0.05)
+
+    def step():
+        opt.zero_grad(set_to_none=False)
+        e = ring_ising_energy(x, eng)
+        e.backward()
+        opt.step()
+        return e
+
+    for _ in range(3):
+        step()
+    with torch.no_grad():
+        x.copy_(torch.tensor(p0, device="cuda"))
+    opt = torch.optim.Adam([x], lr=0.05)
+    torch.cuda.synchronize()
+    s, t = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(steps):
+        e = step()
+    t.record()
+    t.synchronize()
+    loop_ms = s.elapsed_time(t)
+    final = float(e.item())
+    # bare device entry point
+    flat = torch.tensor(p0.reshape(-1), device="cuda")
+    ed = torch.empty(1, dtype=torch.float64, device="cuda")
+    gd = torch.empty_like(flat)
+    for _ in range(3):
+        eng.energy_and_grad_device(flat, ed, gd)
+    s.record()
+    reps = 50
+    for _ in range(reps):
+        eng.energy_and_grad_device(flat, ed, gd)
+    t.record()
+    t.synchronize()
+    dev_ms = s.elapsed_time(t) / reps
+    eng.close()
+    threads = oracle.set_num_threads(0)
+    oracle.energy_and_grad(n, L, field, p0.reshape(-1))
+    t0 = time.perf_counter()
+    creps = 3
+    for _ in range(creps):
+        oracle.energy_and_grad(n, L, field, p0.reshape(-1))
+    cpu_s = (time.perf_counter() - t0) / creps
+    return {
+        "workload": f"n={n} L={L} h={field}, {steps} torch Adam steps (lr 0.05) through the autograd Function, seed {seed}",
+        "adam_steps_per_s": steps * 1000.0 / loop_ms, "ms_per_adam_step": loop_ms / steps,
+        "final_energy": final,
+        "energy_and_grad_per_s_device": 1000.0 / dev_ms, "ms_per_energy_and_grad_device": dev_ms,
+        "cpu_baseline": {"value": 1.0 / cpu_s, "unit": "energy_and_grad/s", "cores": threads, "kind": "port",
+                         "sample": f"{creps} energy_and_grad calls on the CPU restatement (oracle/)"},
+    }
+
+
 def warmstart_section():
     """Warm start (n=16, L=6): plain VQE (Adam lr 0.05, 300 steps) from seeded
     random angles vs from the network's prediction, on 128 held-out fields."""
@@ -466,6 +537,9 @@ def main():
         line["batch"] = batch_section(args, rank, world, dist, barrier, max_over_ranks)
     if world == 1 and not args.no_warmstart:
         line["warm_start"] = warmstart_section()
+    if world == 1 and not args.no_small:
+        line["adam_n12_l3"] = adam_section(12, 3, 20, seed=7)
+        line["autograd_n20_l8"] = adam_section(20, 8, 100, seed=7)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
