@@ -665,10 +665,10 @@ void fill_pass_params(rsv_backend *B, const Step &s, PassParams &P) {
   }
   P.need_l1 = l1 ? 1 : 0;
   P.need_l2 = l2 ? 1 : 0;
-  // Register layouts: 0 holds tile bits 8..11 in registers, 1 holds 4..7,
-  // 2 holds 0..3.  Forward passes load and store in layout 0; backward passes
-  // start in any layout (they read from the shared-memory staging area) and
-  // store from layout 0.
+  // Forward register layouts (rsv_pass.cu): 0 holds tile bits 8..11 in
+  // registers, 1 holds 4..7, 2 holds 0..3; layouts 0 and 1 have tile bits
+  // 0..3 on the lanes and load and store directly.  (The backward kernels use
+  // their own fixed layout families.)
   bool hi = false, mid = false, lo = false;
   for (int b = 0; b < 12; ++b) {
     if (s.tile.gate_wire[b] < 0) continue;
@@ -681,10 +681,18 @@ void fill_pass_params(rsv_backend *B, const Step &s, PassParams &P) {
     ++P.nseq;
   };
   if (!s.bwd) {
-    visit(0, hi);
-    if (mid) visit(1, true);
-    if (lo) visit(2, true);
-    if (P.nseq > 1) visit(0, false);
+    // load in layout 1 when bits 4..7 carry gates, end in layout 0 or 1 (both
+    // store whole segments): 1 (4..7) -> [2 (0..3)] -> 0 (8..11)
+    if (lo) {
+      visit(1, mid);
+      visit(2, true);
+      visit(0, hi);
+    } else if (mid) {
+      visit(1, true);
+      if (hi) visit(0, true);
+    } else {
+      visit(0, hi);
+    }
   } else {
     if (mid) visit(1, true);
     if (lo) visit(2, true);

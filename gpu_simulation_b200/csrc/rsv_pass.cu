@@ -28,27 +28,20 @@ namespace rsv {
 namespace {
 
 // Thread layouts of a tile (tile index t has 12 bits):
-//   layout 0: lanes -> t bits 0..4, warps -> 5..7,  registers -> 8..11 (global load/store)
-//   layout 1: lanes -> t bits 8..11,0, warps -> 1..3, registers -> 4..7
-//   layout 2: lanes -> t bits 4..8, warps -> 9..11, registers -> 0..3
+//   layout 0: lanes -> t bits 0..4,     warps -> 5..7,  registers -> 8..11
+//   layout 1: lanes -> t bits 0..3, 8,  warps -> 9..11, registers -> 4..7
+//   layout 2: lanes -> t bits 4..8,     warps -> 9..11, registers -> 0..3
+// Layouts 0 and 1 keep tile bits 0..3 on the lanes (the c >= 2 contiguous low
+// bits of every tile, so at least whole 32-byte sectors, 256-byte segments for
+// c >= 4), so both load and store directly; a pass visits 1 (bits 4..7) ->
+// [2 (bits 0..3)] -> 0 (bits 8..11): a tile with gates on bits 4..11 needs one
+// CTA-wide transpose and the 12-wire tile two.
 __device__ __forceinline__ int thread_part(int layout, int lane, int warp) {
   if (layout == 0) return lane | (warp << 5);
-  if (layout == 1) return (lane >> 4) | (warp << 1) | ((lane & 15) << 8);
+  if (layout == 1) return (lane & 15) | ((lane >> 4) << 8) | (warp << 9);
   return (lane << 4) | (warp << 9);
 }
 __device__ __forceinline__ int reg_shift(int layout) { return layout == 0 ? 8 : (layout == 1 ? 4 : 0); }
-
-// Tile bit held by lane bit j / warp bit j of a layout.
-__device__ __forceinline__ int lane_tile_bit(int layout, int j) {
-  if (layout == 0) return j;
-  if (layout == 1) return j < 4 ? 8 + j : 0;
-  return 4 + j;
-}
-__device__ __forceinline__ int warp_tile_bit(int layout, int j) {
-  if (layout == 0) return 5 + j;
-  if (layout == 1) return 1 + j;
-  return 9 + j;
-}
 
 // Forward rotation of the four register bits of `layout` (tile bits
 // rb..rb+3): RY / f in tangent form, one FMA per component.
@@ -321,30 +314,36 @@ __global__ void __launch_bounds__(kThreads, 2) fwd_pass_kernel(const PassParams 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int n = P.n;
-  const int tp0 = thread_part(0, lane, warp);
-  const u32 toff0 = thread_offset(P, tp0);
-  const u32 v8 = P.vec[8], v9 = P.vec[9], v10 = P.vec[10], v11 = P.vec[11];
+  // the tile is loaded in the first visited layout and stored from the last
+  const int first = P.seq_layout[0], last = P.seq_layout[P.nseq - 1];
+  const u32 toffl = thread_offset(P, thread_part(first, lane, warp));
+  const int rl = reg_shift(first);
+  const u32 v0 = P.vec[rl], v1 = P.vec[rl + 1], v2 = P.vec[rl + 2], v3 = P.vec[rl + 3];
+  const u32 toffs = thread_offset(P, thread_part(last, lane, warp));
+  const int rs = reg_shift(last);
+  const u32 w0 = P.vec[rs], w1 = P.vec[rs + 1], w2 = P.vec[rs + 2], w3 = P.vec[rs + 3];
   const u32 num_tiles = static_cast<u32>(P.num_tiles);
   double2 dummy[kRegs];
   double2 ratio[4];
   if (PHASE) {
 #pragma unroll
-    for (int j = 0; j < 4; ++j) ratio[j] = phase_ratio(P, unit_bit(P.vec[8 + j]));
+    for (int j = 0; j < 4; ++j) ratio[j] = phase_ratio(P, unit_bit(P.vec[rs + j]));
   }
 
   for (u32 tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
-    const u32 base = deposit(P, tile) ^ toff0;
+    const u32 cbase = deposit(P, tile);
+    const u32 base = cbase ^ toffl;
     double2 a[kRegs];
 #pragma unroll
     for (int r = 0; r < kRegs; ++r) {
-      const u32 p = base ^ reg_offset(r, v8, v9, v10, v11);
+      const u32 p = base ^ reg_offset(r, v0, v1, v2, v3);
       if (PSRC == kLoadNatural) a[r] = __ldcs(&P.psi_in[p]);
       if (PSRC == kLoadProduct) a[r] = table4(P.prod, static_cast<u32>(ring_pinv(p, n)));
       if (PSRC == kLoadProductPlain) a[r] = table4(P.prod, p);
     }
     if (P.sync_after_load) __syncthreads();
 
-    int prev = 0;
+    int prev = first;
     for (int k = 0; k < P.nseq; ++k) {
       const int layout = P.seq_layout[k];
       const int tp = thread_part(layout, lane, warp);
@@ -353,13 +352,14 @@ __global__ void __launch_bounds__(kThreads, 2) fwd_pass_kernel(const PassParams 
       prev = layout;
     }
 
+    const u32 sbase = cbase ^ toffs;
     if (PHASE) {
-      const double2 ph = table4(P.ptab, base);
+      const double2 ph = table4(P.ptab, sbase);
       const double K = P.lscale[P.layer];
       apply_phase_gray<4, false, false>(make_double2(K * ph.x, K * ph.y), ratio, a, dummy);
     }
 #pragma unroll
-    for (int r = 0; r < kRegs; ++r) store_amp<PDST>(P.psi_out, base ^ reg_offset(r, v8, v9, v10, v11), n, a[r]);
+    for (int r = 0; r < kRegs; ++r) store_amp<PDST>(P.psi_out, sbase ^ reg_offset(r, w0, w1, w2, w3), n, a[r]);
   }
 }
 
