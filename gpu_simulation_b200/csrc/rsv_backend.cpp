@@ -780,7 +780,7 @@ void run_energy(rsv_backend *B, cudaStream_t st) {
   const double bytes = 2.0 * 16.0 * static_cast<double>(u64{1} << B->n);
   timed(B, st, 2, bytes, [&] {
     check(launch_energy(state_buf(B, B->plan.chi_buf), state_buf(B, B->plan.mu_buf), B->n, B->field,
-                        u64{1} << B->n, B->energy_partials.p, B->energy_grid, st),
+                        u64{1} << B->n, B->energy_partials.p, B->energy_grid, B->sms, st),
           "energy launch");
   });
 }

@@ -1,6 +1,8 @@
 // sm_100a kernels for the ring-Ising structured adjoint: coefficient and
 // byte-table preparation, the energy (lambda = H psi) kernel and the final
 // deterministic reduction.  The tile-pass kernels are in rsv_pass.cu.
+#include <algorithm>
+
 #include "rsv_device.cuh"
 #include "rsv_types.h"
 
@@ -149,32 +151,60 @@ __global__ void rot_kernel(const double4 *__restrict__ coef, int n, int L, const
 // last layer before its CNOT ring (the ring is folded into H).  Equivalent to
 // the reference's lambda = H psi (cpp/ising_cuda_kernels.cu:313-358) followed
 // by its inverse ring gather on lambda and psi.
+//
+// In this frame the field term of wire w flips the index bits of
+// m_w = P^-1(e_w): bits {w, w+1}, and {n-1, 0, 1} for the last wire.  A flip
+// of a high bit reads an amplitude far away, which for large states comes
+// from DRAM once more per amplitude.  From kEnergySplitQubits on, the masks
+// on the top nine bits (and the two on bits 0..2) are therefore applied by a
+// tile kernel that holds cosets of bits {0,1,2} and {n-9..n-1} in shared
+// memory; the grid-stride kernel adds the remaining masks, whose partners
+// are near enough to come from L1/L2, and forms the energy.
 // ------------------------------------------------------------------------
 constexpr int kEnergyThreads = 256;
+constexpr int kEnergySplitQubits = 21;
+constexpr int kEnergyHighBits = 9;
+constexpr int kEnergyTileThreads = 256;
+constexpr int kEnergyTileBits = 12;  // 3 low + kEnergyHighBits high bits
+constexpr size_t kEnergyTileSmem = (size_t{1} << kEnergyTileBits) * sizeof(double2);
+// masks inside a tile: wires 0 and 1, the eight wires n-9..n-2 and the last wire
+constexpr int kEnergyTileMasks = 11;
 
+// Index masks of the grid-stride part, compacted on the host.
+struct EnergyMasks {
+  u64 m[kMaxQubits];
+};
+
+// grid-stride part: the K masks of M, plus mu_in (the tile kernel's part,
+// diagonal included) when given, else the diagonal.  K is a template
+// parameter so that all K partner loads of an amplitude are issued before
+// the first is used.
+template <int K>
 __global__ void __launch_bounds__(kEnergyThreads) energy_kernel(const double2 *__restrict__ chi,
                                                                  double2 *__restrict__ mu, int n,
                                                                  double field, u64 size,
+                                                                 const EnergyMasks M, int with_mu_in,
                                                                  double *__restrict__ partials) {
   __shared__ double red[kEnergyThreads / 32];
-  u64 masks[kMaxQubits];
-#pragma unroll
-  for (int w = 0; w < kMaxQubits; ++w) masks[w] = (w < n) ? ring_pinv(u64{1} << w, n) : 0;
   double e = 0.0;
   const u64 stride = static_cast<u64>(gridDim.x) * kEnergyThreads;
   for (u64 i = static_cast<u64>(blockIdx.x) * kEnergyThreads + threadIdx.x; i < size; i += stride) {
     const double2 c = chi[i];
-    const double d = diag_after_ring(i, n);
     double2 x = make_double2(0.0, 0.0);
 #pragma unroll
-    for (int w = 0; w < kMaxQubits; ++w) {
-      if (w < n) {
-        const double2 t = __ldg(&chi[i ^ masks[w]]);
-        x.x += t.x;
-        x.y += t.y;
-      }
+    for (int j = 0; j < K; ++j) {
+      const double2 t = __ldg(&chi[i ^ M.m[j]]);
+      x.x += t.x;
+      x.y += t.y;
     }
-    const double2 m = make_double2(fma(d, c.x, -field * x.x), fma(d, c.y, -field * x.y));
+    double2 m;
+    if (with_mu_in) {
+      const double2 mi = mu[i];
+      m = make_double2(fma(-field, x.x, mi.x), fma(-field, x.y, mi.y));
+    } else {
+      const double d = diag_after_ring(i, n);
+      m = make_double2(fma(d, c.x, -field * x.x), fma(d, c.y, -field * x.y));
+    }
     mu[i] = m;
     e += fma(c.x, m.x, c.y * m.y);
   }
@@ -185,6 +215,71 @@ __global__ void __launch_bounds__(kEnergyThreads) energy_kernel(const double2 *_
     double s = 0.0;
     for (int i = 0; i < kEnergyThreads / 32; ++i) s += red[i];
     partials[blockIdx.x] = s;
+  }
+}
+
+template <int K>
+cudaError_t launch_energy_k(int count, int grid, cudaStream_t s, const double2 *chi, double2 *mu, int n,
+                            double field, u64 size, const EnergyMasks &M, int with_mu_in, double *partials) {
+  if (count == K) {
+    energy_kernel<K><<<grid, kEnergyThreads, 0, s>>>(chi, mu, n, field, size, M, with_mu_in, partials);
+    return cudaGetLastError();
+  }
+  if constexpr (K < kMaxQubits) {
+    return launch_energy_k<K + 1>(count, grid, s, chi, mu, n, field, size, M, with_mu_in, partials);
+  } else {
+    return cudaErrorInvalidValue;
+  }
+}
+
+struct EnergyTile {
+  int n, hs, num_masks;
+  double field;
+  u64 num_tiles;
+  unsigned int tmask[kEnergyTileBits];  // masks in tile coordinates
+};
+
+// Tile index tau: bits 0..2 -> index bits 0..2 (one 128-byte line),
+// bits 3..11 -> index bits hs..hs+8; the coset runs over index bits 3..hs-1.
+__device__ __forceinline__ u64 energy_tile_index(u64 cbase, int tau, int hs) {
+  return cbase | static_cast<u64>(tau & 7) | (static_cast<u64>(tau >> 3) << hs);
+}
+
+__global__ void __launch_bounds__(kEnergyTileThreads) energy_tile_kernel(const double2 *__restrict__ chi,
+                                                                          double2 *__restrict__ mu,
+                                                                          const EnergyTile T) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2 *tile = reinterpret_cast<double2 *>(smem_raw);
+  constexpr int kPer = (1 << kEnergyTileBits) / kEnergyTileThreads;
+  for (u64 t = blockIdx.x; t < T.num_tiles; t += gridDim.x) {
+    const u64 cbase = t << 3;
+    __syncthreads();  // the previous tile's partner reads are done
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const int tau = threadIdx.x + k * kEnergyTileThreads;
+      const unsigned int s = static_cast<unsigned int>(__cvta_generic_to_shared(&tile[tau]));
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s),
+                   "l"(&chi[energy_tile_index(cbase, tau, T.hs)])
+                   : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+#pragma unroll 4
+    for (int k = 0; k < kPer; ++k) {
+      const int tau = threadIdx.x + k * kEnergyTileThreads;
+      const u64 p = energy_tile_index(cbase, tau, T.hs);
+      const double2 c = tile[tau];
+      double2 x = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int j = 0; j < kEnergyTileMasks; ++j) {
+        const double2 v = tile[tau ^ T.tmask[j]];
+        x.x += v.x;
+        x.y += v.y;
+      }
+      const double d = diag_after_ring(p, T.n);
+      __stcg(&mu[p], make_double2(fma(d, c.x, -T.field * x.x), fma(d, c.y, -T.field * x.y)));
+    }
   }
 }
 
@@ -258,9 +353,41 @@ cudaError_t launch_rot(const double4 *coef, int n, int L, const int *order, bool
 }
 
 cudaError_t launch_energy(const double2 *chi, double2 *mu, int n, double field, u64 size,
-                          double *partials, int grid, cudaStream_t s) {
-  energy_kernel<<<grid, kEnergyThreads, 0, s>>>(chi, mu, n, field, size, partials);
-  return cudaGetLastError();
+                          double *partials, int grid, int sms, cudaStream_t s) {
+  if (n < 1 || n > kMaxQubits) return cudaErrorInvalidValue;
+  EnergyMasks M{};
+  int count = 0;
+  if (n < kEnergySplitQubits) {
+    for (int w = 0; w < n; ++w) M.m[count++] = ring_pinv(u64{1} << w, n);
+    return launch_energy_k<1>(count, grid, s, chi, mu, n, field, size, M, 0, partials);
+  }
+  EnergyTile T{};
+  T.n = n;
+  T.hs = n - kEnergyHighBits;
+  T.field = field;
+  T.num_tiles = u64{1} << (n - kEnergyTileBits);
+  for (int w = 0; w < n; ++w) {
+    const u64 m = ring_pinv(u64{1} << w, n);
+    if ((m & ~u64{7} & ((u64{1} << T.hs) - 1)) == 0) {
+      if (T.num_masks == kEnergyTileMasks) return cudaErrorInvalidValue;
+      T.tmask[T.num_masks++] = static_cast<unsigned int>((m & 7) | ((m >> T.hs) << 3));
+    } else {
+      M.m[count++] = m;
+    }
+  }
+  if (T.num_masks != kEnergyTileMasks) return cudaErrorInvalidValue;
+  static bool configured = false;
+  if (!configured) {
+    const cudaError_t e = cudaFuncSetAttribute(energy_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               static_cast<int>(kEnergyTileSmem));
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  const int tgrid = static_cast<int>(std::min<u64>(T.num_tiles, static_cast<u64>(std::max(1, sms)) * 3));
+  energy_tile_kernel<<<tgrid, kEnergyTileThreads, kEnergyTileSmem, s>>>(chi, mu, T);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return launch_energy_k<1>(count, grid, s, chi, mu, n, field, size, M, 1, partials);
 }
 
 cudaError_t launch_finalize(const FinalizeParams &F, cudaStream_t s) {

@@ -17,7 +17,7 @@ TOL = 1e-10
 
 @pytest.mark.parametrize("n,L,h", [
     (13, 1, 0.8), (13, 3, 1.1), (14, 2, 1.0), (15, 5, 0.4), (16, 4, 1.3), (17, 3, 0.9),
-    (19, 2, 1.0), (20, 3, 0.6), (22, 2, 1.7),
+    (19, 2, 1.0), (20, 3, 0.6), (21, 2, 0.8), (22, 2, 1.7),
 ])
 def test_both_schedules_match_oracle(n, L, h):
     p = np.random.default_rng(500 + 7 * n + L).uniform(0.0, 2.0 * np.pi, 2 * n * L)
