@@ -56,6 +56,7 @@ void check(cudaError_t e, const char *what) {
 struct Tile {
   u64 vec[12]{};
   int gate_wire[12];
+  int dims = 12;  // tile bits in use (11: half tile of a backward pass)
   int num_runs = 0;
   int run_start[4]{};
   int run_len[4]{};
@@ -68,10 +69,11 @@ struct Tile {
 // indices); `phys` is the number of physical index bits.  Gates are placed on
 // the tile bits whose physical bit is listed in `gates`.
 Tile unit_tile(int phys, const std::vector<int> &bits, const std::vector<int> &gates) {
-  if (bits.size() != 12) throw Error(RSV_ERR_INTERNAL, "tile needs 12 directions");
+  if (bits.size() != 12 && bits.size() != 11) throw Error(RSV_ERR_INTERNAL, "tile needs 12 or 11 directions");
   Tile t;
+  t.dims = static_cast<int>(bits.size());
   std::vector<bool> in(phys, false);
-  for (int b = 0; b < 12; ++b) {
+  for (int b = 0; b < t.dims; ++b) {
     t.vec[b] = u64{1} << bits[b];
     in[bits[b]] = true;
     if (std::find(gates.begin(), gates.end(), bits[b]) != gates.end()) t.gate_wire[b] = bits[b];
@@ -89,7 +91,7 @@ Tile unit_tile(int phys, const std::vector<int> &bits, const std::vector<int> &g
     ++t.num_runs;
     p = q;
   }
-  t.num_tiles = u64{1} << (phys - 12);
+  t.num_tiles = u64{1} << (phys - t.dims);
   return t;
 }
 
@@ -193,6 +195,48 @@ void record_theta(Plan &pl, const Step &s) {
     if (pl.theta_pass[k] >= 0) throw Error(RSV_ERR_INTERNAL, "wire planned twice");
     pl.theta_pass[k] = s.pass_index;
     pl.theta_slot[k] = b;
+  }
+}
+
+// Backward passes whose gates all lie on tile bits 4..11 of a unit tile with
+// tile bits 0..3 = index bits 0..3 run on the 11-bit half tile (tile bit 3
+// moves to the coset) with two 256-thread CTAs per SM (rsv_pass_half.cu),
+// for the load/store variants that kernel has, once the pass has at least
+// eight 12-bit tiles per SM (smaller states sit in L2, where the extra CTAs
+// only add launch cost: n = 20 ran 6% slower on half tiles).
+bool half_tile_variant(const Step &s) {
+  const int pl = s.psi_load, ll = s.lam_load, ps = s.psi_store, ls = s.lam_store;
+  if (pl == kLoadNatural && ps == kStoreNatural && ls == kStoreNatural)
+    return ll == kLoadNatural || ll == kLoadGatherP;
+  if (ps != kStoreNone || ls != kStoreNatural) return false;
+  return (pl == kLoadNatural && ll == kLoadNatural) || (pl == kLoadGatherP && ll == kLoadGatherP) ||
+         (pl == kLoadProductPlain && (ll == kLoadGatherP || ll == kLoadNatural));
+}
+
+void use_half_tiles(Plan &pl, int sms) {
+  const int ctas = 2 * std::max(1, sms);
+  for (auto &s : pl.bwd) {
+    const Tile &t = s.tile;
+    if (!t.unit || t.dims != 12 || !half_tile_variant(s)) continue;
+    if (t.num_tiles < static_cast<u64>(8) * std::max(1, sms)) continue;
+    bool ok = true;
+    for (int b = 0; b < 4; ++b) ok = ok && t.gate_wire[b] < 0 && t.vec[b] == (u64{1} << b);
+    if (!ok) continue;
+    std::vector<int> bits, gates;
+    for (int b = 0; b < 12; ++b) {
+      if (b == 3) continue;
+      int bit = 0;
+      while (!((t.vec[b] >> bit) & 1)) ++bit;
+      bits.push_back(bit);
+      if (t.gate_wire[b] >= 0) gates.push_back(t.gate_wire[b]);
+    }
+    s.tile = unit_tile(pl.phys, bits, gates);
+    s.grid = static_cast<int>(std::min<u64>(s.tile.num_tiles, static_cast<u64>(ctas)));
+    pl.max_grid = std::max(pl.max_grid, s.grid);
+    for (int b = 0; b < s.tile.dims; ++b) {
+      const int w = s.tile.gate_wire[b];
+      if (w >= 0) pl.theta_slot[static_cast<size_t>(s.layer) * pl.n + w] = b;
+    }
   }
 }
 
@@ -307,7 +351,18 @@ Plan make_checkpoint_plan(Plan pl, const std::vector<Tile> &fwd_tiles, int fwd_c
 //     Reference counterpart: run_structured_backward_sweep
 //     (cpp/ising_cuda_structured_adjoint_modes.inc:188-307), which always
 //     un-computes psi.
+Plan make_plan_full(int n, int L, int sms, bool checkpoint);
+
+// Plans of the single-circuit engine (half tiles on the eligible backward
+// passes); the batched kernel and the fixed-workspace entry point use
+// make_plan_full, whose tiles all have 12 bits.
 Plan make_plan(int n, int L, int sms, bool checkpoint = false) {
+  Plan pl = make_plan_full(n, L, sms, checkpoint);
+  use_half_tiles(pl, sms);
+  return pl;
+}
+
+Plan make_plan_full(int n, int L, int sms, bool checkpoint) {
   Plan pl;
   pl.n = n;
   pl.L = L;
@@ -451,13 +506,16 @@ Plan make_plan(int n, int L, int sms, bool checkpoint = false) {
 // carries kUndoPassStart (the gradient correction restarts there, see
 // rot_kernel).
 std::vector<int> undo_order(const Plan &pl) {
+  // tile bits in the order the backward kernels rotate them: bwd_pass_kernel
+  // B0, B1, A1, A2 (rsv_pass.cu); bwd_half_kernel H0, H1, HA (rsv_pass_half.cu)
   static const int kBits[12] = {9, 10, 11, 6, 7, 8, 0, 1, 2, 3, 4, 5};
+  static const int kBitsHalf[11] = {8, 9, 10, 5, 6, 7, 3, 4, 0, 1, 2};
   std::vector<int> ord;
   for (const auto &s : pl.bwd) {
     if (s.layer != pl.L - 1) continue;
     bool start = pl.checkpoint;
-    for (int i = 0; i < 12; ++i) {
-      const int w = s.tile.gate_wire[kBits[i]];
+    for (int i = 0; i < s.tile.dims; ++i) {
+      const int w = s.tile.gate_wire[s.tile.dims == 12 ? kBits[i] : kBitsHalf[i]];
       if (w < 0) continue;
       ord.push_back(start ? (w | kUndoPassStart) : w);
       start = false;
@@ -492,7 +550,7 @@ std::string describe(const Plan &pl) {
   auto tile_str = [](const Tile &t) {
     std::ostringstream ts;
     ts << "dirs=[";
-    for (int b = 0; b < 12; ++b) {
+    for (int b = 0; b < t.dims; ++b) {
       if (b) ts << ",";
       if ((t.vec[b] & (t.vec[b] - 1)) == 0) {
         int bit = 0;
@@ -651,13 +709,14 @@ void fill_pass_params(rsv_backend *B, const Step &s, PassParams &P) {
   }
   P.num_tiles = s.tile.num_tiles;
   for (int b = 0; b < 32; ++b) P.wire_tile_bit[b] = -1;
+  P.tile_bits = s.tile.dims;
   bool l1 = false, l2 = false;
   for (int b = 0; b < 12; ++b) {
     P.vec[b] = s.tile.vec[b];
     P.gate_wire[b] = s.tile.gate_wire[b];
     if (s.tile.gate_wire[b] >= 0 && b < 8) l1 = true;
     if (s.tile.gate_wire[b] >= 0 && b < 4) l2 = true;
-    if (s.tile.unit) {
+    if (s.tile.unit && b < s.tile.dims) {
       int bit = 0;
       while (!((s.tile.vec[b] >> bit) & 1)) ++bit;
       if (bit < 32) P.wire_tile_bit[bit] = b;
@@ -1008,7 +1067,7 @@ namespace {
 int batch_plan_index(rsv_batch *Bt, int n, int L) {
   for (size_t i = 0; i < Bt->plan_keys.size(); ++i)
     if (Bt->plan_keys[i] == std::make_pair(n, L)) return static_cast<int>(i);
-  const Plan pl = make_plan(n, L, Bt->sms);
+  const Plan pl = make_plan_full(n, L, Bt->sms, false);
   BatchPlan bp{};
   bp.first_step = static_cast<int>(Bt->steps.size());
   bp.undo_off = static_cast<int>(Bt->undo.size());
@@ -1143,7 +1202,7 @@ rsv_status run_in_workspace(int n, int L, double field, const double *d_params, 
     B.num_params = num_params;
     check(cudaGetDevice(&B.device), "cudaGetDevice");
     check(cudaDeviceGetAttribute(&B.sms, cudaDevAttrMultiProcessorCount, B.device), "cudaDeviceGetAttribute");
-    B.plan = make_plan(n, L, B.sms);
+    B.plan = make_plan_full(n, L, B.sms, false);
     B.num_bwd_passes = static_cast<int>(B.plan.bwd.size());
     B.state_len = size_t{1} << B.plan.phys;
     B.energy_grid = static_cast<int>(std::min<u64>(std::max<u64>(1, (u64{1} << n) / 256),

@@ -17,6 +17,8 @@ cudaError_t launch_rot(const double4 *coef, int n, int L, const int *order, bool
 cudaError_t configure_pass_kernels();
 size_t pass_smem_bytes(bool bwd);
 cudaError_t launch_pass(const PassParams &P, bool bwd, int grid, cudaStream_t s);
+// backward pass on an 11-bit half tile (rsv_pass_half.cu)
+cudaError_t launch_bwd_half(const PassParams &P, int grid, cudaStream_t s);
 // mu = (P^T H P) chi and per-CTA energy partials ([grid]); for large n a
 // shared-memory tile kernel takes the masks on the top index bits first
 cudaError_t launch_energy(const double2 *chi, double2 *mu, int n, double field,

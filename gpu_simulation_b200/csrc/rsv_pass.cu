@@ -22,6 +22,7 @@
 // The load/store variants are template parameters, so every instantiation
 // carries only the code of its own variant; the register gate code exists
 // once and is visited once per layout.
+#include "rsv_launch.h"
 #include "rsv_tile.cuh"
 
 namespace rsv {
@@ -394,6 +395,10 @@ cudaError_t launch_fwd(const PassParams &P, int grid, cudaStream_t s) {
 }  // namespace
 
 cudaError_t launch_pass(const PassParams &P, bool bwd, int grid, cudaStream_t s) {
+  if (P.tile_bits != 12) {
+    if (bwd && P.tile_bits == 11) return launch_bwd_half(P, grid, s);
+    return cudaErrorInvalidValue;
+  }
   if (bwd) {
     const bool phase = P.phase != 0;
     if (P.phi_grad != P.phase) return cudaErrorInvalidValue;

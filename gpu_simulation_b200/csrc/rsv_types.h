@@ -74,6 +74,7 @@ struct PassParams {
   const double2 *ptab;         // phase byte tables of this layer, [4][256]
   const double2 *prod;         // layer-0 product-state byte tables, [4][256] (full or partial)
   double *partials;            // [gridDim.x][kPartialStride] for this pass
+  int tile_bits;               // 12, or 11 for a backward pass on the half tile (rsv_pass_half.cu)
 };
 
 // Inputs of the deterministic final reduction (energy + gradient).

@@ -109,7 +109,7 @@ def tile_indices(step: dict) -> np.ndarray:
     for start, ln in step["runs"]:
         base |= (rem & ((1 << ln) - 1)) << start
         rem >>= ln
-    t = np.arange(4096, dtype=np.int64)
+    t = np.arange(1 << len(step["dirs"]), dtype=np.int64)
     off = np.zeros_like(t)
     for b, v in enumerate(step["dirs"]):
         off ^= np.where((t >> b) & 1, v, 0)
@@ -122,13 +122,13 @@ def check_pair_roles(step: dict, n: int) -> None:
     (flip bit) has coordinate 1.  Check that rule against the physical bit w
     of every element of every tile."""
     dirs = step["dirs"]
-    flip = 12
+    flip = len(dirs)
     for b, v in enumerate(dirs):
         if v & (v - 1) and any((v >> w) & 1 for w in step["gates"]):
             flip = b
-    ids = tile_indices(step).reshape(step["tiles"], 4096)
-    t = np.arange(4096, dtype=np.int64)
-    flip_coord = (t >> flip) & 1 if flip < 12 else np.zeros_like(t)
+    ids = tile_indices(step).reshape(step["tiles"], 1 << len(dirs))
+    t = np.arange(1 << len(dirs), dtype=np.int64)
+    flip_coord = (t >> flip) & 1 if flip < len(dirs) else np.zeros_like(t)
     for w in step["gates"]:
         b = [i for i, v in enumerate(dirs) if v == (1 << w)]
         assert len(b) == 1, "a gated wire needs its unit direction in the tile"
