@@ -464,6 +464,10 @@ def main():
     e2e_ms = max_over_ranks(e2e_ms)
 
     peak, peak_src = measured_peaks()
+    KERNEL_NAMES = {
+        "backward_pass": "backward passes (bwd_pass_kernel 12-bit tiles + bwd_half_kernel 11-bit tiles)",
+        "forward_pass": "fwd_pass_kernel", "energy": "energy_tile_kernel + energy_kernel",
+    }
     kinds = {k: v for k, v in stats.items() if v["launches"]}
     dom = max(kinds, key=lambda k: kinds[k]["ms"])
     d = kinds[dom]
@@ -477,7 +481,7 @@ def main():
             if len(cells) == 3 and cells[0] == dom and cells[1] == str(n):
                 traffic = float(cells[2])
     roofline = {
-        "bound": "hbm", "kernel": f"pass_kernel ({dom})", "achieved": achieved, "peak": peak,
+        "bound": "hbm", "kernel": KERNEL_NAMES.get(dom, dom), "achieved": achieved, "peak": peak,
         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
         "peak_source": peak_src,
         "algorithmic_bytes_per_launch": d["bytes"] / d["launches"],
