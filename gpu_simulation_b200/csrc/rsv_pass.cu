@@ -196,6 +196,9 @@ __global__ void __launch_bounds__(bw::kT, 1) bwd_pass_kernel(const PassParams P)
 
   double2 ratio[4];
   const u32 toffp = thread_offset(P, tpart<B0>(lane, warp));
+  u32 poff[kR];  // register offsets of layout B0 (analytic psi)
+#pragma unroll
+  for (int r = 0; r < kR; ++r) poff[r] = ((r & 1) ? v9 : 0u) ^ ((r & 2) ? v10 : 0u) ^ ((r & 4) ? v11 : 0u);
   if (PHASE) {
 #pragma unroll
     for (int j = 0; j < 3; ++j) ratio[j] = phase_ratio(P, unit_bit(P.vec[9 + j]));
@@ -245,9 +248,7 @@ __global__ void __launch_bounds__(bw::kT, 1) bwd_pass_kernel(const PassParams P)
     if (PSRC == kLoadProductPlain) {
       // layout B0: registers -> tile bits 9..11
       const u32 base = cbase ^ toffp;
-#pragma unroll
-      for (int r = 0; r < kR; ++r)
-        a[r] = table4(P.prod, base ^ ((r & 1) ? v9 : 0u) ^ ((r & 2) ? v10 : 0u) ^ ((r & 4) ? v11 : 0u));
+      table4_regs(P.prod, base, poff, a);
     }
     if (PHASE) {
       // RZ^dagger of the layer (with the layer's factor K) on psi and lambda,
@@ -331,17 +332,25 @@ __global__ void __launch_bounds__(kThreads, 2) fwd_pass_kernel(const PassParams 
     for (int j = 0; j < 4; ++j) ratio[j] = phase_ratio(P, unit_bit(P.vec[rs + j]));
   }
 
+  // analytic sources: per-register offsets of the product-table index
+  // (ring_pinv is linear, so the index of base ^ o is ring_pinv(base) ^ ring_pinv(o))
+  u32 poff[kRegs];
+#pragma unroll
+  for (int r = 0; r < kRegs; ++r) {
+    const u32 o = reg_offset(r, v0, v1, v2, v3);
+    poff[r] = PSRC == kLoadProduct ? static_cast<u32>(ring_pinv(o, n)) : o;
+  }
+
   for (u32 tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
     const u32 cbase = deposit(P, tile);
     const u32 base = cbase ^ toffl;
     double2 a[kRegs];
+    if (PSRC == kLoadNatural) {
 #pragma unroll
-    for (int r = 0; r < kRegs; ++r) {
-      const u32 p = base ^ reg_offset(r, v0, v1, v2, v3);
-      if (PSRC == kLoadNatural) a[r] = __ldcs(&P.psi_in[p]);
-      if (PSRC == kLoadProduct) a[r] = table4(P.prod, static_cast<u32>(ring_pinv(p, n)));
-      if (PSRC == kLoadProductPlain) a[r] = table4(P.prod, p);
+      for (int r = 0; r < kRegs; ++r) a[r] = __ldcs(&P.psi_in[base ^ reg_offset(r, v0, v1, v2, v3)]);
     }
+    if (PSRC == kLoadProduct) table4_regs(P.prod, static_cast<u32>(ring_pinv(base, n)), poff, a);
+    if (PSRC == kLoadProductPlain) table4_regs(P.prod, base, poff, a);
     if (P.sync_after_load) __syncthreads();
 
     int prev = first;

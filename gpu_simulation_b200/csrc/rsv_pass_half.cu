@@ -216,6 +216,9 @@ __global__ void __launch_bounds__(hw::kT, 2) bwd_half_kernel(const PassParams P)
   const u32 toffs = thread_offset(P, tpart<HA>(lane, warp));
   const u32 v3 = P.vec[3], v4 = P.vec[4], v7 = P.vec[7];
   const u32 toffp = thread_offset(P, tpart<H0>(lane, warp));
+  u32 poff[kR];  // register offsets of layout H0 (analytic psi)
+#pragma unroll
+  for (int r = 0; r < kR; ++r) poff[r] = ((r & 1) ? v8 : 0u) ^ ((r & 2) ? v9 : 0u) ^ ((r & 4) ? v10 : 0u);
 
   double2 ratio[4];
   if (PHASE) {
@@ -263,9 +266,7 @@ __global__ void __launch_bounds__(hw::kT, 2) bwd_half_kernel(const PassParams P)
     const u32 cbase = deposit(P, tile);
     if (PSRC == kLoadProductPlain) {
       const u32 base = cbase ^ toffp;
-#pragma unroll
-      for (int r = 0; r < kR; ++r)
-        a[r] = table4(P.prod, base ^ ((r & 1) ? v8 : 0u) ^ ((r & 2) ? v9 : 0u) ^ ((r & 4) ? v10 : 0u));
+      table4_regs(P.prod, base, poff, a);
     }
     if (PHASE) {
       // RZ^dagger of the layer (with the layer's factor K) on psi and lambda,

@@ -62,6 +62,29 @@ __device__ __forceinline__ double2 table4(const double2 *__restrict__ t, u32 p) 
   return v;
 }
 
+// table4(t, base ^ off[r]) for all registers of a thread: the bytes of the
+// index that no register offset touches are looked up and multiplied once.
+template <int NR>
+__device__ __forceinline__ void table4_regs(const double2 *__restrict__ t, u32 base, const u32 (&off)[NR],
+                                            double2 (&out)[NR]) {
+  u32 vary = 0;
+#pragma unroll
+  for (int r = 0; r < NR; ++r) vary |= off[r];
+  double2 c = make_double2(1.0, 0.0);
+#pragma unroll
+  for (int b = 0; b < 4; ++b)
+    if (((vary >> (8 * b)) & 255u) == 0) c = cmul(c, RSV_TABLE_LOAD(&t[256 * b + ((base >> (8 * b)) & 255u)]));
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    const u32 j = base ^ off[r];
+    double2 v = c;
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+      if (((vary >> (8 * b)) & 255u) != 0) v = cmul(v, RSV_TABLE_LOAD(&t[256 * b + ((j >> (8 * b)) & 255u)]));
+    out[r] = v;
+  }
+}
+
 template <int SRC>
 __device__ __forceinline__ u32 source_index(u32 p, int n) {
   if (SRC == kLoadGatherP) return static_cast<u32>(ring_p(p, n));
