@@ -170,6 +170,11 @@ struct Plan {
   // checkpoint mode: wire masks of the partial layer-0 product tables 1..
   std::vector<unsigned int> partial_masks;
   int max_grid = 1;
+  // layer 0 on the layer-0 kernel (rsv_layer0.cu): its backward passes are
+  // dropped; the kernel reads lambda from buffer layer0_lam (gathered
+  // through P when layer0_load is kLoadGatherP)
+  bool layer0_kernel = false;
+  int layer0_lam = -1, layer0_load = kLoadNatural, layer0_grid = 1;
 };
 
 // Checkpoint-mode plans keep max((L-1) * passes + 1, 2) state buffers; they
@@ -211,6 +216,27 @@ bool half_tile_variant(const Step &s) {
   if (ps != kStoreNone || ls != kStoreNatural) return false;
   return (pl == kLoadNatural && ll == kLoadNatural) || (pl == kLoadGatherP && ll == kLoadGatherP) ||
          (pl == kLoadProductPlain && (ll == kLoadGatherP || ll == kLoadNatural));
+}
+
+// Layer 0's gradients need only lambda at the output of layer 0 (its state is
+// an analytic product state): n >= 13 replaces the layer's backward passes by
+// one read of lambda on the layer-0 kernel.
+void use_layer0_kernel(Plan &pl, int sms) {
+  if (pl.n < 13) return;
+  auto first = std::find_if(pl.bwd.begin(), pl.bwd.end(), [](const Step &s) { return s.layer == 0; });
+  if (first == pl.bwd.end()) return;
+  pl.layer0_lam = first->lam_in;
+  pl.layer0_load = first->lam_load;
+  if (pl.layer0_load != kLoadNatural && pl.layer0_load != kLoadGatherP) return;
+  pl.bwd.erase(std::remove_if(pl.bwd.begin(), pl.bwd.end(), [](const Step &s) { return s.layer == 0; }),
+               pl.bwd.end());
+  for (int w = 0; w < pl.n; ++w) {
+    pl.theta_pass[static_cast<size_t>(w)] = -1;
+    pl.theta_slot[static_cast<size_t>(w)] = -1;
+  }
+  pl.phi_pass[0] = -1;
+  pl.layer0_kernel = true;
+  pl.layer0_grid = static_cast<int>(std::min<u64>(u64{1} << (pl.n - 12), static_cast<u64>(std::max(1, sms))));
 }
 
 void use_half_tiles(Plan &pl, int sms) {
@@ -359,6 +385,7 @@ Plan make_plan_full(int n, int L, int sms, bool checkpoint);
 Plan make_plan(int n, int L, int sms, bool checkpoint = false) {
   Plan pl = make_plan_full(n, L, sms, checkpoint);
   use_half_tiles(pl, sms);
+  use_layer0_kernel(pl, sms);
   return pl;
 }
 
@@ -521,6 +548,10 @@ std::vector<int> undo_order(const Plan &pl) {
       start = false;
     }
   }
+  if (ord.empty() && pl.layer0_kernel) {
+    // one layer, computed by the layer-0 kernel: no gradient correction is used
+    for (int w = 0; w < pl.n; ++w) ord.push_back(w);
+  }
   if (static_cast<int>(ord.size()) != pl.n) throw Error(RSV_ERR_INTERNAL, "undo order incomplete");
   return ord;
 }
@@ -593,6 +624,8 @@ std::string describe(const Plan &pl) {
        << "(" << s.psi_out << ") lam:" << load_name(s.lam_load) << "(" << s.lam_in << ")->"
        << store_name(s.lam_store) << "(" << s.lam_out << ")" << (s.phase ? " phase" : "")
        << (s.phi_grad ? " phi" : "") << " grid=" << s.grid << "\n";
+  if (pl.layer0_kernel)
+    os << "layer0 lam:" << load_name(pl.layer0_load) << "(" << pl.layer0_lam << ") grid=" << pl.layer0_grid << "\n";
   os << "finalize\n";
   return os.str();
 }
@@ -670,6 +703,7 @@ struct rsv_backend {
   rsv::DevBuf<double4> coef;
   rsv::DevBuf<double2> ptab, prod;
   rsv::DevBuf<double> energy_partials, pass_partials, outputs;  // outputs: [1 + num_params]
+  rsv::DevBuf<double> layer0_partials;                           // [layer0_grid][kLayer0Stride]
   rsv::DevBuf<int> tables;  // pass_grid | theta_pass | theta_slot | phi_pass
   rsv::DevBuf<int> order;   // undo order of the wires within a backward layer
   rsv::DevBuf<double2> rot;
@@ -844,12 +878,28 @@ void run_energy(rsv_backend *B, cudaStream_t st) {
   });
 }
 
+Layer0Params layer0_params(rsv_backend *B) {
+  Layer0Params Q{};
+  Q.n = B->n;
+  Q.gather = B->plan.layer0_load == kLoadGatherP ? 1 : 0;
+  Q.coef = B->coef.p;
+  Q.lam = state_buf(B, B->plan.layer0_lam);
+  Q.num_tiles = u64{1} << (B->n - 12);
+  Q.partials = B->layer0_partials.p;
+  return Q;
+}
+
 void run_backward(rsv_backend *B, cudaStream_t st) {
   PassParams P;
   for (const auto &s : B->plan.bwd) {
     fill_pass_params(B, s, P);
     timed(B, st, 3, pass_bytes(B, s),
           [&] { check(launch_pass(P, true, s.grid, st), "backward pass launch"); });
+  }
+  if (B->plan.layer0_kernel) {
+    const Layer0Params Q = layer0_params(B);
+    timed(B, st, 3, 16.0 * static_cast<double>(u64{1} << B->n),
+          [&] { check(launch_layer0_grad(Q, B->plan.layer0_grid, st), "layer-0 gradient launch"); });
   }
 }
 
@@ -872,6 +922,12 @@ void run_finalize(rsv_backend *B, bool grad, double *energy_out, double *grad_ou
   F.energy_out = energy_out;
   F.grad_out = grad ? grad_out : nullptr;
   timed(B, st, 4, 0.0, [&] { check(launch_finalize(F, st), "finalize launch"); });
+  if (grad && B->plan.layer0_kernel) {
+    const Layer0Params Q = layer0_params(B);
+    timed(B, st, 4, 0.0, [&] {
+      check(launch_layer0_finalize(Q, B->plan.layer0_grid, grad_out, st), "layer-0 finalize launch");
+    });
+  }
 }
 
 void upload_host_coefs(rsv_backend *B, const double *params, cudaStream_t st) {
@@ -1291,6 +1347,7 @@ void setup_plan(rsv_backend *B, int mode) {
   B->backward_mode = mode;
   B->num_bwd_passes = static_cast<int>(B->plan.bwd.size());
   B->prod.alloc(1024 * (1 + B->plan.partial_masks.size()));
+  B->layer0_partials.alloc(static_cast<size_t>(B->plan.layer0_grid) * kLayer0Stride);
   B->pass_partials.alloc(static_cast<size_t>(std::max(1, B->num_bwd_passes)) * B->plan.max_grid *
                          kPartialStride);
   std::vector<int> tab;

@@ -309,6 +309,7 @@ __global__ void finalize_kernel(const FinalizeParams F) {
   for (int k = t; k < np; k += blockDim.x) {
     const int layer = k / F.n;
     const int w = k % F.n;
+    if (F.theta_pass[k] < 0) continue;  // layer 0 on the layer-0 kernel
     {
       const int pass = F.theta_pass[k];
       const int slot = F.theta_slot[k];

@@ -24,5 +24,9 @@ cudaError_t launch_bwd_half(const PassParams &P, int grid, cudaStream_t s);
 cudaError_t launch_energy(const double2 *chi, double2 *mu, int n, double field,
                           unsigned long long size, double *partials, int grid, int sms, cudaStream_t s);
 cudaError_t launch_finalize(const FinalizeParams &F, cudaStream_t s);
+// layer-0 gradients in one read of lambda (n >= 13), and their final reduction
+// into grad_out[0 .. 2n)
+cudaError_t launch_layer0_grad(const Layer0Params &Q, int grid, cudaStream_t s);
+cudaError_t launch_layer0_finalize(const Layer0Params &Q, int grid, double *grad_out, cudaStream_t s);
 
 }  // namespace rsv

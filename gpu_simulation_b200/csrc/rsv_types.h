@@ -77,6 +77,18 @@ struct PassParams {
   int tile_bits;               // 12, or 11 for a backward pass on the half tile (rsv_pass_half.cu)
 };
 
+// Layer-0 gradients from lambda alone (rsv_layer0.cu): per-CTA records of
+// S_w(0), S_w(1) (complex) for w < 32.
+constexpr int kLayer0Stride = 128;
+struct Layer0Params {
+  int n;
+  int gather;                  // lambda0(p) = lam[P(p)] (1) or lam[p] (0)
+  const double4 *coef;         // layer-0 coefficients [n]
+  const double2 *lam;
+  unsigned long long num_tiles;  // 2^(n-12)
+  double *partials;            // [grid][kLayer0Stride]
+};
+
 // Inputs of the deterministic final reduction (energy + gradient).
 struct FinalizeParams {
   int n, L;

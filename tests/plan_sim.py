@@ -49,7 +49,14 @@ def parse_plan(text: str) -> dict:
     head = dict(kv.split("=") for kv in lines[0].split())
     steps = []
     energy = None
+    layer0 = None
     for ln in lines[1:]:
+        if ln.startswith("layer0"):
+            m0 = re.match(r"layer0 lam:(\w+)\((-?\d+)\) grid=(\d+)", ln)
+            if not m0:
+                raise ValueError(f"cannot parse plan line: {ln}")
+            layer0 = dict(load=m0[1], buf=int(m0[2]), grid=int(m0[3]))
+            continue
         if ln.startswith("energy"):
             kv = dict(x.split("=") for x in ln.split()[1:])
             energy = (int(kv["chi"]), int(kv["mu"]))
@@ -74,7 +81,7 @@ def parse_plan(text: str) -> dict:
             phase=" phase" in m["flags"], phi=" phi" in m["flags"], grid=int(m["grid"]),
         ))
     return dict(n=int(head["n"]), L=int(head["L"]), phys=int(head["phys"]), steps=steps,
-                energy=energy, bufs=int(head["bufs"]), mode=head["mode"])
+                energy=energy, bufs=int(head["bufs"]), mode=head["mode"], layer0=layer0)
 
 
 def ring_p(i: np.ndarray, n: int) -> np.ndarray:
@@ -211,6 +218,24 @@ def simulate(n: int, layers: int, field: float, params: np.ndarray, check_indice
     theta = np.zeros((layers, n))
     phi = np.zeros((layers, n))
     energy = None
+
+    def energy_step():
+        chi_b, mu_b = plan["energy"]
+        chi = bufs[chi_b]
+        real = idx < (1 << n)
+        pi = ring_p(idx, n) & ((1 << n) - 1)
+        rot = ((pi << 1) & ((1 << n) - 1)) | (pi >> (n - 1))
+        walls = np.zeros(size, dtype=np.int64)
+        x = pi ^ rot
+        for w in range(n):
+            walls += (x >> w) & 1
+        mu = (2.0 * walls - n) * chi
+        for w in range(n):
+            mu = mu - field * chi[idx ^ int(ring_pinv(np.array([1 << w]), n)[0])]
+        mu = np.where(real, mu, 0.0)
+        bufs[mu_b][:] = mu
+        return float(np.sum((np.conj(chi) * mu).real))
+
     for st in plan["steps"]:
         if check_indices:
             ids = tile_indices(st)
@@ -231,22 +256,7 @@ def simulate(n: int, layers: int, field: float, params: np.ndarray, check_indice
             store(st["psi_store"], st["psi_out"], a)
             continue
         if energy is None:
-            chi_b, mu_b = plan["energy"]
-            chi = bufs[chi_b]
-            mu = np.zeros(size, dtype=np.complex128)
-            real = idx < (1 << n)
-            pi = ring_p(idx, n) & ((1 << n) - 1)
-            rot = ((pi << 1) & ((1 << n) - 1)) | (pi >> (n - 1))
-            walls = np.zeros(size, dtype=np.int64)
-            x = pi ^ rot
-            for w in range(n):
-                walls += (x >> w) & 1
-            mu = (2.0 * walls - n) * chi
-            for w in range(n):
-                mu = mu - field * chi[idx ^ int(ring_pinv(np.array([1 << w]), n)[0])]
-            mu = np.where(real, mu, 0.0)
-            energy = float(np.sum((np.conj(chi) * mu).real))
-            bufs[mu_b][:] = mu
+            energy = energy_step()
         a = load(st["psi_load"], st["psi_in"])
         b = load(st["lam_load"], st["lam_in"])
         if st["phase"]:
@@ -267,5 +277,26 @@ def simulate(n: int, layers: int, field: float, params: np.ndarray, check_indice
             b[lo], b[lo | m] = cc * b0 + ss * b1, -ss * b0 + cc * b1
         store(st["psi_store"], st["psi_out"], a)
         store(st["lam_store"], st["lam_out"], b)
+    if energy is None:
+        energy = energy_step()
+    if plan["layer0"] is not None:
+        # layer 0 from lambda alone: 2 Re <lambda0 | d psi0>, psi0 the product state
+        l0 = plan["layer0"]
+        lam0 = load(l0["load"], l0["buf"])
+        a0 = c[0] * (ch[0] - 1j * sh[0])  # a_w(0)
+        a1 = s[0] * (ch[0] + 1j * sh[0])  # a_w(1)
+        for w in range(n):
+            rest = np.ones(size, dtype=np.complex128)
+            for v in range(n):
+                if v != w:
+                    rest *= np.where(bits[:, v] == 1, a1[v], a0[v])
+            rest = np.where(idx < (1 << n), rest, 0.0)
+            cl = np.conj(lam0) * rest
+            S0, S1 = cl[bits[:, w] == 0].sum(), cl[bits[:, w] == 1].sum()
+            e_m, e_p = ch[0, w] - 1j * sh[0, w], ch[0, w] + 1j * sh[0, w]
+            dt0, dt1 = -0.5 * s[0, w] * e_m, 0.5 * c[0, w] * e_p
+            dp0, dp1 = -0.5j * a0[w], 0.5j * a1[w]
+            theta[0, w] = 2.0 * (dt0 * S0 + dt1 * S1).real
+            phi[0, w] = 2.0 * (dp0 * S0 + dp1 * S1).real
     grad = np.stack([theta, phi], axis=-1).reshape(-1)
     return energy, grad

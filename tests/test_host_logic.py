@@ -93,6 +93,12 @@ def check_large_plan(plan, n, L):
                 key = (st["layer"], w)
                 assert key not in seen
                 seen[key] = st["pass_index"]
+    if plan["layer0"] is not None:
+        # layer 0 is one read of lambda on the layer-0 kernel, no backward pass
+        assert all(layer != 0 for layer, _ in seen)
+        assert 0 <= plan["layer0"]["buf"] < plan["bufs"]
+        for w in range(n):
+            seen[(0, w)] = -1
     assert len(seen) == n * L
     # at most three backward passes per layer for these sizes
     bwd = [s for s in plan["steps"] if s["bwd"]]
