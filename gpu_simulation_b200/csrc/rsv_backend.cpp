@@ -236,7 +236,7 @@ void use_layer0_kernel(Plan &pl, int sms) {
   }
   pl.phi_pass[0] = -1;
   pl.layer0_kernel = true;
-  pl.layer0_grid = static_cast<int>(std::min<u64>(u64{1} << (pl.n - 12), static_cast<u64>(std::max(1, sms))));
+  pl.layer0_grid = static_cast<int>(std::min<u64>(u64{1} << (pl.n - 12), static_cast<u64>(2 * std::max(1, sms))));
 }
 
 void use_half_tiles(Plan &pl, int sms) {

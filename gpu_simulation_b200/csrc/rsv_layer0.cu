@@ -14,7 +14,7 @@
 // from one pass that only reads lambda.
 //
 // Tiles are 4096 contiguous indices p (index bits 0..11; coset = bits 12..n-1,
-// n >= 13).  Per tile, with c(p) = conj(lambda0(p)) split as c(h, a) (a = bits
+// n >= 13), loaded straight into registers (two 256-thread CTAs per SM).  Per tile, with c(p) = conj(lambda0(p)) split as c(h, a) (a = bits
 // 0..5, h = bits 6..11):
 //   X1(a) = sum_h c(h, a) W2(h),  X2(h) = sum_a c(h, a) W1(a)
 // (W1, W2 = products of a_v over wires 0..5 and 6..11), then the in-tile
@@ -30,12 +30,8 @@
 namespace rsv {
 namespace {
 
-constexpr int kL0Threads = 512;
-constexpr int kL0Tile = 4096;
-constexpr int kL0Per = kL0Tile / kL0Threads;  // 8 loads per thread and tile
-
-// stage slot of tile index i: the X2 sums read i = a + 64 h across lanes h
-__device__ __forceinline__ int l0_slot(int i) { return i ^ ((i >> 6) & 7); }
+constexpr int kL0Threads = 256;
+constexpr int kL0Warps = kL0Threads / 32;
 
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 // conj(x) * w
@@ -52,20 +48,21 @@ __device__ __forceinline__ double2 warp_sum2(double2 v) {
   return v;
 }
 
-__global__ void __launch_bounds__(kL0Threads, 1) layer0_grad_kernel(const Layer0Params Q) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double2 *stage = reinterpret_cast<double2 *>(smem_raw);  // [2][kL0Tile]
-  __shared__ double2 amp[32][2];      // a_w(b)
-  __shared__ double2 w1[64], w2[64];  // products over wires 0..5 / 6..11
-  __shared__ double2 loo[12][64];     // loo[j][x]: w1 (j < 6) or w2 (j >= 6) without wire j
-  __shared__ double2 xp[4][128];      // partial X1 (0..63) / X2 (64..127) sums
-  __shared__ double2 lsum[25];        // L_w(b) at 2w + b, T at 24
+// Thread (lane, warp) holds c(a, h) for a = lane + 32 a5 (a5 = 0, 1) and
+// h = 8 warp + j (j = 0..7): rows of 32 contiguous amplitudes per load.
+__global__ void __launch_bounds__(kL0Threads, 2) layer0_grad_kernel(const Layer0Params Q) {
+  __shared__ double2 amp[32][2];          // a_w(b)
+  __shared__ double2 w1[64], w2[64];      // products over wires 0..5 / 6..11
+  __shared__ double2 loo[12][64];         // loo[j][x]: w1 (j < 6) or w2 (j >= 6) without wire j
+  __shared__ double2 x1p[kL0Warps][64];   // per-warp partial X1
+  __shared__ double2 x2s[64];             // X2
+  __shared__ double2 lsum[25];            // L_w(b) at 2w + b, T at 24
 
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int n = Q.n;
   if (t < 64) {
     const int w = t >> 1, b = t & 1;
-    double2 v = make_double2(b ? 0.0 : 1.0, 0.0);  // wires >= n: |0> (not used for n >= 13)
+    double2 v = make_double2(b ? 0.0 : 1.0, 0.0);
     if (w < n) {
       const double4 k = Q.coef[w];
       // (c e^{-i phi/2}, s e^{+i phi/2})
@@ -88,71 +85,81 @@ __global__ void __launch_bounds__(kL0Threads, 1) layer0_grad_kernel(const Layer0
     loo[j][x] = p;
   }
   __syncthreads();
-
-  const u64 num_tiles = Q.num_tiles;
-  auto issue = [&](u64 tile, double2 *buf) {
-    if (tile < num_tiles) {
-      const u64 base = tile << 12;
+  // this thread's weights: W1 of its two a, W2 of its eight h
+  const double2 wa0 = w1[lane], wa1 = w1[lane + 32];
+  double2 wh[8];
 #pragma unroll
-      for (int r = 0; r < kL0Per; ++r) {
-        const int tau = t + r * kL0Threads;
-        const u64 p = base | static_cast<u64>(tau);
-        const u64 src = Q.gather ? ring_p(p, n) : p;
-        cp_async16(&buf[l0_slot(tau)], &Q.lam[src]);
-      }
-    }
-    cp_async_commit();
-  };
-  issue(blockIdx.x, stage);
-  issue(blockIdx.x + gridDim.x, stage + kL0Tile);
+  for (int j = 0; j < 8; ++j) wh[j] = w2[8 * warp + j];
 
   // accumulators: lane l of warp 0 keeps S_l(0), S_l(1)
   double2 s0 = make_double2(0.0, 0.0), s1 = make_double2(0.0, 0.0);
-  int k = 0;
-  for (u64 tile = blockIdx.x; tile < num_tiles; tile += gridDim.x, ++k) {
-    double2 *buf = stage + (k & 1) * kL0Tile;
-    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-    __syncthreads();
-    {
-      // partial X1 / X2: q = warp group (4 x 4 warps), o = output
-      const int q = t >> 7, o = t & 127;
-      double2 acc = make_double2(0.0, 0.0);
-      if (o < 64) {
-#pragma unroll 4
-        for (int kk = 0; kk < 16; ++kk) {
-          const int h = 16 * q + kk;
-          acc = cadd(acc, cjmul(buf[l0_slot(o + 64 * h)], w2[h]));
-        }
-      } else {
-        const int h = o - 64;
-#pragma unroll 4
-        for (int kk = 0; kk < 16; ++kk) {
-          const int a = 16 * q + kk;
-          acc = cadd(acc, cjmul(buf[l0_slot(a + 64 * h)], w1[a]));
+  const u64 num_tiles = Q.num_tiles;
+  for (u64 tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
+    const u64 base = tile << 12;
+    double2 c[2][8];
+#pragma unroll
+    for (int a5 = 0; a5 < 2; ++a5)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const u64 p = base | static_cast<u64>(lane + 32 * a5 + 64 * (8 * warp + j));
+        c[a5][j] = __ldcs(&Q.lam[Q.gather ? ring_p(p, n) : p]);
+      }
+    // X1 partials (sum over this warp's eight h) and X2 rows (sum over the 64 a)
+    double2 x1a = make_double2(0.0, 0.0), x1b = make_double2(0.0, 0.0);
+    double2 x2[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      x1a = cadd(x1a, cjmul(c[0][j], wh[j]));
+      x1b = cadd(x1b, cjmul(c[1][j], wh[j]));
+      x2[j] = cadd(cjmul(c[0][j], wa0), cjmul(c[1][j], wa1));
+    }
+    // reduce-scatter the eight X2 rows over the lanes: after the three
+    // exchanges lane l holds row j = l >> 2 summed over 8 lanes
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      const int m = 16 >> s, cnt = 4 >> s;
+      const bool up = (lane & m) != 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (q < cnt) {
+          const double2 send = up ? x2[q] : x2[q + cnt];
+          const double2 keep = up ? x2[q + cnt] : x2[q];
+          x2[q] = cadd(keep, shfl_xor2(send, m));
         }
       }
-      xp[q][o] = acc;
     }
+    double2 xr = cadd(x2[0], shfl_xor2(x2[0], 1));
+    xr = cadd(xr, shfl_xor2(xr, 2));
+    __syncthreads();  // the previous tile's readers of x1p / x2s / lsum are done
+    x1p[warp][lane] = x1a;
+    x1p[warp][lane + 32] = x1b;
+    if ((lane & 3) == 0) x2s[8 * warp + (lane >> 2)] = xr;
     __syncthreads();
-    // buf is free: prefetch the tile after next
-    issue(tile + 2 * static_cast<u64>(gridDim.x), buf);
-    for (int out = warp; out < 25; out += kL0Threads / 32) {
+    for (int out = warp; out < 25; out += kL0Warps) {
       // output 2w + b (w < 12) -> L_w(b); 24 -> T
       double2 v = make_double2(0.0, 0.0);
       if (out < 24) {
         const int w = out >> 1, b = out & 1;
-        const int off = w < 6 ? 0 : 64;
         const int bit = w < 6 ? w : w - 6;
         // the 32 indices x of the 6-bit half with bit `bit` = b
         const int lo = lane & ((1 << bit) - 1), hi = lane >> bit;
         const int x = lo | (b << bit) | (hi << (bit + 1));
-        const double2 X = cadd(cadd(xp[0][off + x], xp[1][off + x]), cadd(xp[2][off + x], xp[3][off + x]));
+        double2 X;
+        if (w < 6) {
+          X = x1p[0][x];
+#pragma unroll
+          for (int ww = 1; ww < kL0Warps; ++ww) X = cadd(X, x1p[ww][x]);
+        } else {
+          X = x2s[x];
+        }
         v = cmul(X, loo[w][x]);
       } else {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const int x = lane + 32 * h;
-          const double2 X = cadd(cadd(xp[0][x], xp[1][x]), cadd(xp[2][x], xp[3][x]));
+          double2 X = x1p[0][x];
+#pragma unroll
+          for (int ww = 1; ww < kL0Warps; ++ww) X = cadd(X, x1p[ww][x]);
           v = cadd(v, cmul(X, w1[x]));
         }
       }
@@ -162,10 +169,9 @@ __global__ void __launch_bounds__(kL0Threads, 1) layer0_grad_kernel(const Layer0
     __syncthreads();
     if (warp == 0) {
       // coset factors of this tile (wires 12..n-1)
-      const u64 cb = tile << 12;
       double2 all = make_double2(1.0, 0.0), others = make_double2(1.0, 0.0);
       for (int v = 12; v < n; ++v) {
-        const double2 A = amp[v][(cb >> v) & 1];
+        const double2 A = amp[v][(base >> v) & 1];
         all = cmul(all, A);
         if (v != lane) others = cmul(others, A);
       }
@@ -173,13 +179,12 @@ __global__ void __launch_bounds__(kL0Threads, 1) layer0_grad_kernel(const Layer0
         s0 = cadd(s0, cmul(all, lsum[2 * lane]));
         s1 = cadd(s1, cmul(all, lsum[2 * lane + 1]));
       } else if (lane < n) {
-        const double2 c = cmul(others, lsum[24]);
-        if ((cb >> lane) & 1) s1 = cadd(s1, c);
-        else s0 = cadd(s0, c);
+        const double2 cc = cmul(others, lsum[24]);
+        if ((base >> lane) & 1) s1 = cadd(s1, cc);
+        else s0 = cadd(s0, cc);
       }
     }
   }
-  cp_async_wait_all();
   if (warp == 0) {
     double *rec = Q.partials + static_cast<size_t>(blockIdx.x) * kLayer0Stride;
     rec[4 * lane + 0] = s0.x;
@@ -214,18 +219,9 @@ __global__ void layer0_finalize_kernel(const Layer0Params Q, int grid, double *g
 
 }  // namespace
 
-size_t layer0_smem_bytes() { return 2 * kL0Tile * sizeof(double2); }
-
 cudaError_t launch_layer0_grad(const Layer0Params &Q, int grid, cudaStream_t s) {
   if (Q.n < 13 || Q.n > 31 || grid < 1) return cudaErrorInvalidValue;
-  static bool configured = false;
-  if (!configured) {
-    const cudaError_t e = cudaFuncSetAttribute(layer0_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               static_cast<int>(layer0_smem_bytes()));
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
-  layer0_grad_kernel<<<grid, kL0Threads, layer0_smem_bytes(), s>>>(Q);
+  layer0_grad_kernel<<<grid, kL0Threads, 0, s>>>(Q);
   return cudaGetLastError();
 }
 
