@@ -175,6 +175,10 @@ struct Plan {
   // through P when layer0_load is kLoadGatherP)
   bool layer0_kernel = false;
   int layer0_lam = -1, layer0_load = kLoadNatural, layer0_grid = 1;
+  // layers 0 and 1 on the grad01 kernel (rsv_mps01.cu, L >= 2): their
+  // backward passes are dropped; lambda1 is read from buffer grad01_lam
+  bool grad01 = false;
+  int grad01_lam = -1, grad01_load = kLoadNatural, grad01_grid = 1;
 };
 
 // Checkpoint-mode plans keep max((L-1) * passes + 1, 2) state buffers; they
@@ -237,6 +241,29 @@ void use_layer0_kernel(Plan &pl, int sms) {
   pl.phi_pass[0] = -1;
   pl.layer0_kernel = true;
   pl.layer0_grid = static_cast<int>(std::min<u64>(u64{1} << (pl.n - 12), static_cast<u64>(2 * std::max(1, sms))));
+}
+
+// Layers 0 and 1 together form a bond-2 matrix-product state, so with
+// L >= 2 and n >= 13 their 4n gradients come from one read of lambda at
+// layer 1's output on the grad01 kernel, replacing both layers' backward
+// passes.
+bool use_grad01(Plan &pl, int sms) {
+  if (pl.n < 13 || pl.L < 2) return false;
+  auto first = std::find_if(pl.bwd.begin(), pl.bwd.end(), [](const Step &s) { return s.layer == 1; });
+  if (first == pl.bwd.end()) return false;
+  if (first->lam_load != kLoadNatural && first->lam_load != kLoadGatherP) return false;
+  pl.grad01_lam = first->lam_in;
+  pl.grad01_load = first->lam_load;
+  pl.bwd.erase(std::remove_if(pl.bwd.begin(), pl.bwd.end(), [](const Step &s) { return s.layer <= 1; }),
+               pl.bwd.end());
+  for (int k = 0; k < 2 * pl.n; ++k) {
+    pl.theta_pass[static_cast<size_t>(k)] = -1;
+    pl.theta_slot[static_cast<size_t>(k)] = -1;
+  }
+  pl.phi_pass[0] = pl.phi_pass[1] = -1;
+  pl.grad01 = true;
+  pl.grad01_grid = static_cast<int>(std::min<u64>(u64{1} << (pl.n - 12), static_cast<u64>(2 * std::max(1, sms))));
+  return true;
 }
 
 void use_half_tiles(Plan &pl, int sms) {
@@ -385,7 +412,7 @@ Plan make_plan_full(int n, int L, int sms, bool checkpoint);
 Plan make_plan(int n, int L, int sms, bool checkpoint = false) {
   Plan pl = make_plan_full(n, L, sms, checkpoint);
   use_half_tiles(pl, sms);
-  use_layer0_kernel(pl, sms);
+  if (!use_grad01(pl, sms)) use_layer0_kernel(pl, sms);
   return pl;
 }
 
@@ -548,7 +575,7 @@ std::vector<int> undo_order(const Plan &pl) {
       start = false;
     }
   }
-  if (ord.empty() && pl.layer0_kernel) {
+  if (ord.empty() && (pl.layer0_kernel || pl.grad01)) {
     // one layer, computed by the layer-0 kernel: no gradient correction is used
     for (int w = 0; w < pl.n; ++w) ord.push_back(w);
   }
@@ -624,6 +651,8 @@ std::string describe(const Plan &pl) {
        << "(" << s.psi_out << ") lam:" << load_name(s.lam_load) << "(" << s.lam_in << ")->"
        << store_name(s.lam_store) << "(" << s.lam_out << ")" << (s.phase ? " phase" : "")
        << (s.phi_grad ? " phi" : "") << " grid=" << s.grid << "\n";
+  if (pl.grad01)
+    os << "grad01 lam:" << load_name(pl.grad01_load) << "(" << pl.grad01_lam << ") grid=" << pl.grad01_grid << "\n";
   if (pl.layer0_kernel)
     os << "layer0 lam:" << load_name(pl.layer0_load) << "(" << pl.layer0_lam << ") grid=" << pl.layer0_grid << "\n";
   os << "finalize\n";
@@ -704,6 +733,7 @@ struct rsv_backend {
   rsv::DevBuf<double2> ptab, prod;
   rsv::DevBuf<double> energy_partials, pass_partials, outputs;  // outputs: [1 + num_params]
   rsv::DevBuf<double> layer0_partials;                           // [layer0_grid][kLayer0Stride]
+  rsv::DevBuf<double> grad01_partials;                           // [grad01_grid][kGrad01Stride]
   rsv::DevBuf<int> tables;  // pass_grid | theta_pass | theta_slot | phi_pass
   rsv::DevBuf<int> order;   // undo order of the wires within a backward layer
   rsv::DevBuf<double2> rot;
@@ -889,6 +919,17 @@ Layer0Params layer0_params(rsv_backend *B) {
   return Q;
 }
 
+Grad01Params grad01_params(rsv_backend *B) {
+  Grad01Params Q{};
+  Q.n = B->n;
+  Q.gather = B->plan.grad01_load == kLoadGatherP ? 1 : 0;
+  Q.coef = B->coef.p;
+  Q.lam = state_buf(B, B->plan.grad01_lam);
+  Q.num_tiles = u64{1} << (B->n - 12);
+  Q.partials = B->grad01_partials.p;
+  return Q;
+}
+
 void run_backward(rsv_backend *B, cudaStream_t st) {
   PassParams P;
   for (const auto &s : B->plan.bwd) {
@@ -900,6 +941,11 @@ void run_backward(rsv_backend *B, cudaStream_t st) {
     const Layer0Params Q = layer0_params(B);
     timed(B, st, 3, 16.0 * static_cast<double>(u64{1} << B->n),
           [&] { check(launch_layer0_grad(Q, B->plan.layer0_grid, st), "layer-0 gradient launch"); });
+  }
+  if (B->plan.grad01) {
+    const Grad01Params Q = grad01_params(B);
+    timed(B, st, 3, 16.0 * static_cast<double>(u64{1} << B->n),
+          [&] { check(launch_grad01(Q, B->plan.grad01_grid, st), "layers 0-1 gradient launch"); });
   }
 }
 
@@ -922,6 +968,12 @@ void run_finalize(rsv_backend *B, bool grad, double *energy_out, double *grad_ou
   F.energy_out = energy_out;
   F.grad_out = grad ? grad_out : nullptr;
   timed(B, st, 4, 0.0, [&] { check(launch_finalize(F, st), "finalize launch"); });
+  if (grad && B->plan.grad01) {
+    const Grad01Params Q = grad01_params(B);
+    timed(B, st, 4, 0.0, [&] {
+      check(launch_grad01_finalize(Q, B->plan.grad01_grid, grad_out, st), "layers 0-1 finalize launch");
+    });
+  }
   if (grad && B->plan.layer0_kernel) {
     const Layer0Params Q = layer0_params(B);
     timed(B, st, 4, 0.0, [&] {
@@ -1348,6 +1400,7 @@ void setup_plan(rsv_backend *B, int mode) {
   B->num_bwd_passes = static_cast<int>(B->plan.bwd.size());
   B->prod.alloc(1024 * (1 + B->plan.partial_masks.size()));
   B->layer0_partials.alloc(static_cast<size_t>(B->plan.layer0_grid) * kLayer0Stride);
+  B->grad01_partials.alloc(static_cast<size_t>(B->plan.grad01_grid) * kGrad01Stride);
   B->pass_partials.alloc(static_cast<size_t>(std::max(1, B->num_bwd_passes)) * B->plan.max_grid *
                          kPartialStride);
   std::vector<int> tab;

@@ -28,5 +28,9 @@ cudaError_t launch_finalize(const FinalizeParams &F, cudaStream_t s);
 // into grad_out[0 .. 2n)
 cudaError_t launch_layer0_grad(const Layer0Params &Q, int grid, cudaStream_t s);
 cudaError_t launch_layer0_finalize(const Layer0Params &Q, int grid, double *grad_out, cudaStream_t s);
+// layers 0 and 1 in one read of lambda (n >= 13, L >= 2), and their final
+// reduction into grad_out[0 .. 4n)
+cudaError_t launch_grad01(const Grad01Params &Q, int grid, cudaStream_t s);
+cudaError_t launch_grad01_finalize(const Grad01Params &Q, int grid, double *grad_out, cudaStream_t s);
 
 }  // namespace rsv

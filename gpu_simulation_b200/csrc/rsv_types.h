@@ -89,6 +89,19 @@ struct Layer0Params {
   double *partials;            // [grid][kLayer0Stride]
 };
 
+// Layers 0 and 1 from one read of lambda (rsv_mps01.cu): per-CTA records of
+// G(a), F(h) (64 2x2 complex matrices each) and the coset environments
+// E_v[b] (32 x 2 matrices).
+constexpr int kGrad01Stride = 1536;
+struct Grad01Params {
+  int n;
+  int gather;                  // lambda1(r) = lam[P(r)] (1) or lam[r] (0)
+  const double4 *coef;         // layer 0 at [0, n), layer 1 at [n, 2n)
+  const double2 *lam;
+  unsigned long long num_tiles;  // 2^(n-12)
+  double *partials;            // [grid][kGrad01Stride]
+};
+
 // Inputs of the deterministic final reduction (energy + gradient).
 struct FinalizeParams {
   int n, L;

@@ -50,7 +50,14 @@ def parse_plan(text: str) -> dict:
     steps = []
     energy = None
     layer0 = None
+    grad01 = None
     for ln in lines[1:]:
+        if ln.startswith("grad01"):
+            m0 = re.match(r"grad01 lam:(\w+)\((-?\d+)\) grid=(\d+)", ln)
+            if not m0:
+                raise ValueError(f"cannot parse plan line: {ln}")
+            grad01 = dict(load=m0[1], buf=int(m0[2]), grid=int(m0[3]))
+            continue
         if ln.startswith("layer0"):
             m0 = re.match(r"layer0 lam:(\w+)\((-?\d+)\) grid=(\d+)", ln)
             if not m0:
@@ -81,7 +88,8 @@ def parse_plan(text: str) -> dict:
             phase=" phase" in m["flags"], phi=" phi" in m["flags"], grid=int(m["grid"]),
         ))
     return dict(n=int(head["n"]), L=int(head["L"]), phys=int(head["phys"]), steps=steps,
-                energy=energy, bufs=int(head["bufs"]), mode=head["mode"], layer0=layer0)
+                energy=energy, bufs=int(head["bufs"]), mode=head["mode"], layer0=layer0,
+                grad01=grad01)
 
 
 def ring_p(i: np.ndarray, n: int) -> np.ndarray:
@@ -298,5 +306,46 @@ def simulate(n: int, layers: int, field: float, params: np.ndarray, check_indice
             dp0, dp1 = -0.5j * a0[w], 0.5j * a1[w]
             theta[0, w] = 2.0 * (dt0 * S0 + dt1 * S1).real
             phi[0, w] = 2.0 * (dp0 * S0 + dp1 * S1).real
+    if plan["grad01"] is not None:
+        # layers 0 and 1 from lambda at layer 1's output: 2 Re <lambda1 | d chi1>,
+        # chi1 = (U1 on every wire) P (U0 on every wire)|0>, by direct simulation
+        g0 = plan["grad01"]
+        lam1 = load(g0["load"], g0["buf"])
+
+        def ry_rz(th, ph, dth=False, dph=False):
+            cc, ss = np.cos(th / 2), np.sin(th / 2)
+            ry = np.array([[-ss / 2, -cc / 2], [cc / 2, -ss / 2]]) if dth else np.array([[cc, -ss], [ss, cc]])
+            rz = np.diag([np.exp(-0.5j * ph), np.exp(0.5j * ph)])
+            if dph:
+                rz = rz @ np.diag([-0.5j, 0.5j])
+            return rz @ ry
+
+        def chi1(u0, u1):
+            amp0 = np.ones(size, dtype=np.complex128)
+            for w in range(phys):
+                b = bits[:, w]
+                if w < n:
+                    amp0 *= np.where(b == 1, u0[w][1, 0], u0[w][0, 0])
+                else:
+                    amp0 *= np.where(b == 1, 0.0, 1.0)
+            out = np.zeros(size, dtype=np.complex128)
+            out[ring_p(idx, n)] = amp0
+            for w in range(n):
+                m = 1 << w
+                lo = idx[(idx & m) == 0]
+                x0, x1 = out[lo].copy(), out[lo | m].copy()
+                u = u1[w]
+                out[lo], out[lo | m] = u[0, 0] * x0 + u[0, 1] * x1, u[1, 0] * x0 + u[1, 1] * x1
+            return out
+
+        base0 = [ry_rz(p[0, w, 0], p[0, w, 1]) for w in range(n)]
+        base1 = [ry_rz(p[1, w, 0], p[1, w, 1]) for w in range(n)]
+        for w in range(n):
+            for layer, (dth, dph) in ((0, (True, False)), (0, (False, True)), (1, (True, False)), (1, (False, True))):
+                u0, u1 = list(base0), list(base1)
+                d = ry_rz(p[layer, w, 0], p[layer, w, 1], dth, dph)
+                (u0 if layer == 0 else u1)[w] = d
+                val = 2.0 * np.sum(np.conj(lam1) * chi1(u0, u1)).real
+                (theta if dth else phi)[layer, w] = val
     grad = np.stack([theta, phi], axis=-1).reshape(-1)
     return energy, grad

@@ -93,6 +93,13 @@ def check_large_plan(plan, n, L):
                 key = (st["layer"], w)
                 assert key not in seen
                 seen[key] = st["pass_index"]
+    if plan["grad01"] is not None:
+        # layers 0 and 1 are one read of lambda on the grad01 kernel
+        assert all(layer > 1 for layer, _ in seen)
+        assert 0 <= plan["grad01"]["buf"] < plan["bufs"]
+        for layer in (0, 1):
+            for w in range(n):
+                seen[(layer, w)] = -1
     if plan["layer0"] is not None:
         # layer 0 is one read of lambda on the layer-0 kernel, no backward pass
         assert all(layer != 0 for layer, _ in seen)
