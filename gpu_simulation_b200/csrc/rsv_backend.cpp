@@ -179,6 +179,10 @@ struct Plan {
   // backward passes are dropped; lambda1 is read from buffer grad01_lam
   bool grad01 = false;
   int grad01_lam = -1, grad01_load = kLoadNatural, grad01_grid = 1;
+  // the forward of layers 0 and 1 as one write of their matrix-product state
+  // (rsv_mps01.cu) into buffer fwd01_out, scattered through P unless L = 2
+  bool fwd01 = false, fwd01_scatter = false;
+  int fwd01_out = -1, fwd01_grid = 1;
 };
 
 // Checkpoint-mode plans keep max((L-1) * passes + 1, 2) state buffers; they
@@ -264,6 +268,23 @@ bool use_grad01(Plan &pl, int sms) {
   pl.grad01 = true;
   pl.grad01_grid = static_cast<int>(std::min<u64>(u64{1} << (pl.n - 12), static_cast<u64>(2 * std::max(1, sms))));
   return true;
+}
+
+// With layers 0 and 1 on the grad01 kernel no backward pass reads layer 1's
+// checkpoints, so its forward passes become one write of chi1.
+void use_fwd01(Plan &pl, int sms) {
+  int last = -1;
+  for (size_t i = 0; i < pl.fwd.size(); ++i)
+    if (pl.fwd[i].layer == 1) last = static_cast<int>(i);
+  if (last < 0) return;
+  const Step &s = pl.fwd[static_cast<size_t>(last)];
+  if (s.psi_store != kStoreNatural && s.psi_store != kStoreScatterP) return;
+  pl.fwd01_out = s.psi_out;
+  pl.fwd01_scatter = s.psi_store == kStoreScatterP;
+  pl.fwd.erase(std::remove_if(pl.fwd.begin(), pl.fwd.end(), [](const Step &x) { return x.layer == 1; }),
+               pl.fwd.end());
+  pl.fwd01 = true;
+  pl.fwd01_grid = static_cast<int>(std::min<u64>(u64{1} << (pl.n - 12), static_cast<u64>(8 * std::max(1, sms))));
 }
 
 void use_half_tiles(Plan &pl, int sms) {
@@ -412,7 +433,8 @@ Plan make_plan_full(int n, int L, int sms, bool checkpoint);
 Plan make_plan(int n, int L, int sms, bool checkpoint = false) {
   Plan pl = make_plan_full(n, L, sms, checkpoint);
   use_half_tiles(pl, sms);
-  if (!use_grad01(pl, sms)) use_layer0_kernel(pl, sms);
+  if (use_grad01(pl, sms)) use_fwd01(pl, sms);
+  else use_layer0_kernel(pl, sms);
   return pl;
 }
 
@@ -632,6 +654,9 @@ std::string describe(const Plan &pl) {
   };
   os << "n=" << pl.n << " L=" << pl.L << " phys=" << pl.phys << " bufs=" << pl.num_bufs
      << " mode=" << (pl.checkpoint ? "checkpoint" : "uncompute") << "\n";
+  if (pl.fwd01)
+    os << "fwd01 psi:" << (pl.fwd01_scatter ? "scatterP" : "store") << "(" << pl.fwd01_out << ") grid=" << pl.fwd01_grid
+       << "\n";
   for (const auto &s : pl.fwd)
     os << "fwd layer=" << s.layer << " " << tile_str(s.tile) << " psi:" << load_name(s.psi_load)
        << "(" << s.psi_in << ")->" << store_name(s.psi_store) << "(" << s.psi_out << ")"
@@ -734,6 +759,7 @@ struct rsv_backend {
   rsv::DevBuf<double> energy_partials, pass_partials, outputs;  // outputs: [1 + num_params]
   rsv::DevBuf<double> layer0_partials;                           // [layer0_grid][kLayer0Stride]
   rsv::DevBuf<double> grad01_partials;                           // [grad01_grid][kGrad01Stride]
+  rsv::DevBuf<double2> mps_btab;                                 // [4][256][4] layer-0/1 byte tables
   rsv::DevBuf<int> tables;  // pass_grid | theta_pass | theta_slot | phi_pass
   rsv::DevBuf<int> order;   // undo order of the wires within a backward layer
   rsv::DevBuf<double2> rot;
@@ -891,6 +917,17 @@ double pass_bytes(const rsv_backend *B, const Step &s) {
 }
 
 void run_forward(rsv_backend *B, cudaStream_t st) {
+  if (B->plan.fwd01) {
+    Fwd01Params Q{};
+    Q.n = B->n;
+    Q.scatter = B->plan.fwd01_scatter ? 1 : 0;
+    Q.coef = B->coef.p;
+    Q.btab = B->mps_btab.p;
+    Q.out = state_buf(B, B->plan.fwd01_out);
+    Q.num_tiles = u64{1} << (B->n - 12);
+    timed(B, st, 1, 16.0 * static_cast<double>(u64{1} << B->n),
+          [&] { check(launch_fwd01(Q, B->plan.fwd01_grid, st), "layers 0-1 forward launch"); });
+  }
   PassParams P;
   for (const auto &s : B->plan.fwd) {
     fill_pass_params(B, s, P);
@@ -1401,6 +1438,7 @@ void setup_plan(rsv_backend *B, int mode) {
   B->prod.alloc(1024 * (1 + B->plan.partial_masks.size()));
   B->layer0_partials.alloc(static_cast<size_t>(B->plan.layer0_grid) * kLayer0Stride);
   B->grad01_partials.alloc(static_cast<size_t>(B->plan.grad01_grid) * kGrad01Stride);
+  B->mps_btab.alloc(4 * 256 * 4);
   B->pass_partials.alloc(static_cast<size_t>(std::max(1, B->num_bwd_passes)) * B->plan.max_grid *
                          kPartialStride);
   std::vector<int> tab;

@@ -32,5 +32,8 @@ cudaError_t launch_layer0_finalize(const Layer0Params &Q, int grid, double *grad
 // reduction into grad_out[0 .. 4n)
 cudaError_t launch_grad01(const Grad01Params &Q, int grid, cudaStream_t s);
 cudaError_t launch_grad01_finalize(const Grad01Params &Q, int grid, double *grad_out, cudaStream_t s);
+// forward of layers 0 and 1 in one write (n >= 13, L >= 2): the byte tables,
+// then chi1 into Q.out
+cudaError_t launch_fwd01(const Fwd01Params &Q, int grid, cudaStream_t s);
 
 }  // namespace rsv

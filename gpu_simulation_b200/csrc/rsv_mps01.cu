@@ -327,7 +327,71 @@ __global__ void __launch_bounds__(256) grad01_finalize_kernel(const Grad01Params
 
 size_t grad01_smem_bytes() { return kG01Tile * sizeof(double2); }
 
+// ---------------------------------------------------------------- forward
+// Byte tables of the layer-0/1 matrix-product state: btab[k][v] = product of
+// T_w[v_{w-8k}] over the eight wires w = 8k..8k+7 (identity beyond n), as
+// four complex entries each.
+__global__ void __launch_bounds__(256) mps_bytes_kernel(const double4 *__restrict__ coef, int n,
+                                                        double2 *__restrict__ btab) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;  // 0 .. 1023
+  if (e >= 1024) return;
+  const int k = e >> 8, v = e & 255;
+  M2x2 p = ident();
+  for (int j = 0; j < 8; ++j) {
+    const int w = 8 * k + j;
+    if (w < n) p = mmul(p, tmat(wire_gates(coef, n, w, 0), w, (v >> j) & 1));
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) btab[4 * e + q] = p.m[q];
+}
+
+__device__ __forceinline__ M2x2 load_m(const double2 *__restrict__ btab, int k, int v) {
+  M2x2 R;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) R.m[q] = __ldg(&btab[4 * (256 * k + v) + q]);
+  return R;
+}
+
+// chi1(r) = Tr(B0[r0] B1[r1] B2[r2] B3[r3]) for 4096 contiguous r per tile;
+// thread t takes r = base + t + 256 k (k = 0..15): byte 0 is t for all its
+// amplitudes, so chi1 = Tr(B1[r1] W) with W = B2 B3 B0[t] fixed per tile.
+// SCATTER stores chi1(r) at P(r) (the input of layer 2), else at r.
+template <bool SCATTER>
+__global__ void __launch_bounds__(256) fwd01_kernel(const Fwd01Params Q) {
+  const int t = threadIdx.x;
+  const int n = Q.n;
+  const M2x2 b0 = load_m(Q.btab, 0, t);
+  for (u64 tile = blockIdx.x; tile < Q.num_tiles; tile += gridDim.x) {
+    const u64 base = tile << 12;
+    const M2x2 W = mmul(mmul(load_m(Q.btab, 2, static_cast<int>((base >> 16) & 255)),
+                             load_m(Q.btab, 3, static_cast<int>((base >> 24) & 255))),
+                        b0);
+    const int hi1 = static_cast<int>((base >> 8) & 0xF0);
+#pragma unroll 4
+    for (int k = 0; k < 16; ++k) {
+      const M2x2 b1 = load_m(Q.btab, 1, hi1 | k);
+      // Tr(b1 W) = sum_{i,j} b1[i][j] W[j][i]
+      double2 v = cmul(b1.m[0], W.m[0]);
+      v = cfma(b1.m[1], W.m[2], v);
+      v = cfma(b1.m[2], W.m[1], v);
+      v = cfma(b1.m[3], W.m[3], v);
+      const u64 r = base | static_cast<u64>(t + 256 * k);
+      __stcs(&Q.out[SCATTER ? ring_p(r, n) : r], v);
+    }
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_fwd01(const Fwd01Params &Q, int grid, cudaStream_t s) {
+  if (Q.n < 13 || Q.n > 31 || grid < 1) return cudaErrorInvalidValue;
+  mps_bytes_kernel<<<4, 256, 0, s>>>(Q.coef, Q.n, Q.btab);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (Q.scatter) fwd01_kernel<true><<<grid, 256, 0, s>>>(Q);
+  else fwd01_kernel<false><<<grid, 256, 0, s>>>(Q);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_grad01(const Grad01Params &Q, int grid, cudaStream_t s) {
   if (Q.n < 13 || Q.n > 31 || grid < 1) return cudaErrorInvalidValue;

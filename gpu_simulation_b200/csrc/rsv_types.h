@@ -102,6 +102,17 @@ struct Grad01Params {
   double *partials;            // [grid][kGrad01Stride]
 };
 
+// Forward of layers 0 and 1 as one write of their matrix-product state
+// (rsv_mps01.cu).
+struct Fwd01Params {
+  int n;
+  int scatter;                 // store chi1(r) at P(r) (1) or at r (0)
+  const double4 *coef;         // layer 0 at [0, n), layer 1 at [n, 2n)
+  double2 *btab;               // [4][256][4] byte tables, rebuilt per call
+  double2 *out;
+  unsigned long long num_tiles;  // 2^(n-12)
+};
+
 // Inputs of the deterministic final reduction (energy + gradient).
 struct FinalizeParams {
   int n, L;

@@ -52,6 +52,12 @@ def parse_plan(text: str) -> dict:
     layer0 = None
     grad01 = None
     for ln in lines[1:]:
+        if ln.startswith("fwd01"):
+            m0 = re.match(r"fwd01 psi:(\w+)\((-?\d+)\) grid=(\d+)", ln)
+            if not m0:
+                raise ValueError(f"cannot parse plan line: {ln}")
+            steps.append(dict(kind="fwd01", store=m0[1], out=int(m0[2]), grid=int(m0[3])))
+            continue
         if ln.startswith("grad01"):
             m0 = re.match(r"grad01 lam:(\w+)\((-?\d+)\) grid=(\d+)", ln)
             if not m0:
@@ -227,6 +233,36 @@ def simulate(n: int, layers: int, field: float, params: np.ndarray, check_indice
     phi = np.zeros((layers, n))
     energy = None
 
+    def ry_rz(th, ph, dth=False, dph=False):
+        cc, ss = np.cos(th / 2), np.sin(th / 2)
+        ry = np.array([[-ss / 2, -cc / 2], [cc / 2, -ss / 2]]) if dth else np.array([[cc, -ss], [ss, cc]])
+        rz = np.diag([np.exp(-0.5j * ph), np.exp(0.5j * ph)])
+        if dph:
+            rz = rz @ np.diag([-0.5j, 0.5j])
+        return rz @ ry
+
+    def chi1(u0, u1):
+        amp0 = np.ones(size, dtype=np.complex128)
+        for w in range(phys):
+            b = bits[:, w]
+            if w < n:
+                amp0 *= np.where(b == 1, u0[w][1, 0], u0[w][0, 0])
+            else:
+                amp0 *= np.where(b == 1, 0.0, 1.0)
+        out = np.zeros(size, dtype=np.complex128)
+        out[ring_p(idx, n)] = amp0
+        for w in range(n):
+            m = 1 << w
+            lo = idx[(idx & m) == 0]
+            x0, x1 = out[lo].copy(), out[lo | m].copy()
+            u = u1[w]
+            out[lo], out[lo | m] = u[0, 0] * x0 + u[0, 1] * x1, u[1, 0] * x0 + u[1, 1] * x1
+        return out
+
+    def mps_chi1():
+        return chi1([ry_rz(p[0, w, 0], p[0, w, 1]) for w in range(n)],
+                    [ry_rz(p[1, w, 0], p[1, w, 1]) for w in range(n)])
+
     def energy_step():
         chi_b, mu_b = plan["energy"]
         chi = bufs[chi_b]
@@ -245,6 +281,10 @@ def simulate(n: int, layers: int, field: float, params: np.ndarray, check_indice
         return float(np.sum((np.conj(chi) * mu).real))
 
     for st in plan["steps"]:
+        if st.get("kind") == "fwd01":
+            # layers 0 and 1: chi1 = (U1 on every wire) P (U0 on every wire)|0>
+            store(st["store"], st["out"], mps_chi1())
+            continue
         if check_indices:
             ids = tile_indices(st)
             if ids.size != size or not np.array_equal(np.sort(ids), idx):
@@ -311,32 +351,6 @@ def simulate(n: int, layers: int, field: float, params: np.ndarray, check_indice
         # chi1 = (U1 on every wire) P (U0 on every wire)|0>, by direct simulation
         g0 = plan["grad01"]
         lam1 = load(g0["load"], g0["buf"])
-
-        def ry_rz(th, ph, dth=False, dph=False):
-            cc, ss = np.cos(th / 2), np.sin(th / 2)
-            ry = np.array([[-ss / 2, -cc / 2], [cc / 2, -ss / 2]]) if dth else np.array([[cc, -ss], [ss, cc]])
-            rz = np.diag([np.exp(-0.5j * ph), np.exp(0.5j * ph)])
-            if dph:
-                rz = rz @ np.diag([-0.5j, 0.5j])
-            return rz @ ry
-
-        def chi1(u0, u1):
-            amp0 = np.ones(size, dtype=np.complex128)
-            for w in range(phys):
-                b = bits[:, w]
-                if w < n:
-                    amp0 *= np.where(b == 1, u0[w][1, 0], u0[w][0, 0])
-                else:
-                    amp0 *= np.where(b == 1, 0.0, 1.0)
-            out = np.zeros(size, dtype=np.complex128)
-            out[ring_p(idx, n)] = amp0
-            for w in range(n):
-                m = 1 << w
-                lo = idx[(idx & m) == 0]
-                x0, x1 = out[lo].copy(), out[lo | m].copy()
-                u = u1[w]
-                out[lo], out[lo | m] = u[0, 0] * x0 + u[0, 1] * x1, u[1, 0] * x0 + u[1, 1] * x1
-            return out
 
         base0 = [ry_rz(p[0, w, 0], p[0, w, 1]) for w in range(n)]
         base1 = [ry_rz(p[1, w, 0], p[1, w, 1]) for w in range(n)]
