@@ -175,14 +175,13 @@ struct Plan {
   // through P when layer0_load is kLoadGatherP)
   bool layer0_kernel = false;
   int layer0_lam = -1, layer0_load = kLoadNatural, layer0_grid = 1;
-  // layers 0 and 1 on the grad01 kernel (rsv_mps01.cu, L >= 2): their
-  // backward passes are dropped; lambda1 is read from buffer grad01_lam
-  bool grad01 = false;
-  int grad01_lam = -1, grad01_load = kLoadNatural, grad01_grid = 1;
-  // the forward of layers 0 and 1 as one write of their matrix-product state
-  // (rsv_mps01.cu) into buffer fwd01_out, scattered through P unless L = 2
-  bool fwd01 = false, fwd01_scatter = false;
-  int fwd01_out = -1, fwd01_grid = 1;
+  // the first mps_k layers as a matrix-product state of bond 2^(mps_k - 1)
+  // (rsv_mps.cu, 0: not used): their passes are dropped; the forward writes
+  // their output into buffer mps_out (scattered through P when layers
+  // follow), the backward reads lambda at that point from buffer mps_lam
+  int mps_k = 0;
+  bool mps_scatter = false;
+  int mps_out = -1, mps_lam = -1, mps_load = kLoadNatural, mps_fwd_grid = 1, mps_grad_grid = 1;
 };
 
 // Checkpoint-mode plans keep max((L-1) * passes + 1, 2) state buffers; they
@@ -247,44 +246,39 @@ void use_layer0_kernel(Plan &pl, int sms) {
   pl.layer0_grid = static_cast<int>(std::min<u64>(u64{1} << (pl.n - 12), static_cast<u64>(2 * std::max(1, sms))));
 }
 
-// Layers 0 and 1 together form a bond-2 matrix-product state, so with
-// L >= 2 and n >= 13 their 4n gradients come from one read of lambda at
-// layer 1's output on the grad01 kernel, replacing both layers' backward
-// passes.
-bool use_grad01(Plan &pl, int sms) {
-  if (pl.n < 13 || pl.L < 2) return false;
-  auto first = std::find_if(pl.bwd.begin(), pl.bwd.end(), [](const Step &s) { return s.layer == 1; });
-  if (first == pl.bwd.end()) return false;
-  if (first->lam_load != kLoadNatural && first->lam_load != kLoadGatherP) return false;
-  pl.grad01_lam = first->lam_in;
-  pl.grad01_load = first->lam_load;
-  pl.bwd.erase(std::remove_if(pl.bwd.begin(), pl.bwd.end(), [](const Step &s) { return s.layer <= 1; }),
+// The first K = min(L, 3) layers form a matrix-product state of bond
+// 2^(K-1) (rsv_mps.cu).  For n >= 13 their forward passes become one write of
+// that state and their backward passes one read of lambda at its output, which
+// gives all their 2nK gradients.
+void use_mps(Plan &pl, int sms) {
+  if (pl.n < 13 || pl.L < 2) return;
+  const int K = std::min(pl.L, 3);
+  int last = -1;
+  for (size_t i = 0; i < pl.fwd.size(); ++i)
+    if (pl.fwd[i].layer == K - 1) last = static_cast<int>(i);
+  auto first = std::find_if(pl.bwd.begin(), pl.bwd.end(), [K](const Step &s) { return s.layer == K - 1; });
+  if (last < 0 || first == pl.bwd.end()) return;
+  const Step &s = pl.fwd[static_cast<size_t>(last)];
+  if (s.psi_store != kStoreNatural && s.psi_store != kStoreScatterP) return;
+  if (first->lam_load != kLoadNatural && first->lam_load != kLoadGatherP) return;
+  pl.mps_out = s.psi_out;
+  pl.mps_scatter = s.psi_store == kStoreScatterP;
+  pl.mps_lam = first->lam_in;
+  pl.mps_load = first->lam_load;
+  pl.fwd.erase(std::remove_if(pl.fwd.begin(), pl.fwd.end(), [K](const Step &x) { return x.layer < K; }),
+               pl.fwd.end());
+  pl.bwd.erase(std::remove_if(pl.bwd.begin(), pl.bwd.end(), [K](const Step &x) { return x.layer < K; }),
                pl.bwd.end());
-  for (int k = 0; k < 2 * pl.n; ++k) {
+  for (int k = 0; k < K * pl.n; ++k) {
     pl.theta_pass[static_cast<size_t>(k)] = -1;
     pl.theta_slot[static_cast<size_t>(k)] = -1;
   }
-  pl.phi_pass[0] = pl.phi_pass[1] = -1;
-  pl.grad01 = true;
-  pl.grad01_grid = static_cast<int>(std::min<u64>(u64{1} << (pl.n - 12), static_cast<u64>(2 * std::max(1, sms))));
-  return true;
-}
-
-// With layers 0 and 1 on the grad01 kernel no backward pass reads layer 1's
-// checkpoints, so its forward passes become one write of chi1.
-void use_fwd01(Plan &pl, int sms) {
-  int last = -1;
-  for (size_t i = 0; i < pl.fwd.size(); ++i)
-    if (pl.fwd[i].layer == 1) last = static_cast<int>(i);
-  if (last < 0) return;
-  const Step &s = pl.fwd[static_cast<size_t>(last)];
-  if (s.psi_store != kStoreNatural && s.psi_store != kStoreScatterP) return;
-  pl.fwd01_out = s.psi_out;
-  pl.fwd01_scatter = s.psi_store == kStoreScatterP;
-  pl.fwd.erase(std::remove_if(pl.fwd.begin(), pl.fwd.end(), [](const Step &x) { return x.layer == 1; }),
-               pl.fwd.end());
-  pl.fwd01 = true;
-  pl.fwd01_grid = static_cast<int>(std::min<u64>(u64{1} << (pl.n - 12), static_cast<u64>(8 * std::max(1, sms))));
+  for (int l = 0; l < K; ++l) pl.phi_pass[static_cast<size_t>(l)] = -1;
+  pl.mps_k = K;
+  const u64 tiles = u64{1} << (pl.n - 12);
+  pl.mps_fwd_grid = static_cast<int>(std::min<u64>(tiles, static_cast<u64>(8 * std::max(1, sms))));
+  // bond 2: two CTAs per SM (83 KiB of shared memory), bond 4: one (135 KiB)
+  pl.mps_grad_grid = static_cast<int>(std::min<u64>(tiles, static_cast<u64>((K == 2 ? 2 : 1) * std::max(1, sms))));
 }
 
 void use_half_tiles(Plan &pl, int sms) {
@@ -433,8 +427,8 @@ Plan make_plan_full(int n, int L, int sms, bool checkpoint);
 Plan make_plan(int n, int L, int sms, bool checkpoint = false) {
   Plan pl = make_plan_full(n, L, sms, checkpoint);
   use_half_tiles(pl, sms);
-  if (use_grad01(pl, sms)) use_fwd01(pl, sms);
-  else use_layer0_kernel(pl, sms);
+  use_mps(pl, sms);
+  if (pl.mps_k == 0) use_layer0_kernel(pl, sms);
   return pl;
 }
 
@@ -597,7 +591,7 @@ std::vector<int> undo_order(const Plan &pl) {
       start = false;
     }
   }
-  if (ord.empty() && (pl.layer0_kernel || pl.grad01)) {
+  if (ord.empty() && (pl.layer0_kernel || pl.mps_k > 0)) {
     // one layer, computed by the layer-0 kernel: no gradient correction is used
     for (int w = 0; w < pl.n; ++w) ord.push_back(w);
   }
@@ -654,9 +648,9 @@ std::string describe(const Plan &pl) {
   };
   os << "n=" << pl.n << " L=" << pl.L << " phys=" << pl.phys << " bufs=" << pl.num_bufs
      << " mode=" << (pl.checkpoint ? "checkpoint" : "uncompute") << "\n";
-  if (pl.fwd01)
-    os << "fwd01 psi:" << (pl.fwd01_scatter ? "scatterP" : "store") << "(" << pl.fwd01_out << ") grid=" << pl.fwd01_grid
-       << "\n";
+  if (pl.mps_k > 0)
+    os << "mps K=" << pl.mps_k << " fwd psi:" << (pl.mps_scatter ? "scatterP" : "store") << "(" << pl.mps_out
+       << ") grid=" << pl.mps_fwd_grid << "\n";
   for (const auto &s : pl.fwd)
     os << "fwd layer=" << s.layer << " " << tile_str(s.tile) << " psi:" << load_name(s.psi_load)
        << "(" << s.psi_in << ")->" << store_name(s.psi_store) << "(" << s.psi_out << ")"
@@ -676,8 +670,9 @@ std::string describe(const Plan &pl) {
        << "(" << s.psi_out << ") lam:" << load_name(s.lam_load) << "(" << s.lam_in << ")->"
        << store_name(s.lam_store) << "(" << s.lam_out << ")" << (s.phase ? " phase" : "")
        << (s.phi_grad ? " phi" : "") << " grid=" << s.grid << "\n";
-  if (pl.grad01)
-    os << "grad01 lam:" << load_name(pl.grad01_load) << "(" << pl.grad01_lam << ") grid=" << pl.grad01_grid << "\n";
+  if (pl.mps_k > 0)
+    os << "mps K=" << pl.mps_k << " grad lam:" << load_name(pl.mps_load) << "(" << pl.mps_lam
+       << ") grid=" << pl.mps_grad_grid << "\n";
   if (pl.layer0_kernel)
     os << "layer0 lam:" << load_name(pl.layer0_load) << "(" << pl.layer0_lam << ") grid=" << pl.layer0_grid << "\n";
   os << "finalize\n";
@@ -758,8 +753,9 @@ struct rsv_backend {
   rsv::DevBuf<double2> ptab, prod;
   rsv::DevBuf<double> energy_partials, pass_partials, outputs;  // outputs: [1 + num_params]
   rsv::DevBuf<double> layer0_partials;                           // [layer0_grid][kLayer0Stride]
-  rsv::DevBuf<double> grad01_partials;                           // [grad01_grid][kGrad01Stride]
-  rsv::DevBuf<double2> mps_btab;                                 // [4][256][4] layer-0/1 byte tables
+  // matrix-product stage (rsv_mps.cu): site matrices, forward byte tables,
+  // coset tables, per-tile Z, coset sums, per-CTA G/F and their sums
+  rsv::DevBuf<double2> mps_tsite, mps_btab, mps_coslo, mps_coshi, mps_zt, mps_ylo, mps_yhi, mps_partials, mps_gf;
   rsv::DevBuf<int> tables;  // pass_grid | theta_pass | theta_slot | phi_pass
   rsv::DevBuf<int> order;   // undo order of the wires within a backward layer
   rsv::DevBuf<double2> rot;
@@ -916,17 +912,35 @@ double pass_bytes(const rsv_backend *B, const Step &s) {
   return k * amp;
 }
 
+MpsParams mps_params(rsv_backend *B) {
+  MpsParams Q{};
+  Q.n = B->n;
+  Q.bond = 1 << (B->plan.mps_k - 1);
+  const int m = B->n - 12;
+  Q.m1 = (m + 1) / 2;
+  Q.m2 = m - Q.m1;
+  Q.coef = B->coef.p;
+  Q.tsite = B->mps_tsite.p;
+  Q.btab = B->mps_btab.p;
+  Q.coslo = B->mps_coslo.p;
+  Q.coshi = B->mps_coshi.p;
+  Q.zt = B->mps_zt.p;
+  Q.ylo = B->mps_ylo.p;
+  Q.yhi = B->mps_yhi.p;
+  Q.partials = B->mps_partials.p;
+  Q.gf = B->mps_gf.p;
+  Q.num_tiles = u64{1} << (B->n - 12);
+  return Q;
+}
+
 void run_forward(rsv_backend *B, cudaStream_t st) {
-  if (B->plan.fwd01) {
-    Fwd01Params Q{};
-    Q.n = B->n;
-    Q.scatter = B->plan.fwd01_scatter ? 1 : 0;
-    Q.coef = B->coef.p;
-    Q.btab = B->mps_btab.p;
-    Q.out = state_buf(B, B->plan.fwd01_out);
-    Q.num_tiles = u64{1} << (B->n - 12);
-    timed(B, st, 1, 16.0 * static_cast<double>(u64{1} << B->n),
-          [&] { check(launch_fwd01(Q, B->plan.fwd01_grid, st), "layers 0-1 forward launch"); });
+  if (B->plan.mps_k > 0) {
+    const MpsParams Q = mps_params(B);
+    timed(B, st, 1, 16.0 * static_cast<double>(u64{1} << B->n), [&] {
+      check(launch_mps_tables(Q, st), "matrix-product tables launch");
+      check(launch_mps_forward(Q, state_buf(B, B->plan.mps_out), B->plan.mps_scatter ? 1 : 0, B->plan.mps_fwd_grid, st),
+            "matrix-product forward launch");
+    });
   }
   PassParams P;
   for (const auto &s : B->plan.fwd) {
@@ -956,17 +970,6 @@ Layer0Params layer0_params(rsv_backend *B) {
   return Q;
 }
 
-Grad01Params grad01_params(rsv_backend *B) {
-  Grad01Params Q{};
-  Q.n = B->n;
-  Q.gather = B->plan.grad01_load == kLoadGatherP ? 1 : 0;
-  Q.coef = B->coef.p;
-  Q.lam = state_buf(B, B->plan.grad01_lam);
-  Q.num_tiles = u64{1} << (B->n - 12);
-  Q.partials = B->grad01_partials.p;
-  return Q;
-}
-
 void run_backward(rsv_backend *B, cudaStream_t st) {
   PassParams P;
   for (const auto &s : B->plan.bwd) {
@@ -979,10 +982,13 @@ void run_backward(rsv_backend *B, cudaStream_t st) {
     timed(B, st, 3, 16.0 * static_cast<double>(u64{1} << B->n),
           [&] { check(launch_layer0_grad(Q, B->plan.layer0_grid, st), "layer-0 gradient launch"); });
   }
-  if (B->plan.grad01) {
-    const Grad01Params Q = grad01_params(B);
-    timed(B, st, 3, 16.0 * static_cast<double>(u64{1} << B->n),
-          [&] { check(launch_grad01(Q, B->plan.grad01_grid, st), "layers 0-1 gradient launch"); });
+  if (B->plan.mps_k > 0) {
+    const MpsParams Q = mps_params(B);
+    timed(B, st, 3, 16.0 * static_cast<double>(u64{1} << B->n), [&] {
+      check(launch_mps_grad(Q, state_buf(B, B->plan.mps_lam), B->plan.mps_load == kLoadGatherP ? 1 : 0,
+                            B->plan.mps_grad_grid, st),
+            "matrix-product gradient launch");
+    });
   }
 }
 
@@ -1005,11 +1011,9 @@ void run_finalize(rsv_backend *B, bool grad, double *energy_out, double *grad_ou
   F.energy_out = energy_out;
   F.grad_out = grad ? grad_out : nullptr;
   timed(B, st, 4, 0.0, [&] { check(launch_finalize(F, st), "finalize launch"); });
-  if (grad && B->plan.grad01) {
-    const Grad01Params Q = grad01_params(B);
-    timed(B, st, 4, 0.0, [&] {
-      check(launch_grad01_finalize(Q, B->plan.grad01_grid, grad_out, st), "layers 0-1 finalize launch");
-    });
+  if (grad && B->plan.mps_k > 0) {
+    const MpsParams Q = mps_params(B);
+    timed(B, st, 4, 0.0, [&] { check(launch_mps_finalize(Q, grad_out, st), "matrix-product finalize launch"); });
   }
   if (grad && B->plan.layer0_kernel) {
     const Layer0Params Q = layer0_params(B);
@@ -1437,8 +1441,19 @@ void setup_plan(rsv_backend *B, int mode) {
   B->num_bwd_passes = static_cast<int>(B->plan.bwd.size());
   B->prod.alloc(1024 * (1 + B->plan.partial_masks.size()));
   B->layer0_partials.alloc(static_cast<size_t>(B->plan.layer0_grid) * kLayer0Stride);
-  B->grad01_partials.alloc(static_cast<size_t>(B->plan.grad01_grid) * kGrad01Stride);
-  B->mps_btab.alloc(4 * 256 * 4);
+  if (B->plan.mps_k > 0) {
+    const size_t e = static_cast<size_t>(1) << (2 * (B->plan.mps_k - 1));  // bond^2
+    const int m = B->n - 12, m1 = (m + 1) / 2, m2 = m - m1;
+    B->mps_tsite.alloc(64 * e);
+    B->mps_btab.alloc(1024 * e);
+    B->mps_coslo.alloc((size_t{1} << m1) * e);
+    B->mps_coshi.alloc((size_t{1} << m2) * e);
+    B->mps_zt.alloc((size_t{1} << m) * e);
+    B->mps_ylo.alloc((size_t{1} << m1) * e);
+    B->mps_yhi.alloc((size_t{1} << m2) * e);
+    B->mps_partials.alloc(static_cast<size_t>(B->plan.mps_grad_grid) * 128 * e);
+    B->mps_gf.alloc(128 * e);
+  }
   B->pass_partials.alloc(static_cast<size_t>(std::max(1, B->num_bwd_passes)) * B->plan.max_grid *
                          kPartialStride);
   std::vector<int> tab;

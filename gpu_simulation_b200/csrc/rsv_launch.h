@@ -28,12 +28,13 @@ cudaError_t launch_finalize(const FinalizeParams &F, cudaStream_t s);
 // into grad_out[0 .. 2n)
 cudaError_t launch_layer0_grad(const Layer0Params &Q, int grid, cudaStream_t s);
 cudaError_t launch_layer0_finalize(const Layer0Params &Q, int grid, double *grad_out, cudaStream_t s);
-// layers 0 and 1 in one read of lambda (n >= 13, L >= 2), and their final
-// reduction into grad_out[0 .. 4n)
-cudaError_t launch_grad01(const Grad01Params &Q, int grid, cudaStream_t s);
-cudaError_t launch_grad01_finalize(const Grad01Params &Q, int grid, double *grad_out, cudaStream_t s);
-// forward of layers 0 and 1 in one write (n >= 13, L >= 2): the byte tables,
-// then chi1 into Q.out
-cudaError_t launch_fwd01(const Fwd01Params &Q, int grid, cudaStream_t s);
+// the first K layers as a matrix-product state (n >= 13, bond 2 or 4): the
+// site and table set-up, the forward write of their output, the gradient
+// read of lambda (tile sums, coset sums, CTA sums) and the final per-wire
+// environments into grad_out[0 .. 2nK)
+cudaError_t launch_mps_tables(const MpsParams &Q, cudaStream_t s);
+cudaError_t launch_mps_forward(const MpsParams &Q, double2 *out, int scatter, int grid, cudaStream_t s);
+cudaError_t launch_mps_grad(const MpsParams &Q, const double2 *lam, int gather, int grid, cudaStream_t s);
+cudaError_t launch_mps_finalize(const MpsParams &Q, double *grad_out, cudaStream_t s);
 
 }  // namespace rsv

@@ -1,0 +1,536 @@
+// The first K layers of the ansatz as a matrix-product state (sm_100a).
+//
+// The circuit starts from |0...0>.  With q the index after a layer's
+// rotations, that layer's CNOT ring turns q into prefix parities
+// s_w = q_0 ^ ... ^ q_w (bit 0 of P(q) is s_{n-1} ^ s_0).  If the state after
+// k - 1 layers is a periodic matrix-product state chi(q) = Tr prod_w A_w[q_w]
+// of bond dimension d, the state after layer k's rotations is one of bond
+// dimension 2d, with the new bond index (x, s) (x the old bond, s the prefix
+// parity):
+//   T_w[b]((x, s'), (y, s)) = U_w[b, s]      A_w[s ^ s'](x, y)    (w >= 1),
+//   T_0[b]((x, s'), (y, s)) = U_0[b, s' ^ s] A_0[s](x, y),
+// starting from the 1 x 1 tensors A_w[b] = (U_w |0>)_b of layer 0 (U = RZ RY of
+// the layer).  So the first K layers are chi_{K-1}(r) = Tr prod_w T_w[r_w] with
+// bond D = 2^(K-1).  K = 2 (D = 2) and K = 3 (D = 4) are used here.
+//
+// Forward (mps_fwd_kernel): one write of chi_{K-1} (scattered through P when
+// more layers follow) from byte tables of products of eight site matrices.
+// Backward: every parameter of the first K layers on wire w enters T_w only,
+// so with lambda the adjoint state at the output of layer K - 1
+//   dE/dx = 2 Re sum_b Tr( d_x T_w[b] E_w[b] ),
+//   E_w[b] = sum over r with r_w = b of conj(lambda(r)) R_w(r)
+// (R_w the cyclic product of the other site matrices after w).  One read of
+// lambda in 4096-amplitude tiles (a = bits 0..5, h = bits 6..11, t = coset
+// bits 12..n-1 split into lo (m1 bits) and hi):
+//   X1(a) = sum_h conj(lambda) M2(h),  X2(h) = sum_a conj(lambda) M1(a),
+//   G(a) += X1(a) C_t,  F(h) += C_t X2(h),  Z_t = sum_a M1(a) X1(a)
+// (M1 = T_0..T_5, M2 = T_6..T_11, C_t = CosLo(lo) CosHi(hi) the product of the
+// coset sites), then Y(lo) = sum_hi CosHi(hi) Z_t and Y'(hi) = sum_lo Z_t
+// CosLo(lo) (mps_coset_kernel), and per wire the leave-one-out products over
+// its group of bits (mps_finalize_kernel).
+// The reference walks these layers back gate by gate
+// (cpp/ising_cuda_statevector_grad_kernels.cu:223-319, scheduled by
+// cpp/ising_cuda_structured_adjoint_modes.inc:272-307) and computes layer 0
+// analytically in the forward (cpp/ising_cuda_rotation_kernels.cu:20-41); the
+// sums are the same.
+#include "rsv_launch.h"
+#include "rsv_tile.cuh"
+
+namespace rsv {
+namespace {
+
+template <int D>
+struct Mat {
+  double2 m[D * D];  // row-major
+};
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {  // a * b + c
+  return make_double2(fma(a.x, b.x, fma(-a.y, b.y, c.x)), fma(a.x, b.y, fma(a.y, b.x, c.y)));
+}
+// conj(x) * w + c
+__device__ __forceinline__ double2 cjfma(double2 x, double2 w, double2 c) {
+  return make_double2(fma(x.x, w.x, fma(x.y, w.y, c.x)), fma(x.x, w.y, fma(-x.y, w.x, c.y)));
+}
+template <int D>
+__device__ __forceinline__ Mat<D> mmul(const Mat<D> &A, const Mat<D> &B) {
+  Mat<D> R;
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      double2 s = cmul(A.m[i * D], B.m[j]);
+#pragma unroll
+      for (int k = 1; k < D; ++k) s = cfma(A.m[i * D + k], B.m[k * D + j], s);
+      R.m[i * D + j] = s;
+    }
+  return R;
+}
+template <int D>
+__device__ __forceinline__ Mat<D> ident() {
+  Mat<D> R;
+#pragma unroll
+  for (int e = 0; e < D * D; ++e) R.m[e] = make_double2((e % (D + 1)) == 0 ? 1.0 : 0.0, 0.0);
+  return R;
+}
+template <int D>
+__device__ __forceinline__ Mat<D> load_mat(const double2 *p) {
+  Mat<D> R;
+#pragma unroll
+  for (int e = 0; e < D * D; ++e) R.m[e] = p[e];
+  return R;
+}
+template <int D>
+__device__ __forceinline__ void store_mat(double2 *p, const Mat<D> &A) {
+#pragma unroll
+  for (int e = 0; e < D * D; ++e) p[e] = A.m[e];
+}
+template <int D>
+__device__ __forceinline__ Mat<D> ldg_mat(const double2 *__restrict__ p) {
+  Mat<D> R;
+#pragma unroll
+  for (int e = 0; e < D * D; ++e) R.m[e] = __ldg(&p[e]);
+  return R;
+}
+
+// Layer-k gate of wire w, U = RZ(phi) RY(theta) = [[c e-, -s e-], [s e+, c e+]]
+// (e-+ = e^{-+ i phi/2}), or its theta- (kind 1) or phi-derivative (kind 2).
+__device__ __forceinline__ void layer_gate(const double4 *coef, int n, int k, int w, int kind, double2 (&u)[2][2]) {
+  const double4 q = coef[k * n + w];
+  const double2 em = make_double2(q.z, -q.w), ep = make_double2(q.z, q.w);
+  double c = q.x, s = q.y;
+  if (kind == 1) {  // d RY / d theta = [[-s/2, -c/2], [c/2, -s/2]]: the (c, s) pattern with c -> -s/2, s -> c/2
+    c = -0.5 * q.y;
+    s = 0.5 * q.x;
+  }
+  u[0][0] = make_double2(c * em.x, c * em.y);
+  u[0][1] = make_double2(-s * em.x, -s * em.y);
+  u[1][0] = make_double2(s * ep.x, s * ep.y);
+  u[1][1] = make_double2(c * ep.x, c * ep.y);
+  if (kind == 2) {  // d RZ / d phi: row 0 times -i/2, row 1 times +i/2
+#pragma unroll
+    for (int y = 0; y < 2; ++y) {
+      u[0][y] = make_double2(0.5 * u[0][y].y, -0.5 * u[0][y].x);
+      u[1][y] = make_double2(-0.5 * u[1][y].y, 0.5 * u[1][y].x);
+    }
+  }
+}
+
+// Site matrices T_w[0], T_w[1] of the first K = log2(D) + 1 layers, with the
+// gate of layer dlayer replaced by its derivative dkind (0: none).
+template <int D>
+__device__ void site_tensor(const double4 *coef, int n, int w, int dlayer, int dkind, Mat<D> (&T)[2]) {
+  double2 cur[2][D * D], nxt[2][D * D];
+  double2 u[2][2];
+  layer_gate(coef, n, 0, w, dlayer == 0 ? dkind : 0, u);
+  cur[0][0] = u[0][0];  // (U |0>)_b
+  cur[1][0] = u[1][0];
+  int d = 1;
+  for (int k = 1; 2 * d <= D; ++k) {
+    layer_gate(coef, n, k, w, dlayer == k ? dkind : 0, u);
+    const int d2 = 2 * d;
+    for (int b = 0; b < 2; ++b)
+      for (int sp = 0; sp < 2; ++sp)
+        for (int s = 0; s < 2; ++s)
+          for (int x = 0; x < d; ++x)
+            for (int y = 0; y < d; ++y)
+              nxt[b][(2 * x + sp) * d2 + (2 * y + s)] =
+                  w >= 1 ? cmul(u[b][s], cur[s ^ sp][x * d + y]) : cmul(u[b][sp ^ s], cur[s][x * d + y]);
+    for (int b = 0; b < 2; ++b)
+      for (int e = 0; e < d2 * d2; ++e) cur[b][e] = nxt[b][e];
+    d = d2;
+  }
+  for (int b = 0; b < 2; ++b)
+    for (int e = 0; e < D * D; ++e) T[b].m[e] = cur[b][e];
+}
+
+// ---------------------------------------------------------------- tables
+// tsite[w][b] for w < 32 (identity for w >= n)
+template <int D>
+__global__ void mps_site_kernel(const MpsParams Q) {
+  const int t = threadIdx.x;
+  if (t >= 32) return;
+  Mat<D> T[2];
+  if (t < Q.n) {
+    site_tensor<D>(Q.coef, Q.n, t, -1, 0, T);
+  } else {
+    T[0] = T[1] = ident<D>();
+  }
+  store_mat<D>(Q.tsite + (2 * t) * D * D, T[0]);
+  store_mat<D>(Q.tsite + (2 * t + 1) * D * D, T[1]);
+}
+
+// product of the site matrices of wires w0 .. w0 + nb - 1 for the bits of v
+template <int D>
+__device__ __forceinline__ Mat<D> site_chain(const double2 *tsite, int w0, int nb, unsigned v) {
+  Mat<D> p = ident<D>();
+  for (int j = 0; j < nb; ++j) p = mmul<D>(p, load_mat<D>(tsite + (2 * (w0 + j) + ((v >> j) & 1)) * D * D));
+  return p;
+}
+
+// byte tables (4 x 256) for the forward, coset tables CosLo (2^m1) and CosHi
+// (2^m2) for the backward
+template <int D>
+__global__ void mps_tables_kernel(const MpsParams Q) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nlo = 1 << Q.m1, nhi = 1 << Q.m2;
+  if (e < 1024) {
+    const int k = e >> 8, v = e & 255;
+    store_mat<D>(Q.btab + e * D * D, site_chain<D>(Q.tsite, 8 * k, 8, static_cast<unsigned>(v)));
+  } else if (e < 1024 + nlo) {
+    const int lo = e - 1024;
+    store_mat<D>(Q.coslo + lo * D * D, site_chain<D>(Q.tsite, 12, Q.m1, static_cast<unsigned>(lo)));
+  } else if (e < 1024 + nlo + nhi) {
+    const int hi = e - 1024 - nlo;
+    store_mat<D>(Q.coshi + hi * D * D, site_chain<D>(Q.tsite, 12 + Q.m1, Q.m2, static_cast<unsigned>(hi)));
+  }
+}
+
+// --------------------------------------------------------------- forward
+// chi(r) = Tr(B0[r0] B1[r1] B2[r2] B3[r3]) for 4096 contiguous r per tile;
+// thread t takes r = base + t + 256 k: byte 0 is t, so chi = Tr(B1[r1] W)
+// with W = B2 B3 B0[t] fixed per tile.
+template <int D, bool SCATTER>
+__global__ void __launch_bounds__(256) mps_fwd_kernel(const MpsParams Q, double2 *__restrict__ out) {
+  const int t = threadIdx.x, n = Q.n;
+  const Mat<D> b0 = ldg_mat<D>(Q.btab + t * D * D);
+  for (u64 tile = blockIdx.x; tile < Q.num_tiles; tile += gridDim.x) {
+    const u64 base = tile << 12;
+    const Mat<D> W = mmul<D>(mmul<D>(ldg_mat<D>(Q.btab + (512 + ((base >> 16) & 255)) * D * D),
+                                     ldg_mat<D>(Q.btab + (768 + ((base >> 24) & 255)) * D * D)),
+                             b0);
+    const int hi1 = static_cast<int>((base >> 8) & 0xF0);
+#pragma unroll 2
+    for (int k = 0; k < 16; ++k) {
+      const double2 *b1 = Q.btab + (256 + (hi1 | k)) * D * D;
+      double2 v = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j) v = cfma(__ldg(&b1[i * D + j]), W.m[j * D + i], v);
+      const u64 r = base | static_cast<u64>(t + 256 * k);
+      __stcs(&out[SCATTER ? ring_p(r, n) : r], v);
+    }
+  }
+}
+
+// -------------------------------------------------------------- backward
+constexpr int kMpsThreads = 256;
+__device__ __forceinline__ int mps_slot(int i) { return i ^ ((i >> 6) & 7); }
+
+template <int D>
+constexpr size_t mps_grad_smem() {
+  // stage, M1, M2, X1, X2, C, Z partials (two buffers of 8 warps)
+  return (4096 + 4 * 64 * D * D + D * D + 2 * 8 * D * D) * sizeof(double2);
+}
+
+template <int D>
+__global__ void __launch_bounds__(kMpsThreads) mps_grad_kernel(const MpsParams Q, const double2 *__restrict__ lam,
+                                                                int gather) {
+  constexpr int E = D * D;
+  constexpr int EPT = E / 4;  // X / G / F entries per thread
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2 *stage = reinterpret_cast<double2 *>(smem_raw);
+  double2 *m1 = stage + 4096;  // [64][E]
+  double2 *m2 = m1 + 64 * E;
+  double2 *x1 = m2 + 64 * E;
+  double2 *x2 = x1 + 64 * E;
+  double2 *csm = x2 + 64 * E;  // [E]
+  double2 *zp = csm + E;       // [2][8][E]
+
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int n = Q.n;
+  if (t < 128) {
+    const int half = t >> 6, x = t & 63;
+    store_mat<D>((half ? m2 : m1) + x * E, site_chain<D>(Q.tsite, 6 * half, 6, static_cast<unsigned>(x)));
+  }
+  __syncthreads();
+
+  const int idx = t >> 2, q = t & 3;
+  double2 g[EPT], f[EPT];
+#pragma unroll
+  for (int j = 0; j < EPT; ++j) g[j] = f[j] = make_double2(0.0, 0.0);
+  // Z partial of this thread: entry ze, a-range zp0 .. zp0 + 64 / (256 / E) - 1
+  constexpr int kZParts = kMpsThreads / E, kZA = 64 / kZParts;
+  const int ze = t % E, zpart = t / E;
+  const int zi = ze / D, zj = ze % D;
+
+  const u64 num_tiles = Q.num_tiles;
+  const unsigned lomask = (1u << Q.m1) - 1u;
+  auto issue = [&](u64 tile) {
+    if (tile < num_tiles) {
+      const u64 base = tile << 12;
+#pragma unroll
+      for (int r = 0; r < 4096 / kMpsThreads; ++r) {
+        const int tau = t + r * kMpsThreads;
+        const u64 p = base | static_cast<u64>(tau);
+        cp_async16(&stage[mps_slot(tau)], &lam[gather ? ring_p(p, n) : p]);
+      }
+    }
+    cp_async_commit();
+  };
+  issue(blockIdx.x);
+
+  int k = 0;
+  u64 prev = 0;
+  for (u64 tile = blockIdx.x; tile < num_tiles; tile += gridDim.x, ++k) {
+    cp_async_wait_all();
+    __syncthreads();
+    // the previous tile's Z, from the per-warp partials
+    if (k > 0 && t < E) {
+      const double2 *zb = zp + ((k - 1) & 1) * 8 * E;
+      double2 s = zb[t];
+      for (int w = 1; w < 8; ++w) s = cadd(s, zb[w * E + t]);
+      Q.zt[prev * E + t] = s;
+    }
+    if (t < E) {
+      // C_t = CosLo(lo) CosHi(hi), entry t
+      const unsigned lo = static_cast<unsigned>(tile) & lomask, hi = static_cast<unsigned>(tile >> Q.m1);
+      const double2 *cl = Q.coslo + lo * E, *ch = Q.coshi + hi * E;
+      const int i = t / D, j = t % D;
+      double2 s = cmul(__ldg(&cl[i * D]), __ldg(&ch[j]));
+#pragma unroll
+      for (int kk = 1; kk < D; ++kk) s = cfma(__ldg(&cl[i * D + kk]), __ldg(&ch[kk * D + j]), s);
+      csm[t] = s;
+    }
+    {
+      double2 a1[EPT], a2[EPT];
+#pragma unroll
+      for (int j = 0; j < EPT; ++j) a1[j] = a2[j] = make_double2(0.0, 0.0);
+#pragma unroll 4
+      for (int kk = 0; kk < 64; ++kk) {
+        const double2 c1 = stage[mps_slot(idx + 64 * kk)];  // a = idx, h = kk
+        const double2 c2 = stage[mps_slot(kk + 64 * idx)];  // a = kk, h = idx
+#pragma unroll
+        for (int j = 0; j < EPT; ++j) {
+          a1[j] = cjfma(c1, m2[kk * E + q + 4 * j], a1[j]);
+          a2[j] = cjfma(c2, m1[kk * E + q + 4 * j], a2[j]);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < EPT; ++j) {
+        x1[idx * E + q + 4 * j] = a1[j];
+        x2[idx * E + q + 4 * j] = a2[j];
+      }
+    }
+    __syncthreads();
+    issue(tile + gridDim.x);  // the stage is free
+    // G(a) += X1(a) C, F(h) += C X2(h)
+#pragma unroll
+    for (int j = 0; j < EPT; ++j) {
+      const int e = q + 4 * j, i = e / D, jj = e % D;
+      double2 sg = g[j], sf = f[j];
+#pragma unroll
+      for (int kk = 0; kk < D; ++kk) {
+        sg = cfma(x1[idx * E + i * D + kk], csm[kk * D + jj], sg);
+        sf = cfma(csm[i * D + kk], x2[idx * E + kk * D + jj], sf);
+      }
+      g[j] = sg;
+      f[j] = sf;
+    }
+    // Z partial: sum over this thread's a-range of (M1(a) X1(a))[zi][zj]
+    {
+      double2 z = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int aa = 0; aa < kZA; ++aa) {
+        const int a = zpart * kZA + aa;
+#pragma unroll
+        for (int kk = 0; kk < D; ++kk) z = cfma(m1[a * E + zi * D + kk], x1[a * E + kk * D + zj], z);
+      }
+      // threads with the same entry in a warp differ in lane bits >= log2(E)
+#pragma unroll
+      for (int m = E; m < 32; m <<= 1)
+        z = cadd(z, make_double2(__shfl_xor_sync(0xffffffffu, z.x, m), __shfl_xor_sync(0xffffffffu, z.y, m)));
+      if (lane < E) zp[(k & 1) * 8 * E + warp * E + lane] = z;
+    }
+    prev = tile;
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  if (k > 0 && t < E) {
+    const double2 *zb = zp + ((k - 1) & 1) * 8 * E;
+    double2 s = zb[t];
+    for (int w = 1; w < 8; ++w) s = cadd(s, zb[w * E + t]);
+    Q.zt[prev * E + t] = s;
+  }
+  double2 *rec = Q.partials + static_cast<size_t>(blockIdx.x) * 2 * 64 * E;
+#pragma unroll
+  for (int j = 0; j < EPT; ++j) {
+    rec[idx * E + q + 4 * j] = g[j];
+    rec[64 * E + idx * E + q + 4 * j] = f[j];
+  }
+}
+
+// Y(lo) = sum_hi CosHi(hi) Z(lo, hi)   (blocks 0 .. 2^m1 - 1)
+// Y'(hi) = sum_lo Z(lo, hi) CosLo(lo)  (blocks 2^m1 .. 2^m1 + 2^m2 - 1)
+template <int D>
+__global__ void __launch_bounds__(64) mps_coset_kernel(const MpsParams Q) {
+  constexpr int E = D * D;
+  __shared__ double2 red[64][E];
+  const int t = threadIdx.x;
+  const int nlo = 1 << Q.m1, nhi = 1 << Q.m2;
+  const int b = blockIdx.x;
+  Mat<D> acc;
+#pragma unroll
+  for (int e = 0; e < E; ++e) acc.m[e] = make_double2(0.0, 0.0);
+  if (b < nlo) {
+    for (int hi = t; hi < nhi; hi += 64) {
+      const Mat<D> p = mmul<D>(ldg_mat<D>(Q.coshi + hi * E), ldg_mat<D>(Q.zt + (static_cast<u64>(b) + (static_cast<u64>(hi) << Q.m1)) * E));
+#pragma unroll
+      for (int e = 0; e < E; ++e) acc.m[e] = cadd(acc.m[e], p.m[e]);
+    }
+  } else {
+    const int hi = b - nlo;
+    for (int lo = t; lo < nlo; lo += 64) {
+      const Mat<D> p = mmul<D>(ldg_mat<D>(Q.zt + (static_cast<u64>(lo) + (static_cast<u64>(hi) << Q.m1)) * E), ldg_mat<D>(Q.coslo + lo * E));
+#pragma unroll
+      for (int e = 0; e < E; ++e) acc.m[e] = cadd(acc.m[e], p.m[e]);
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < E; ++e) red[t][e] = acc.m[e];
+  __syncthreads();
+  for (int s = 32; s > 0; s >>= 1) {
+    if (t < s)
+#pragma unroll
+      for (int e = 0; e < E; ++e) red[t][e] = cadd(red[t][e], red[t + s][e]);
+    __syncthreads();
+  }
+  if (t < E) (b < nlo ? Q.ylo + b * E : Q.yhi + (b - nlo) * E)[t] = red[0][t];
+}
+
+// G and F summed over the gradient kernel's CTAs, in CTA order
+template <int D>
+__global__ void mps_reduce_kernel(const MpsParams Q, int grid) {
+  constexpr int E = D * D;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 2 * 64 * E) return;
+  double2 s = make_double2(0.0, 0.0);
+  for (int c = 0; c < grid; ++c) s = cadd(s, Q.partials[static_cast<size_t>(c) * 2 * 64 * E + i]);
+  Q.gf[i] = s;
+}
+
+// Block w: E_w[0], E_w[1] from the leave-one-out products over wire w's group
+// of bits, then the 2K gradients of wire w (layers 0 .. K-1).
+template <int D>
+__global__ void __launch_bounds__(64) mps_finalize_kernel(const MpsParams Q, double *__restrict__ grad_out) {
+  constexpr int E = D * D;
+  constexpr int K = D == 2 ? 2 : 3;
+  __shared__ double2 red[64][2 * E];
+  __shared__ double2 env[2 * E];
+  const int t = threadIdx.x, w = blockIdx.x, n = Q.n;
+  // group of wire w: its first wire, bit count, values and their source
+  int g0, nb, count;
+  const double2 *src;
+  if (w < 6) {
+    g0 = 0; nb = 6; count = 64; src = Q.gf;
+  } else if (w < 12) {
+    g0 = 6; nb = 6; count = 64; src = Q.gf + 64 * E;
+  } else if (w < 12 + Q.m1) {
+    g0 = 12; nb = Q.m1; count = 1 << Q.m1; src = Q.ylo;
+  } else {
+    g0 = 12 + Q.m1; nb = Q.m2; count = 1 << Q.m2; src = Q.yhi;
+  }
+  const int bit = w - g0;
+  Mat<D> acc[2];
+#pragma unroll
+  for (int b = 0; b < 2; ++b)
+#pragma unroll
+    for (int e = 0; e < E; ++e) acc[b].m[e] = make_double2(0.0, 0.0);
+  for (int x = t; x < count; x += 64) {
+    const unsigned v = static_cast<unsigned>(x);
+    // post = sites w+1 .. g0+nb-1, pre = sites g0 .. w-1, with the bits of x
+    const Mat<D> post = site_chain<D>(Q.tsite, w + 1, g0 + nb - (w + 1), v >> (bit + 1));
+    const Mat<D> pre = site_chain<D>(Q.tsite, g0, bit, v);
+    const Mat<D> term = mmul<D>(mmul<D>(post, load_mat<D>(src + x * E)), pre);
+    const int b = (x >> bit) & 1;
+#pragma unroll
+    for (int e = 0; e < E; ++e) acc[b].m[e] = cadd(acc[b].m[e], term.m[e]);
+  }
+#pragma unroll
+  for (int b = 0; b < 2; ++b)
+#pragma unroll
+    for (int e = 0; e < E; ++e) red[t][b * E + e] = acc[b].m[e];
+  __syncthreads();
+  for (int s = 32; s > 0; s >>= 1) {
+    if (t < s)
+      for (int e = 0; e < 2 * E; ++e) red[t][e] = cadd(red[t][e], red[t + s][e]);
+    __syncthreads();
+  }
+  if (t < 2 * E) env[t] = red[0][t];
+  __syncthreads();
+  if (t < 2 * K) {
+    const int layer = t >> 1, kind = 1 + (t & 1);
+    Mat<D> dT[2];
+    site_tensor<D>(Q.coef, n, w, layer, kind, dT);
+    double s = 0.0;
+    for (int b = 0; b < 2; ++b)
+      for (int i = 0; i < D; ++i)
+        for (int j = 0; j < D; ++j) s += cmul(dT[b].m[i * D + j], env[b * E + j * D + i]).x;
+    grad_out[2 * (layer * n + w) + (t & 1)] = 2.0 * s;
+  }
+}
+
+template <int D>
+cudaError_t launch_grad_d(const MpsParams &Q, const double2 *lam, int gather, int grid, cudaStream_t s) {
+  static bool configured = false;
+  if (!configured) {
+    const cudaError_t e = cudaFuncSetAttribute(mps_grad_kernel<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               static_cast<int>(mps_grad_smem<D>()));
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  mps_grad_kernel<D><<<grid, kMpsThreads, mps_grad_smem<D>(), s>>>(Q, lam, gather);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  mps_coset_kernel<D><<<(1 << Q.m1) + (1 << Q.m2), 64, 0, s>>>(Q);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  mps_reduce_kernel<D><<<(2 * 64 * D * D + 255) / 256, 256, 0, s>>>(Q, grid);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t mps_partials_count(int bond) { return static_cast<size_t>(2) * 64 * bond * bond; }
+
+cudaError_t launch_mps_tables(const MpsParams &Q, cudaStream_t s) {
+  if (Q.n < 13 || Q.n > 31 || (Q.bond != 2 && Q.bond != 4)) return cudaErrorInvalidValue;
+  const int count = 1024 + (1 << Q.m1) + (1 << Q.m2);
+  if (Q.bond == 2) {
+    mps_site_kernel<2><<<1, 32, 0, s>>>(Q);
+    mps_tables_kernel<2><<<(count + 127) / 128, 128, 0, s>>>(Q);
+  } else {
+    mps_site_kernel<4><<<1, 32, 0, s>>>(Q);
+    mps_tables_kernel<4><<<(count + 127) / 128, 128, 0, s>>>(Q);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mps_forward(const MpsParams &Q, double2 *out, int scatter, int grid, cudaStream_t s) {
+  if (Q.bond == 2) {
+    if (scatter) mps_fwd_kernel<2, true><<<grid, 256, 0, s>>>(Q, out);
+    else mps_fwd_kernel<2, false><<<grid, 256, 0, s>>>(Q, out);
+  } else if (Q.bond == 4) {
+    if (scatter) mps_fwd_kernel<4, true><<<grid, 256, 0, s>>>(Q, out);
+    else mps_fwd_kernel<4, false><<<grid, 256, 0, s>>>(Q, out);
+  } else {
+    return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mps_grad(const MpsParams &Q, const double2 *lam, int gather, int grid, cudaStream_t s) {
+  if (Q.bond == 2) return launch_grad_d<2>(Q, lam, gather, grid, s);
+  if (Q.bond == 4) return launch_grad_d<4>(Q, lam, gather, grid, s);
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_mps_finalize(const MpsParams &Q, double *grad_out, cudaStream_t s) {
+  if (Q.bond == 2) mps_finalize_kernel<2><<<Q.n, 64, 0, s>>>(Q, grad_out);
+  else if (Q.bond == 4) mps_finalize_kernel<4><<<Q.n, 64, 0, s>>>(Q, grad_out);
+  else return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+}  // namespace rsv

@@ -89,27 +89,19 @@ struct Layer0Params {
   double *partials;            // [grid][kLayer0Stride]
 };
 
-// Layers 0 and 1 from one read of lambda (rsv_mps01.cu): per-CTA records of
-// G(a), F(h) (64 2x2 complex matrices each) and the coset environments
-// E_v[b] (32 x 2 matrices).
-constexpr int kGrad01Stride = 1536;
-struct Grad01Params {
-  int n;
-  int gather;                  // lambda1(r) = lam[P(r)] (1) or lam[r] (0)
-  const double4 *coef;         // layer 0 at [0, n), layer 1 at [n, 2n)
-  const double2 *lam;
-  unsigned long long num_tiles;  // 2^(n-12)
-  double *partials;            // [grid][kGrad01Stride]
-};
-
-// Forward of layers 0 and 1 as one write of their matrix-product state
-// (rsv_mps01.cu).
-struct Fwd01Params {
-  int n;
-  int scatter;                 // store chi1(r) at P(r) (1) or at r (0)
-  const double4 *coef;         // layer 0 at [0, n), layer 1 at [n, 2n)
-  double2 *btab;               // [4][256][4] byte tables, rebuilt per call
-  double2 *out;
+// The first K layers as a matrix-product state of bond D = 2^(K-1)
+// (rsv_mps.cu).  Matrices are D x D complex, row-major.  The coset index t of
+// a 4096-amplitude tile (bits 12..n-1) splits into lo = its low m1 bits and hi.
+struct MpsParams {
+  int n, bond, m1, m2;
+  const double4 *coef;         // layers 0 .. K-1 at [k n, (k+1) n)
+  double2 *tsite;              // [32][2] site matrices T_w[b] (identity for w >= n)
+  double2 *btab;               // [4][256] products over the eight wires of a byte
+  double2 *coslo, *coshi;      // [2^m1], [2^m2] products over the coset wires
+  double2 *zt;                 // [2^(n-12)] per-tile Z
+  double2 *ylo, *yhi;          // [2^m1], [2^m2] coset sums
+  double2 *partials;           // [grid][2][64] per-CTA G, F
+  double2 *gf;                 // [2][64] G, F summed over the CTAs
   unsigned long long num_tiles;  // 2^(n-12)
 };
 

@@ -50,19 +50,17 @@ def parse_plan(text: str) -> dict:
     steps = []
     energy = None
     layer0 = None
-    grad01 = None
+    mps = None
     for ln in lines[1:]:
-        if ln.startswith("fwd01"):
-            m0 = re.match(r"fwd01 psi:(\w+)\((-?\d+)\) grid=(\d+)", ln)
+        if ln.startswith("mps "):
+            m0 = re.match(r"mps K=(\d+) fwd psi:(\w+)\((-?\d+)\) grid=(\d+)", ln)
+            if m0:
+                steps.append(dict(kind="mps_fwd", K=int(m0[1]), store=m0[2], out=int(m0[3]), grid=int(m0[4])))
+                continue
+            m0 = re.match(r"mps K=(\d+) grad lam:(\w+)\((-?\d+)\) grid=(\d+)", ln)
             if not m0:
                 raise ValueError(f"cannot parse plan line: {ln}")
-            steps.append(dict(kind="fwd01", store=m0[1], out=int(m0[2]), grid=int(m0[3])))
-            continue
-        if ln.startswith("grad01"):
-            m0 = re.match(r"grad01 lam:(\w+)\((-?\d+)\) grid=(\d+)", ln)
-            if not m0:
-                raise ValueError(f"cannot parse plan line: {ln}")
-            grad01 = dict(load=m0[1], buf=int(m0[2]), grid=int(m0[3]))
+            mps = dict(K=int(m0[1]), load=m0[2], buf=int(m0[3]), grid=int(m0[4]))
             continue
         if ln.startswith("layer0"):
             m0 = re.match(r"layer0 lam:(\w+)\((-?\d+)\) grid=(\d+)", ln)
@@ -95,7 +93,7 @@ def parse_plan(text: str) -> dict:
         ))
     return dict(n=int(head["n"]), L=int(head["L"]), phys=int(head["phys"]), steps=steps,
                 energy=energy, bufs=int(head["bufs"]), mode=head["mode"], layer0=layer0,
-                grad01=grad01)
+                mps=mps)
 
 
 def ring_p(i: np.ndarray, n: int) -> np.ndarray:
@@ -241,27 +239,28 @@ def simulate(n: int, layers: int, field: float, params: np.ndarray, check_indice
             rz = rz @ np.diag([-0.5j, 0.5j])
         return rz @ ry
 
-    def chi1(u0, u1):
+    def chi_k(gates):
+        # gates[k][w]: the 2x2 gate of layer k on wire w; output of the last
+        # given layer before its CNOT ring
         amp0 = np.ones(size, dtype=np.complex128)
         for w in range(phys):
             b = bits[:, w]
             if w < n:
-                amp0 *= np.where(b == 1, u0[w][1, 0], u0[w][0, 0])
+                amp0 *= np.where(b == 1, gates[0][w][1, 0], gates[0][w][0, 0])
             else:
                 amp0 *= np.where(b == 1, 0.0, 1.0)
-        out = np.zeros(size, dtype=np.complex128)
-        out[ring_p(idx, n)] = amp0
-        for w in range(n):
-            m = 1 << w
-            lo = idx[(idx & m) == 0]
-            x0, x1 = out[lo].copy(), out[lo | m].copy()
-            u = u1[w]
-            out[lo], out[lo | m] = u[0, 0] * x0 + u[0, 1] * x1, u[1, 0] * x0 + u[1, 1] * x1
+        out = amp0
+        for k in range(1, len(gates)):
+            nxt = np.zeros(size, dtype=np.complex128)
+            nxt[ring_p(idx, n)] = out
+            out = nxt
+            for w in range(n):
+                m = 1 << w
+                lo = idx[(idx & m) == 0]
+                x0, x1 = out[lo].copy(), out[lo | m].copy()
+                u = gates[k][w]
+                out[lo], out[lo | m] = u[0, 0] * x0 + u[0, 1] * x1, u[1, 0] * x0 + u[1, 1] * x1
         return out
-
-    def mps_chi1():
-        return chi1([ry_rz(p[0, w, 0], p[0, w, 1]) for w in range(n)],
-                    [ry_rz(p[1, w, 0], p[1, w, 1]) for w in range(n)])
 
     def energy_step():
         chi_b, mu_b = plan["energy"]
@@ -281,9 +280,10 @@ def simulate(n: int, layers: int, field: float, params: np.ndarray, check_indice
         return float(np.sum((np.conj(chi) * mu).real))
 
     for st in plan["steps"]:
-        if st.get("kind") == "fwd01":
-            # layers 0 and 1: chi1 = (U1 on every wire) P (U0 on every wire)|0>
-            store(st["store"], st["out"], mps_chi1())
+        if st.get("kind") == "mps_fwd":
+            # the first K layers, before the last one's ring, by direct simulation
+            store(st["store"], st["out"], chi_k([[ry_rz(p[k, w, 0], p[k, w, 1]) for w in range(n)]
+                                                 for k in range(st["K"])]))
             continue
         if check_indices:
             ids = tile_indices(st)
@@ -346,20 +346,18 @@ def simulate(n: int, layers: int, field: float, params: np.ndarray, check_indice
             dp0, dp1 = -0.5j * a0[w], 0.5j * a1[w]
             theta[0, w] = 2.0 * (dt0 * S0 + dt1 * S1).real
             phi[0, w] = 2.0 * (dp0 * S0 + dp1 * S1).real
-    if plan["grad01"] is not None:
-        # layers 0 and 1 from lambda at layer 1's output: 2 Re <lambda1 | d chi1>,
-        # chi1 = (U1 on every wire) P (U0 on every wire)|0>, by direct simulation
-        g0 = plan["grad01"]
-        lam1 = load(g0["load"], g0["buf"])
-
-        base0 = [ry_rz(p[0, w, 0], p[0, w, 1]) for w in range(n)]
-        base1 = [ry_rz(p[1, w, 0], p[1, w, 1]) for w in range(n)]
-        for w in range(n):
-            for layer, (dth, dph) in ((0, (True, False)), (0, (False, True)), (1, (True, False)), (1, (False, True))):
-                u0, u1 = list(base0), list(base1)
-                d = ry_rz(p[layer, w, 0], p[layer, w, 1], dth, dph)
-                (u0 if layer == 0 else u1)[w] = d
-                val = 2.0 * np.sum(np.conj(lam1) * chi1(u0, u1)).real
-                (theta if dth else phi)[layer, w] = val
+    if plan["mps"] is not None:
+        # the first K layers from lambda at their output: 2 Re <lambda | d chi_K>
+        mp = plan["mps"]
+        K = mp["K"]
+        lamk = load(mp["load"], mp["buf"])
+        base = [[ry_rz(p[k, w, 0], p[k, w, 1]) for w in range(n)] for k in range(K)]
+        for k in range(K):
+            for w in range(n):
+                for dth, dph in ((True, False), (False, True)):
+                    g = [list(row) for row in base]
+                    g[k][w] = ry_rz(p[k, w, 0], p[k, w, 1], dth, dph)
+                    val = 2.0 * np.sum(np.conj(lamk) * chi_k(g)).real
+                    (theta if dth else phi)[k, w] = val
     grad = np.stack([theta, phi], axis=-1).reshape(-1)
     return energy, grad

@@ -84,7 +84,7 @@ def test_large_plans_cover_every_wire_once(n, L):
 def check_large_plan(plan, n, L):
     seen = {}
     for st in plan["steps"]:
-        if st.get("kind") == "fwd01":
+        if st.get("kind") == "mps_fwd":
             assert 0 <= st["out"] < plan["bufs"]
             continue
         for b in ("psi_in", "psi_out", "lam_in", "lam_out"):
@@ -96,11 +96,12 @@ def check_large_plan(plan, n, L):
                 key = (st["layer"], w)
                 assert key not in seen
                 seen[key] = st["pass_index"]
-    if plan["grad01"] is not None:
-        # layers 0 and 1 are one read of lambda on the grad01 kernel
-        assert all(layer > 1 for layer, _ in seen)
-        assert 0 <= plan["grad01"]["buf"] < plan["bufs"]
-        for layer in (0, 1):
+    if plan["mps"] is not None:
+        # the first K layers are one read of lambda on the matrix-product kernels
+        K = plan["mps"]["K"]
+        assert all(layer >= K for layer, _ in seen)
+        assert 0 <= plan["mps"]["buf"] < plan["bufs"]
+        for layer in range(K):
             for w in range(n):
                 seen[(layer, w)] = -1
     if plan["layer0"] is not None:
