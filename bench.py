@@ -529,6 +529,19 @@ def main():
             except Exception as exc:  # report, do not hide
                 sweep[f"n={ns}"] = {"error": str(exc)}
         line["sweep"] = sweep
+    if world == 1 and rank == 0 and not args.no_sweep:
+        # the same call with fewer analytic leading layers (matrix-product
+        # shortcut off): 0 = every layer on tile passes, as the reference's
+        # schedule; the headline uses the engine's default of 3
+        info = eng.analytic_layers()
+        alt = {"default_max_layers": info["max_layers"], "used": info["used"]}
+        for k in (0, 1, 2):
+            eng.set_analytic_layers(k)
+            ms_k, _, e_k = device_time(eng, n, L, h, max(3, args.steps // 2), 2, seed=7 + rank)
+            alt[f"max_layers={k}"] = {"ms_per_call": ms_k, "energy_and_grad_per_s": 1000.0 / ms_k,
+                                      "energy": e_k}
+        eng.set_analytic_layers(info["max_layers"])
+        line["analytic_layers"] = alt
     if world == 1 and rank == 0 and not args.no_cpu:
         t, scale, threads, n_s = cpu_sample(n, L, h)
         line["cpu_baseline"] = {

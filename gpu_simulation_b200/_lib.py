@@ -48,6 +48,9 @@ _SIGNATURES = {
     "rsv_zgemm_batched": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                            ctypes.c_void_p], ctypes.c_int),
     "rsv_set_backward_mode": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "rsv_set_analytic_layers": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "rsv_analytic_layers": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
+                            ctypes.c_int),
     "rsv_backward_mode": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                            ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "rsv_describe_plan_mode": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t,

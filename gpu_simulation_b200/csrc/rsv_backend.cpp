@@ -246,13 +246,16 @@ void use_layer0_kernel(Plan &pl, int sms) {
   pl.layer0_grid = static_cast<int>(std::min<u64>(u64{1} << (pl.n - 12), static_cast<u64>(2 * std::max(1, sms))));
 }
 
+constexpr int kDefaultAnalyticLayers = 3;
+
 // The first K = min(L, 3) layers form a matrix-product state of bond
 // 2^(K-1) (rsv_mps.cu).  For n >= 13 their forward passes become one write of
 // that state and their backward passes one read of lambda at its output, which
 // gives all their 2nK gradients.
-void use_mps(Plan &pl, int sms) {
+void use_mps(Plan &pl, int sms, int max_k) {
   if (pl.n < 13 || pl.L < 2) return;
-  const int K = std::min(pl.L, 3);
+  const int K = std::min(pl.L, std::min(max_k, 3));
+  if (K < 2) return;
   int last = -1;
   for (size_t i = 0; i < pl.fwd.size(); ++i)
     if (pl.fwd[i].layer == K - 1) last = static_cast<int>(i);
@@ -424,11 +427,15 @@ Plan make_plan_full(int n, int L, int sms, bool checkpoint);
 // Plans of the single-circuit engine (half tiles on the eligible backward
 // passes); the batched kernel and the fixed-workspace entry point use
 // make_plan_full, whose tiles all have 12 bits.
-Plan make_plan(int n, int L, int sms, bool checkpoint = false) {
+// analytic: how many leading layers may skip their tile passes (3: layers
+// 0..2 as a matrix-product state, 2: layers 0..1, 1: layer 0's backward on the
+// layer-0 kernel, 0: every layer on tile passes, layer 0 computed in layer 1's
+// first forward pass as in the reference).
+Plan make_plan(int n, int L, int sms, bool checkpoint = false, int analytic = kDefaultAnalyticLayers) {
   Plan pl = make_plan_full(n, L, sms, checkpoint);
   use_half_tiles(pl, sms);
-  use_mps(pl, sms);
-  if (pl.mps_k == 0) use_layer0_kernel(pl, sms);
+  if (analytic >= 2) use_mps(pl, sms, analytic);
+  if (pl.mps_k == 0 && analytic >= 1) use_layer0_kernel(pl, sms);
   return pl;
 }
 
@@ -742,6 +749,7 @@ struct rsv_backend {
   rsv::Plan plan;
   rsv::DevBuf<double2> states;  // plan.num_bufs state buffers of state_len amplitudes each
   int backward_mode = RSV_BACKWARD_AUTO;
+  int analytic_layers = 3;  // rsv_set_analytic_layers (default: layers 0..2 as a matrix-product state)
   // gradient_strategy "inverse_walk_cuQuantum": gate-level kernels (rsv_gate.cu)
   bool gate_level = false;
   int gate_grid = 1;
@@ -1425,14 +1433,14 @@ void setup_plan(rsv_backend *B, int mode) {
     invalid("backward mode must be RSV_BACKWARD_AUTO, _UNCOMPUTE or _CHECKPOINT");
   const bool want = mode == RSV_BACKWARD_CHECKPOINT || (mode == RSV_BACKWARD_AUTO && checkpoint_fits(B->n, B->L));
   B->states.release();
-  Plan pl = make_plan(B->n, B->L, B->sms, want);
+  Plan pl = make_plan(B->n, B->L, B->sms, want, B->analytic_layers);
   B->state_len = size_t{1} << pl.phys;
   try {
     B->states.alloc(static_cast<size_t>(pl.num_bufs) * B->state_len);
   } catch (const Error &e) {
     if (mode != RSV_BACKWARD_AUTO || !pl.checkpoint || e.status != RSV_ERR_OUT_OF_MEMORY) throw;
     cudaGetLastError();  // clear the allocation failure
-    pl = make_plan(B->n, B->L, B->sms, false);
+    pl = make_plan(B->n, B->L, B->sms, false, B->analytic_layers);
     B->states.alloc(static_cast<size_t>(pl.num_bufs) * B->state_len);
   }
   check(cudaMemset(B->states.p, 0, B->states.count * sizeof(double2)), "state memset");
@@ -1802,6 +1810,24 @@ rsv_status rsv_set_backward_mode(rsv_backend *B, int mode) {
     if (B == nullptr) invalid("backend is null");
     check(cudaStreamSynchronize(B->stream), "backend synchronize");
     setup_plan(B, mode);
+  });
+}
+
+rsv_status rsv_set_analytic_layers(rsv_backend *B, int max_layers) {
+  return guarded([&] {
+    if (B == nullptr) invalid("backend is null");
+    if (max_layers < 0 || max_layers > 3) invalid("max_layers must be in [0, 3]");
+    check(cudaStreamSynchronize(B->stream), "backend synchronize");
+    B->analytic_layers = max_layers;
+    setup_plan(B, B->backward_mode);
+  });
+}
+
+rsv_status rsv_analytic_layers(rsv_backend *B, int *max_layers_out, int *used_out) {
+  return guarded([&] {
+    if (B == nullptr) invalid("backend is null");
+    if (max_layers_out) *max_layers_out = B->analytic_layers;
+    if (used_out) *used_out = B->plan.mps_k > 0 ? B->plan.mps_k : (B->plan.layer0_kernel ? 1 : 0);
   });
 }
 

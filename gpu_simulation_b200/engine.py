@@ -136,6 +136,17 @@ class Engine:
         names = {v: k for k, v in self.BACKWARD_MODES.items()}
         return {"mode": names[m.value], "checkpoint": bool(ck.value), "state_buffers": nb.value}
 
+    def set_analytic_layers(self, max_layers: int) -> None:
+        """How many leading layers (0..3, default 3) skip their tile passes:
+        the circuit's first layers form a low-bond matrix-product state, written
+        in one pass and differentiated from one read of lambda (n >= 13)."""
+        check(self._lib.rsv_set_analytic_layers(self._h, int(max_layers)))
+
+    def analytic_layers(self) -> dict:
+        m, u = ctypes.c_int(), ctypes.c_int()
+        check(self._lib.rsv_analytic_layers(self._h, ctypes.byref(m), ctypes.byref(u)))
+        return {"max_layers": m.value, "used": u.value}
+
     def set_field(self, field: float) -> None:
         """Change the transverse field h (same circuit shape and buffers)."""
         check(self._lib.rsv_set_field(self._h, float(field)))

@@ -200,6 +200,24 @@ rsv_status rsv_backward_mode(rsv_backend *backend, int *mode_out, int *checkpoin
                              int *num_buffers_out);
 
 /*
+ * Analytic leading layers (n >= 13).  The circuit starts from |0...0>, so after
+ * k layers its state is a periodic matrix-product state of bond dimension
+ * 2^(k-1) (the CNOT ring only turns indices into prefix parities).  With
+ * max_layers = 3 (the default) or 2, the first K = min(L, max_layers) layers
+ * are written in one pass from that form and all their gradients come from one
+ * read of lambda at their output (gpu_simulation_b200/csrc/rsv_mps.cu); with 1
+ * only layer 0's backward is replaced (one read of lambda, the layer-0 kernel);
+ * with 0 every layer runs through the tile passes, with layer 0 computed
+ * analytically inside layer 1's first forward pass like the reference
+ * (cpp/ising_cuda_rotation_kernels.cu:20-41).  Results agree to rounding in
+ * every setting.  rsv_set_analytic_layers re-plans (synchronises the backend's
+ * stream); rsv_analytic_layers reports the setting and the number of layers
+ * the current plan handles analytically.  No reference counterpart.
+ */
+rsv_status rsv_set_analytic_layers(rsv_backend *backend, int max_layers);
+rsv_status rsv_analytic_layers(rsv_backend *backend, int *max_layers_out, int *used_out);
+
+/*
  * Batched complex128 GEMM on FP64 tensor cores (mma.sync f64; the dense_scan
  * product tree uses it): C[b] = A[b] B[b] for b < batch, every matrix dim x dim
  * row-major and the batches contiguous; dim < 32 or a multiple of 32.  Device
