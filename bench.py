@@ -465,8 +465,8 @@ def main():
 
     peak, peak_src = measured_peaks()
     KERNEL_NAMES = {
-        "backward_pass": "backward (bwd_pass_kernel 12-bit tiles, bwd_half_kernel 11-bit tiles, grad01_kernel)",
-        "forward_pass": "fwd_pass_kernel + fwd01_kernel", "energy": "energy_tile_kernel + energy_kernel",
+        "backward_pass": "backward (bwd_pass_kernel 12-bit tiles, bwd_half_kernel 11-bit tiles, mps_grad_kernel)",
+        "forward_pass": "fwd_pass_kernel + mps_fwd_kernel", "energy": "energy_tile_kernel + energy_kernel",
     }
     kinds = {k: v for k, v in stats.items() if v["launches"]}
     dom = max(kinds, key=lambda k: kinds[k]["ms"])
