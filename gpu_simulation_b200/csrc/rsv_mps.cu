@@ -183,31 +183,54 @@ __global__ void mps_tables_kernel(const MpsParams Q) {
   } else if (e < 1024 + nlo + nhi) {
     const int hi = e - 1024 - nlo;
     store_mat<D>(Q.coshi + hi * D * D, site_chain<D>(Q.tsite, 12 + Q.m1, Q.m2, static_cast<unsigned>(hi)));
+  } else if (e < 1024 + nlo + nhi + 128) {
+    // in-tile halves: M1(a) = T_0..T_5 (entries 0..63), M2(h) = T_6..T_11 (64..127)
+    const int x = e - 1024 - nlo - nhi;
+    store_mat<D>(Q.mtab + x * D * D, site_chain<D>(Q.tsite, x < 64 ? 0 : 6, 6, static_cast<unsigned>(x & 63)));
   }
 }
 
 // --------------------------------------------------------------- forward
 // chi(r) = Tr(B0[r0] B1[r1] B2[r2] B3[r3]) for 4096 contiguous r per tile;
-// thread t takes r = base + t + 256 k: byte 0 is t, so chi = Tr(B1[r1] W)
-// with W = B2 B3 B0[t] fixed per tile.
+// thread t takes r = base + t + 256 k (k = 0..15): byte 0 is t, byte 1 is
+// k | (the tile's bits 12..15).  Per tile the 16 products Y_k = B1[r1(k)] B2 B3
+// go to shared memory (double-buffered, one barrier per tile) and every
+// amplitude is Tr(Y_k B0[t]) with B0[t] held in registers.
 template <int D, bool SCATTER>
 __global__ void __launch_bounds__(256) mps_fwd_kernel(const MpsParams Q, double2 *__restrict__ out) {
+  constexpr int E = D * D;
+  __shared__ double2 ysm[2][16][E];
   const int t = threadIdx.x, n = Q.n;
-  const Mat<D> b0 = ldg_mat<D>(Q.btab + t * D * D);
-  for (u64 tile = blockIdx.x; tile < Q.num_tiles; tile += gridDim.x) {
+  const Mat<D> b0 = ldg_mat<D>(Q.btab + t * E);
+  int it = 0;
+  for (u64 tile = blockIdx.x; tile < Q.num_tiles; tile += gridDim.x, ++it) {
     const u64 base = tile << 12;
-    const Mat<D> W = mmul<D>(mmul<D>(ldg_mat<D>(Q.btab + (512 + ((base >> 16) & 255)) * D * D),
-                                     ldg_mat<D>(Q.btab + (768 + ((base >> 24) & 255)) * D * D)),
-                             b0);
-    const int hi1 = static_cast<int>((base >> 8) & 0xF0);
+    double2(*ys)[E] = ysm[it & 1];
+    for (int s = t; s < 16 * E; s += 256) {
+      // entry (i, j) of Y_k = B1[r1] (B2 B3)
+      const int k = s / E, e = s % E, i = e / D, j = e % D;
+      const double2 *b1 = Q.btab + (256 + (static_cast<int>((base >> 8) & 0xF0) | k)) * E;
+      const double2 *b2 = Q.btab + (512 + ((base >> 16) & 255)) * E;
+      const double2 *b3 = Q.btab + (768 + ((base >> 24) & 255)) * E;
+      double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int m = 0; m < D; ++m) {
+        double2 q = make_double2(0.0, 0.0);  // (B2 B3)[m][j]
+#pragma unroll
+        for (int l = 0; l < D; ++l) q = cfma(__ldg(&b2[m * D + l]), __ldg(&b3[l * D + j]), q);
+        acc = cfma(__ldg(&b1[i * D + m]), q, acc);
+      }
+      ys[k][e] = acc;
+    }
+    __syncthreads();
 #pragma unroll 2
     for (int k = 0; k < 16; ++k) {
-      const double2 *b1 = Q.btab + (256 + (hi1 | k)) * D * D;
+      // Tr(Y_k B0) = sum_{i,j} Y_k[i][j] B0[j][i]
       double2 v = make_double2(0.0, 0.0);
 #pragma unroll
       for (int i = 0; i < D; ++i)
 #pragma unroll
-        for (int j = 0; j < D; ++j) v = cfma(__ldg(&b1[i * D + j]), W.m[j * D + i], v);
+        for (int j = 0; j < D; ++j) v = cfma(ys[k][i * D + j], b0.m[j * D + i], v);
       const u64 r = base | static_cast<u64>(t + 256 * k);
       __stcs(&out[SCATTER ? ring_p(r, n) : r], v);
     }
@@ -231,8 +254,8 @@ __global__ void __launch_bounds__(kMpsThreads) mps_grad_kernel(const MpsParams Q
   constexpr int EPT = E / 4;  // X / G / F entries per thread
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2 *stage = reinterpret_cast<double2 *>(smem_raw);
-  double2 *m1 = stage + 4096;  // [64][E]
-  double2 *m2 = m1 + 64 * E;
+  double2 *m1 = stage + 4096;  // [64][E]: T_0..T_5 (a), copied from the tables
+  double2 *m2 = m1 + 64 * E;   // [64][E]: T_6..T_11 (h)
   double2 *x1 = m2 + 64 * E;
   double2 *x2 = x1 + 64 * E;
   double2 *csm = x2 + 64 * E;  // [E]
@@ -240,10 +263,7 @@ __global__ void __launch_bounds__(kMpsThreads) mps_grad_kernel(const MpsParams Q
 
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int n = Q.n;
-  if (t < 128) {
-    const int half = t >> 6, x = t & 63;
-    store_mat<D>((half ? m2 : m1) + x * E, site_chain<D>(Q.tsite, 6 * half, 6, static_cast<unsigned>(x)));
-  }
+  for (int i = t; i < 128 * E; i += kMpsThreads) m1[i] = Q.mtab[i];
   __syncthreads();
 
   const int idx = t >> 2, q = t & 3;
@@ -496,7 +516,7 @@ size_t mps_partials_count(int bond) { return static_cast<size_t>(2) * 64 * bond 
 
 cudaError_t launch_mps_tables(const MpsParams &Q, cudaStream_t s) {
   if (Q.n < 13 || Q.n > 31 || (Q.bond != 2 && Q.bond != 4)) return cudaErrorInvalidValue;
-  const int count = 1024 + (1 << Q.m1) + (1 << Q.m2);
+  const int count = 1024 + (1 << Q.m1) + (1 << Q.m2) + 128;
   if (Q.bond == 2) {
     mps_site_kernel<2><<<1, 32, 0, s>>>(Q);
     mps_tables_kernel<2><<<(count + 127) / 128, 128, 0, s>>>(Q);

@@ -98,6 +98,7 @@ struct MpsParams {
   double2 *tsite;              // [32][2] site matrices T_w[b] (identity for w >= n)
   double2 *btab;               // [4][256] products over the eight wires of a byte
   double2 *coslo, *coshi;      // [2^m1], [2^m2] products over the coset wires
+  double2 *mtab;               // [128] in-tile halves: T_0..T_5 (a), T_6..T_11 (h)
   double2 *zt;                 // [2^(n-12)] per-tile Z
   double2 *ylo, *yhi;          // [2^m1], [2^m2] coset sums
   double2 *partials;           // [grid][2][64] per-CTA G, F
