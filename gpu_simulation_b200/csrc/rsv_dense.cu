@@ -59,12 +59,6 @@ constexpr int kGK = 16;
 constexpr int kAP = kGK + 4;  // A row pitch (16-byte elements)
 constexpr int kBP = kGT + 2;  // B row pitch
 
-__device__ __forceinline__ void mma_f64(double &d0, double &d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
-}
-
 __device__ __forceinline__ void cp16(void *smem, const void *gmem) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");

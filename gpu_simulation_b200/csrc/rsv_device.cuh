@@ -81,6 +81,15 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// D += A B on the FP64 tensor cores, one m8n8k4 tile per warp (row-major A,
+// column-major B).  Lane l holds A[l / 4][l % 4], B[l % 4][l / 4] and
+// D[l / 4][2 (l % 4) + {0, 1}].
+__device__ __forceinline__ void mma_f64(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
 #endif  // __CUDACC__
 
 }  // namespace rsv

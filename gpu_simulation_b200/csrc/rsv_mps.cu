@@ -239,7 +239,16 @@ __global__ void __launch_bounds__(256) mps_fwd_kernel(const MpsParams Q, double2
 
 // -------------------------------------------------------------- backward
 constexpr int kMpsThreads = 256;
-__device__ __forceinline__ int mps_slot(int i) { return i ^ ((i >> 6) & 7); }
+// Stage slot of tile amplitude i = a + 64 h.  Bond 2 reads a column (fixed a)
+// or a row (fixed h) of 32 entries per warp: i ^ (h & 7).  Bond 4 reads m8n8k4
+// fragments, 8 rows x 4 columns per warp in either orientation; with
+// i ^ ((h & 1) << 2 | (h & 2)) the eight 16-byte entries of every
+// quarter-warp fall in different bank groups.
+template <int D>
+__device__ __forceinline__ int mps_slot(int i) {
+  const int h = i >> 6;
+  return D == 4 ? i ^ (((h & 1) << 2) | (h & 2)) : i ^ (h & 7);
+}
 
 template <int D>
 constexpr size_t mps_grad_smem() {
@@ -275,6 +284,28 @@ __global__ void __launch_bounds__(kMpsThreads) mps_grad_kernel(const MpsParams Q
   const int ze = t % E, zpart = t / E;
   const int zi = ze / D, zj = ze % D;
 
+  // Bond 4: X1 and X2 on the FP64 tensor cores.  Warps 0..3 compute X1
+  // (rows a, K = h, B = M2), warps 4..7 X2 (rows h, K = a, B = M1), each warp
+  // 32 rows x 8 columns (columns 8 nt .. 8 nt + 7 of the 16 entries), as four
+  // m8n8k4 row tiles per K step.  The complex product conj(lambda) M is three
+  // real products (Gauss): t1 = lr Mr, t2 = li Mi, t3 = (lr - li)(Mr + Mi);
+  // re = t1 + t2, im = t3 - t1 + t2.  The warp's B fragments, 16 K steps of
+  // Mr, Mi and Mr + Mi, stay in registers for the whole kernel.
+  const int fg = lane >> 2, t4 = lane & 3;
+  const bool xsecond = warp >= 4;
+  const int xnt = warp & 1, xr0 = 32 * ((warp >> 1) & 1);
+  double bre[D == 4 ? 16 : 1], bim[D == 4 ? 16 : 1], bsum[D == 4 ? 16 : 1];
+  if constexpr (D == 4) {
+    const double2 *bt = Q.mtab + (xsecond ? 0 : 64 * E);
+#pragma unroll
+    for (int ks = 0; ks < 16; ++ks) {
+      const double2 v = bt[(4 * ks + t4) * E + 8 * xnt + fg];
+      bre[ks] = v.x;
+      bim[ks] = v.y;
+      bsum[ks] = v.x + v.y;
+    }
+  }
+
   const u64 num_tiles = Q.num_tiles;
   const unsigned lomask = (1u << Q.m1) - 1u;
   auto issue = [&](u64 tile) {
@@ -284,7 +315,7 @@ __global__ void __launch_bounds__(kMpsThreads) mps_grad_kernel(const MpsParams Q
       for (int r = 0; r < 4096 / kMpsThreads; ++r) {
         const int tau = t + r * kMpsThreads;
         const u64 p = base | static_cast<u64>(tau);
-        cp_async16(&stage[mps_slot(tau)], &lam[gather ? ring_p(p, n) : p]);
+        cp_async16(&stage[mps_slot<D>(tau)], &lam[gather ? ring_p(p, n) : p]);
       }
     }
     cp_async_commit();
@@ -313,14 +344,34 @@ __global__ void __launch_bounds__(kMpsThreads) mps_grad_kernel(const MpsParams Q
       for (int kk = 1; kk < D; ++kk) s = cfma(__ldg(&cl[i * D + kk]), __ldg(&ch[kk * D + j]), s);
       csm[t] = s;
     }
-    {
+    if constexpr (D == 4) {
+      double t1[4][2] = {}, t2[4][2] = {}, t3[4][2] = {};
+#pragma unroll
+      for (int ks = 0; ks < 16; ++ks) {
+#pragma unroll
+        for (int rt = 0; rt < 4; ++rt) {
+          const int row = xr0 + 8 * rt + fg, col = 4 * ks + t4;
+          const double2 l = stage[mps_slot<D>(xsecond ? col + 64 * row : row + 64 * col)];
+          mma_f64(t1[rt][0], t1[rt][1], l.x, bre[ks]);
+          mma_f64(t2[rt][0], t2[rt][1], l.y, bim[ks]);
+          mma_f64(t3[rt][0], t3[rt][1], l.x - l.y, bsum[ks]);
+        }
+      }
+      double2 *xo = xsecond ? x2 : x1;
+#pragma unroll
+      for (int rt = 0; rt < 4; ++rt)
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+          xo[(xr0 + 8 * rt + fg) * E + 8 * xnt + 2 * t4 + e] =
+              make_double2(t1[rt][e] + t2[rt][e], t3[rt][e] - t1[rt][e] + t2[rt][e]);
+    } else {
       double2 a1[EPT], a2[EPT];
 #pragma unroll
       for (int j = 0; j < EPT; ++j) a1[j] = a2[j] = make_double2(0.0, 0.0);
 #pragma unroll 4
       for (int kk = 0; kk < 64; ++kk) {
-        const double2 c1 = stage[mps_slot(idx + 64 * kk)];  // a = idx, h = kk
-        const double2 c2 = stage[mps_slot(kk + 64 * idx)];  // a = kk, h = idx
+        const double2 c1 = stage[mps_slot<D>(idx + 64 * kk)];  // a = idx, h = kk
+        const double2 c2 = stage[mps_slot<D>(kk + 64 * idx)];  // a = kk, h = idx
 #pragma unroll
         for (int j = 0; j < EPT; ++j) {
           a1[j] = cjfma(c1, m2[kk * E + q + 4 * j], a1[j]);
