@@ -763,7 +763,7 @@ struct rsv_backend {
   rsv::DevBuf<double> layer0_partials;                           // [layer0_grid][kLayer0Stride]
   // matrix-product stage (rsv_mps.cu): site matrices, forward byte tables,
   // coset tables, per-tile Z, coset sums, per-CTA G/F and their sums
-  rsv::DevBuf<double2> mps_tsite, mps_btab, mps_coslo, mps_coshi, mps_mtab, mps_zt, mps_ylo, mps_yhi, mps_partials,
+  rsv::DevBuf<double2> mps_tsite, mps_btab, mps_coslo, mps_coshi, mps_mtab, mps_wtab, mps_zt, mps_ylo, mps_yhi, mps_partials,
       mps_gf;
   rsv::DevBuf<int> tables;  // pass_grid | theta_pass | theta_slot | phi_pass
   rsv::DevBuf<int> order;   // undo order of the wires within a backward layer
@@ -934,6 +934,7 @@ MpsParams mps_params(rsv_backend *B) {
   Q.coslo = B->mps_coslo.p;
   Q.coshi = B->mps_coshi.p;
   Q.mtab = B->mps_mtab.p;
+  Q.wtab = B->mps_wtab.p;
   Q.zt = B->mps_zt.p;
   Q.ylo = B->mps_ylo.p;
   Q.yhi = B->mps_yhi.p;
@@ -1459,6 +1460,7 @@ void setup_plan(rsv_backend *B, int mode) {
     B->mps_coslo.alloc((size_t{1} << m1) * e);
     B->mps_coshi.alloc((size_t{1} << m2) * e);
     B->mps_mtab.alloc(128 * e);
+    B->mps_wtab.alloc((size_t{1} << std::max(0, B->n - 16)) * e);
     B->mps_zt.alloc((size_t{1} << m) * e);
     B->mps_ylo.alloc((size_t{1} << m1) * e);
     B->mps_yhi.alloc((size_t{1} << m2) * e);

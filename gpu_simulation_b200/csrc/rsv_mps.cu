@@ -187,25 +187,112 @@ __global__ void mps_tables_kernel(const MpsParams Q) {
     // in-tile halves: M1(a) = T_0..T_5 (entries 0..63), M2(h) = T_6..T_11 (64..127)
     const int x = e - 1024 - nlo - nhi;
     store_mat<D>(Q.mtab + x * D * D, site_chain<D>(Q.tsite, x < 64 ? 0 : 6, 6, static_cast<unsigned>(x & 63)));
+  } else if (e < 1024 + nlo + nhi + 128 + (1 << (Q.n > 16 ? Q.n - 16 : 0))) {
+    // W(x) = B2[x & 255] B3[x >> 8]: the product over wires 16..31
+    const int x = e - 1024 - nlo - nhi - 128;
+    store_mat<D>(Q.wtab + x * D * D, site_chain<D>(Q.tsite, 16, 16, static_cast<unsigned>(x)));
   }
 }
 
 // --------------------------------------------------------------- forward
-// chi(r) = Tr(B0[r0] B1[r1] B2[r2] B3[r3]) for 4096 contiguous r per tile;
-// thread t takes r = base + t + 256 k (k = 0..15): byte 0 is t, byte 1 is
-// k | (the tile's bits 12..15).  Per tile the 16 products Y_k = B1[r1(k)] B2 B3
-// go to shared memory (double-buffered, one barrier per tile) and every
-// amplitude is Tr(Y_k B0[t]) with B0[t] held in registers.
+// chi(r) = Tr(B0[r0] B1[r1] B2[r2] B3[r3]) (r_k the bytes of r), written as
+// out[P(r)] = chi(r) when SCATTER (the ring of the last MPS layer applied) and
+// out[r] = chi(r) otherwise.
+//
+// Bond 4: every tile is 4096 contiguous OUTPUT indices o = base + t + 256 k,
+// evaluated at r = P^{-1}(o) (identity without SCATTER), so every store is a
+// whole line.  Byte 0 of P^{-1}(o) depends on o's bits 0..7 and bit n-1 only,
+// bytes 1..3 on o's bits 7..31, so per tile the 32 products
+// Y_{k,s} = B1 W at P^{-1}(base + 256 k + 128 s) (s = bit 7 of t; W = B2 B3
+// from a table over bytes 2 and 3) go to
+// shared memory (double-buffered, one barrier per tile), and the traces
+// out[t][k] = Tr(Y_{k,t7} B0[r0(t)]) = sum_e A[t][e] Y_{k,t7}[e]
+// (A[t][(i, j)] = B0[r0(t)][j][i]) are one complex product per half tile on
+// the FP64 tensor cores: warp w takes rows t = 32 w .. 32 w + 31 (t7 = w / 4)
+// as four m8n8k4 row tiles by two column tiles, its A fragments in registers
+// (reloaded when bit n-1 of the tile changes), Gauss 3-multiply; two CTAs per
+// SM (128 registers) hide the latency of the per-tile table loads.
+//
+// Bond 2: thread t takes r = base + t + 256 k (k = 0..15): byte 0 is t, byte 1
+// is k | (the tile's bits 12..15).  Per tile the 16 products
+// Y_k = B1[r1(k)] B2 B3 go to shared memory and every amplitude is
+// Tr(Y_k B0[t]) with B0[t] held in registers, stored at P(r).
 template <int D, bool SCATTER>
-__global__ void __launch_bounds__(256) mps_fwd_kernel(const MpsParams Q, double2 *__restrict__ out) {
+__global__ void __launch_bounds__(256, D == 4 ? 2 : 1) mps_fwd_kernel(const MpsParams Q, double2 *__restrict__ out) {
   constexpr int E = D * D;
-  __shared__ double2 ysm[2][16][E];
+  constexpr int YP = D == 4 ? 20 : E;  // row pitch of Y: fragment reads free of bank conflicts
+  __shared__ double2 ysm[2][D == 4 ? 32 : 16][YP];
   const int t = threadIdx.x, n = Q.n;
+  if constexpr (D == 4) {
+    const int lane = t & 31, warp = t >> 5, fg = lane >> 2, t4 = lane & 3;
+    const int ys_set = warp >> 2;
+    double are[4][4], aim[4][4], asum[4][4];
+    int aflip = -1;  // bit n-1 of the tiles the A fragments were loaded for
+    int it = 0;
+    for (u64 tile = blockIdx.x; tile < Q.num_tiles; tile += gridDim.x, ++it) {
+      const u64 base = tile << 12;
+      const int flip = SCATTER ? static_cast<int>((base >> (n - 1)) & 1) : 0;
+      if (flip != aflip) {
+        aflip = flip;
+#pragma unroll
+        for (int rt = 0; rt < 4; ++rt) {
+          const u64 o = base | static_cast<u64>(32 * warp + 8 * rt + fg);
+          const int r0 = static_cast<int>((SCATTER ? ring_pinv(o, n) : o) & 255);
+#pragma unroll
+          for (int ks = 0; ks < 4; ++ks) {
+            // K index 4 ks + t4 = (i, j) = (ks, t4): A = B0[r0][t4][ks]
+            const double2 v = __ldg(&Q.btab[r0 * E + t4 * D + ks]);
+            are[rt][ks] = v.x;
+            aim[rt][ks] = v.y;
+            asum[rt][ks] = v.x + v.y;
+          }
+        }
+      }
+      double2(*ys)[YP] = ysm[it & 1];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int ks_ = h * 16 + (t >> 4), e = t & 15, i = e / D, j = e % D;  // ks_ = 16 s + k
+        const u64 o = base | (static_cast<u64>(ks_ & 15) << 8) | (static_cast<u64>(ks_ >> 4) << 7);
+        const u64 r = SCATTER ? ring_pinv(o, n) : o;
+        const double2 *b1 = Q.btab + (256 + ((r >> 8) & 255)) * E;
+        const double2 *w = Q.wtab + (r >> 16) * E;
+        double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int m = 0; m < D; ++m) acc = cfma(__ldg(&b1[i * D + m]), __ldg(&w[m * D + j]), acc);
+        ys[ks_][e] = acc;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int ct = 0; ct < 2; ++ct) {
+        double t1[4][2] = {}, t2[4][2] = {}, t3[4][2] = {};
+#pragma unroll
+        for (int ks = 0; ks < 4; ++ks) {
+          const double2 y = ys[16 * ys_set + 8 * ct + fg][4 * ks + t4];
+          const double ysum = y.x + y.y;
+#pragma unroll
+          for (int rt = 0; rt < 4; ++rt) {
+            mma_f64(t1[rt][0], t1[rt][1], are[rt][ks], y.x);
+            mma_f64(t2[rt][0], t2[rt][1], aim[rt][ks], y.y);
+            mma_f64(t3[rt][0], t3[rt][1], asum[rt][ks], ysum);
+          }
+        }
+#pragma unroll
+        for (int rt = 0; rt < 4; ++rt)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const double2 v = make_double2(t1[rt][e] - t2[rt][e], t3[rt][e] - t1[rt][e] - t2[rt][e]);
+            const u64 o = base | static_cast<u64>(32 * warp + 8 * rt + fg + 256 * (8 * ct + 2 * t4 + e));
+            __stcs(&out[o], v);
+          }
+      }
+    }
+    return;
+  }
   const Mat<D> b0 = ldg_mat<D>(Q.btab + t * E);
   int it = 0;
   for (u64 tile = blockIdx.x; tile < Q.num_tiles; tile += gridDim.x, ++it) {
     const u64 base = tile << 12;
-    double2(*ys)[E] = ysm[it & 1];
+    double2(*ys)[YP] = ysm[it & 1];
     for (int s = t; s < 16 * E; s += 256) {
       // entry (i, j) of Y_k = B1[r1] (B2 B3)
       const int k = s / E, e = s % E, i = e / D, j = e % D;
@@ -567,7 +654,7 @@ size_t mps_partials_count(int bond) { return static_cast<size_t>(2) * 64 * bond 
 
 cudaError_t launch_mps_tables(const MpsParams &Q, cudaStream_t s) {
   if (Q.n < 13 || Q.n > 31 || (Q.bond != 2 && Q.bond != 4)) return cudaErrorInvalidValue;
-  const int count = 1024 + (1 << Q.m1) + (1 << Q.m2) + 128;
+  const int count = 1024 + (1 << Q.m1) + (1 << Q.m2) + 128 + (1 << (Q.n > 16 ? Q.n - 16 : 0));
   if (Q.bond == 2) {
     mps_site_kernel<2><<<1, 32, 0, s>>>(Q);
     mps_tables_kernel<2><<<(count + 127) / 128, 128, 0, s>>>(Q);

@@ -99,6 +99,7 @@ struct MpsParams {
   double2 *btab;               // [4][256] products over the eight wires of a byte
   double2 *coslo, *coshi;      // [2^m1], [2^m2] products over the coset wires
   double2 *mtab;               // [128] in-tile halves: T_0..T_5 (a), T_6..T_11 (h)
+  double2 *wtab;               // [2^max(0, n-16)] products over wires 16..31 (bytes 2 and 3)
   double2 *zt;                 // [2^(n-12)] per-tile Z
   double2 *ylo, *yhi;          // [2^m1], [2^m2] coset sums
   double2 *partials;           // [grid][2][64] per-CTA G, F
