@@ -182,6 +182,9 @@ struct Plan {
   int mps_k = 0;
   bool mps_scatter = false;
   int mps_out = -1, mps_lam = -1, mps_load = kLoadNatural, mps_fwd_grid = 1, mps_grad_grid = 1;
+  // bond 4 with layers after it: the first forward pass of layer mps_k
+  // evaluates the state itself (kLoadMpsP) and nothing writes mps_out
+  bool mps_fused = false;
 };
 
 // Checkpoint-mode plans keep max((L-1) * passes + 1, 2) state buffers; they
@@ -278,6 +281,23 @@ void use_mps(Plan &pl, int sms, int max_k) {
   }
   for (int l = 0; l < K; ++l) pl.phi_pass[static_cast<size_t>(l)] = -1;
   pl.mps_k = K;
+  if (K == 3 && pl.L > K && !pl.fwd.empty() && pl.mps_scatter) {
+    Step &f = pl.fwd.front();
+    bool unit = f.tile.dims == 12;
+    for (int b = 0; unit && b < 12; ++b) unit = f.tile.vec[b] == (u64{1} << b);
+    if (unit && f.layer == K && f.psi_load == kLoadNatural && f.psi_in == pl.mps_out &&
+        f.psi_store == kStoreNatural && !f.phase) {
+      f.psi_load = kLoadMpsP;
+      f.psi_in = -1;
+      pl.mps_fused = true;
+    }
+  }
+  // psi at the input of layer K (written back by the uncompute schedule for
+  // the layers below) is not needed: those layers' gradients come from lambda
+  if (!pl.bwd.empty() && pl.bwd.back().layer == K && pl.bwd.back().tile.dims == 12) {
+    pl.bwd.back().psi_store = kStoreNone;
+    pl.bwd.back().psi_out = -1;
+  }
   const u64 tiles = u64{1} << (pl.n - 12);
   pl.mps_fwd_grid = static_cast<int>(std::min<u64>(tiles, static_cast<u64>(8 * std::max(1, sms))));
   // bond 2: two CTAs per SM (83 KiB of shared memory), bond 4: one (135 KiB)
@@ -612,6 +632,7 @@ const char *load_name(int m) {
     case kLoadGatherP: return "gatherP";
     case kLoadProduct: return "product(P)";
     case kLoadProductPlain: return "product";
+    case kLoadMpsP: return "mpsP";
   }
   return "?";
 }
@@ -655,7 +676,7 @@ std::string describe(const Plan &pl) {
   };
   os << "n=" << pl.n << " L=" << pl.L << " phys=" << pl.phys << " bufs=" << pl.num_bufs
      << " mode=" << (pl.checkpoint ? "checkpoint" : "uncompute") << "\n";
-  if (pl.mps_k > 0)
+  if (pl.mps_k > 0 && !pl.mps_fused)
     os << "mps K=" << pl.mps_k << " fwd psi:" << (pl.mps_scatter ? "scatterP" : "store") << "(" << pl.mps_out
        << ") grid=" << pl.mps_fwd_grid << "\n";
   for (const auto &s : pl.fwd)
@@ -880,6 +901,8 @@ void fill_pass_params(rsv_backend *B, const Step &s, PassParams &P) {
   P.partials = s.bwd ? B->pass_partials.p + static_cast<size_t>(s.pass_index) * B->plan.max_grid *
                                                  kPartialStride
                      : nullptr;
+  P.mps_btab = B->mps_btab.p;
+  P.mps_wtab = B->mps_wtab.p;
 }
 
 cudaEvent_t take_event(rsv_backend *B) {
@@ -945,7 +968,10 @@ MpsParams mps_params(rsv_backend *B) {
 }
 
 void run_forward(rsv_backend *B, cudaStream_t st) {
-  if (B->plan.mps_k > 0) {
+  if (B->plan.mps_k > 0 && B->plan.mps_fused) {
+    const MpsParams Q = mps_params(B);
+    timed(B, st, 0, 0.0, [&] { check(launch_mps_tables(Q, st), "matrix-product tables launch"); });
+  } else if (B->plan.mps_k > 0) {
     const MpsParams Q = mps_params(B);
     timed(B, st, 1, 16.0 * static_cast<double>(u64{1} << B->n), [&] {
       check(launch_mps_tables(Q, st), "matrix-product tables launch");

@@ -93,6 +93,70 @@ __device__ __forceinline__ void transpose(double2 *sm, int tp_from, int rb_from,
 // transpose buffer (CTA-wide, or 16 warp slices of 256 entries).
 constexpr size_t kBwdSmem = 3 * kTileSize * sizeof(double2);
 constexpr size_t kFwdSmem = kTileSize * sizeof(double2);
+// kLoadMpsP: the 32 per-tile products Y (row pitch 20) after the transpose buffer
+constexpr int kMpsYPitch = 20;
+constexpr size_t kFwdMpsSmem = kFwdSmem + 32 * kMpsYPitch * sizeof(double2);
+
+// kLoadMpsP source of a forward pass: the bond-4 matrix-product state chi of
+// the first three layers at r = P^{-1}(o), for the 4096 indices
+// o = cbase + t of a unit tile over index bits 0..11, written to
+// trans[swz(t)].  chi(r) = Tr(B0[r0] B1[r1] W[r >> 16]) (byte tables of site
+// products, W = B2 B3).  Byte 0 of P^{-1}(o) depends only on bits 0..7 of o and
+// bit n-1, bytes 1..3 only on bits 7..31, so the tile needs the 32 products
+// Y_{k,s} = B1 W at P^{-1}(cbase + 256 k + 128 s) and its amplitudes are
+// out[t0][k] = Tr(Y_{k,t0>>7} B0[r0(t0)]) = sum_e A[t0][e] Y[e] (t = t0 + 256 k,
+// A[t0][(i, j)] = B0[r0][j][i]): per warp 32 rows t0 as four m8n8k4 f64
+// tensor-core row tiles by two column tiles, Gauss 3-multiply.
+__device__ __forceinline__ void mps_tile_p(const PassParams &P, u32 cbase, double2 *trans, double2 *ysm,
+                                           int lane, int warp) {
+  constexpr int E = 16;
+  const int t = threadIdx.x, n = P.n;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int ks = h * 16 + (t >> 4), e = t & 15, i = e >> 2, j = e & 3;  // ks = 16 s + k
+    const u64 o = static_cast<u64>(cbase) | (static_cast<u64>(ks & 15) << 8) | (static_cast<u64>(ks >> 4) << 7);
+    const u64 r = ring_pinv(o, n);
+    const double2 *b1 = P.mps_btab + (256 + ((r >> 8) & 255)) * E;
+    const double2 *w = P.mps_wtab + (r >> 16) * E;
+    double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      const double2 x = __ldg(&b1[i * 4 + m]), y = __ldg(&w[m * 4 + j]);
+      acc = make_double2(fma(x.x, y.x, fma(-x.y, y.y, acc.x)), fma(x.x, y.y, fma(x.y, y.x, acc.y)));
+    }
+    ysm[ks * kMpsYPitch + e] = acc;
+  }
+  const int fg = lane >> 2, t4 = lane & 3, ys_set = warp >> 2;
+  // A = B0[r0][t4][ks] for K index 4 ks + t4 = (i, j) = (ks, t4)
+  const double2 *arow[4];
+#pragma unroll
+  for (int rt = 0; rt < 4; ++rt)
+    arow[rt] = P.mps_btab + (ring_pinv(static_cast<u64>(cbase | (32 * warp + 8 * rt + fg)), n) & 255) * E + t4 * 4;
+  __syncthreads();
+#pragma unroll
+  for (int ct = 0; ct < 2; ++ct) {
+    double t1[4][2] = {}, t2[4][2] = {}, t3[4][2] = {};
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks) {
+      const double2 y = ysm[(16 * ys_set + 8 * ct + fg) * kMpsYPitch + 4 * ks + t4];
+      const double ysum = y.x + y.y;
+#pragma unroll
+      for (int rt = 0; rt < 4; ++rt) {
+        const double2 av = __ldg(&arow[rt][ks]);
+        mma_f64(t1[rt][0], t1[rt][1], av.x, y.x);
+        mma_f64(t2[rt][0], t2[rt][1], av.y, y.y);
+        mma_f64(t3[rt][0], t3[rt][1], av.x + av.y, ysum);
+      }
+    }
+#pragma unroll
+    for (int rt = 0; rt < 4; ++rt)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int tt = 32 * warp + 8 * rt + fg + 256 * (8 * ct + 2 * t4 + e);
+        trans[swz(tt)] = make_double2(t1[rt][e] - t2[rt][e], t3[rt][e] - t1[rt][e] - t2[rt][e]);
+      }
+  }
+}
 
 // ---------------------------------------------------------------- backward
 // phi-gradient sums of the first backward pass of a layer without a CTA
@@ -351,6 +415,14 @@ __global__ void __launch_bounds__(kThreads, 2) fwd_pass_kernel(const PassParams 
     }
     if (PSRC == kLoadProduct) table4_regs(P.prod, static_cast<u32>(ring_pinv(base, n)), poff, a);
     if (PSRC == kLoadProductPlain) table4_regs(P.prod, base, poff, a);
+    if (PSRC == kLoadMpsP) {
+      mps_tile_p(P, cbase, trans, trans + kTileSize, lane, warp);
+      __syncthreads();
+      const int tpf = thread_part(first, lane, warp);
+#pragma unroll
+      for (int r = 0; r < kRegs; ++r) a[r] = trans[swz(tpf | (r << rl))];
+      __syncthreads();
+    }
     if (P.sync_after_load) __syncthreads();
 
     int prev = first;
@@ -390,14 +462,14 @@ cudaError_t launch_bwd(const PassParams &P, int grid, cudaStream_t s) {
 template <int PSRC, int PDST, bool PHASE>
 cudaError_t launch_fwd(const PassParams &P, int grid, cudaStream_t s) {
   auto k = fwd_pass_kernel<PSRC, PDST, PHASE>;
+  constexpr size_t smem = PSRC == kLoadMpsP ? kFwdMpsSmem : kFwdSmem;
   static bool configured = false;
   if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(kFwdSmem));
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  k<<<grid, kThreads, kFwdSmem, s>>>(P);
+  k<<<grid, kThreads, smem, s>>>(P);
   return cudaGetLastError();
 }
 
@@ -427,6 +499,7 @@ cudaError_t launch_pass(const PassParams &P, bool bwd, int grid, cudaStream_t s)
     RSV_BWD(kLoadNatural, kLoadGatherP, kStoreNone, kStoreNone)
     // checkpoint schedule: psi read from a checkpoint (or analytic), only lambda written
     RSV_BWD(kLoadNatural, kLoadNatural, kStoreNone, kStoreNatural)
+    RSV_BWD(kLoadNatural, kLoadGatherP, kStoreNone, kStoreNatural)
     RSV_BWD(kLoadGatherP, kLoadGatherP, kStoreNone, kStoreNatural)
     RSV_BWD(kLoadProductPlain, kLoadGatherP, kStoreNone, kStoreNatural)
     RSV_BWD(kLoadProductPlain, kLoadNatural, kStoreNone, kStoreNatural)
@@ -438,6 +511,14 @@ cudaError_t launch_pass(const PassParams &P, bool bwd, int grid, cudaStream_t s)
   const int src = P.psi_load, dst = P.psi_store;
   if (src == kLoadProductPlain && dst == kStoreNatural && !phase)
     return launch_fwd<kLoadProductPlain, kStoreNatural, false>(P, grid, s);
+  if (src == kLoadMpsP) {
+    // unit tile over index bits 0..11 only
+    for (int b = 0; b < 12; ++b)
+      if (P.vec[b] != (1ull << b)) return cudaErrorInvalidValue;
+    if (P.n < 13 || P.n > 31 || P.mps_btab == nullptr || P.mps_wtab == nullptr) return cudaErrorInvalidValue;
+    if (dst == kStoreNatural && !phase) return launch_fwd<kLoadMpsP, kStoreNatural, false>(P, grid, s);
+    return cudaErrorInvalidValue;
+  }
 #define RSV_FWD(SRC)                                                                 \
   if (src == SRC) {                                                                  \
     if (dst == kStoreNatural)                                                        \

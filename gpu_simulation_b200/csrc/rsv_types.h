@@ -12,6 +12,8 @@ enum LoadMode : int {
   kLoadGatherP = 1,   // buf[P(p)]      (undo one ring layer: out = P^{-1} in)
   kLoadProduct = 2,   // analytic layer-0 product state at P^{-1}(p) (= P applied to it)
   kLoadProductPlain = 3,  // analytic layer-0 product state at p
+  kLoadMpsP = 4,      // bond-4 matrix-product state of the first layers at P^{-1}(p)
+                      // (forward, unit tile over index bits 0..11 only)
 };
 
 // How a pass writes its output amplitudes.
@@ -75,6 +77,8 @@ struct PassParams {
   const double2 *prod;         // layer-0 product-state byte tables, [4][256] (full or partial)
   double *partials;            // [gridDim.x][kPartialStride] for this pass
   int tile_bits;               // 12, or 11 for a backward pass on the half tile (rsv_pass_half.cu)
+  const double2 *mps_btab;     // kLoadMpsP: byte tables [4][256] of 4x4 site products
+  const double2 *mps_wtab;     // kLoadMpsP: products over wires 16..31 [2^max(0, n-16)]
 };
 
 // Layer-0 gradients from lambda alone (rsv_layer0.cu): per-CTA records of

@@ -211,6 +211,11 @@ def simulate(n: int, layers: int, field: float, params: np.ndarray, check_indice
             return product(ring_pinv(idx, n))
         if mode == "product":
             return product(idx)
+        if mode == "mpsP":
+            # the first K layers (their last ring applied), evaluated by the pass itself
+            K = plan["mps"]["K"]
+            chi = chi_k([[ry_rz(p[k, w, 0], p[k, w, 1]) for w in range(n)] for k in range(K)])
+            return chi[ring_pinv(idx, n)]
         raise ValueError(mode)
 
     def store(mode, bid, v):
