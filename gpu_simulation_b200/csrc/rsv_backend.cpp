@@ -187,18 +187,18 @@ struct Plan {
   bool mps_fused = false;
 };
 
-// Checkpoint-mode plans keep max((L-1) * passes + 1, 2) state buffers; they
-// are chosen automatically while those fit this budget.
+// Checkpoint-mode plans keep one state buffer per forward pass of the layers
+// on tile passes, plus lambda; they are chosen automatically while those fit
+// this budget.
 constexpr double kCheckpointBudgetBytes = 96.0 * (1ull << 30);
 
-int passes_per_layer(int n) {
-  if (n <= kTileBits) return 1;
-  return 1 + static_cast<int>(high_tiles(n, 12).size());
-}
+Plan make_plan(int n, int L, int sms, bool checkpoint, int analytic);
 
-bool checkpoint_fits(int n, int L) {
+// The checkpoint schedule is chosen automatically while its state buffers
+// (after the leading layers the analytic kernels replace) fit the budget.
+bool checkpoint_fits(int n, int L, int analytic) {
   if (n <= kTileBits) return false;
-  const double bufs = static_cast<double>(std::max((L - 1) * passes_per_layer(n) + 1, 2));
+  const double bufs = static_cast<double>(make_plan(n, L, 148, true, analytic).num_bufs);
   return bufs * 16.0 * static_cast<double>(u64{1} << n) <= kCheckpointBudgetBytes;
 }
 
@@ -451,11 +451,42 @@ Plan make_plan_full(int n, int L, int sms, bool checkpoint);
 // 0..2 as a matrix-product state, 2: layers 0..1, 1: layer 0's backward on the
 // layer-0 kernel, 0: every layer on tile passes, layer 0 computed in layer 1's
 // first forward pass as in the reference).
-Plan make_plan(int n, int L, int sms, bool checkpoint = false, int analytic = kDefaultAnalyticLayers) {
+// Renumber the state buffers the plan still uses as 0, 1, ... (the passes of
+// the layers that the matrix-product or layer-0 kernels replace leave their
+// checkpoints unused); at least two (the gate-level path uses buffers 0, 1).
+void compact_buffers(Plan &pl) {
+  std::vector<int> map(static_cast<size_t>(std::max(pl.num_bufs, 0)), -1);
+  int next = 0;
+  auto use = [&](int &b) {
+    if (b < 0) return;
+    if (b >= static_cast<int>(map.size())) throw Error(RSV_ERR_INTERNAL, "buffer id out of range");
+    if (map[static_cast<size_t>(b)] < 0) map[static_cast<size_t>(b)] = next++;
+    b = map[static_cast<size_t>(b)];
+  };
+  for (auto &s : pl.fwd) {
+    use(s.psi_in);
+    use(s.psi_out);
+  }
+  use(pl.chi_buf);
+  use(pl.mu_buf);
+  for (auto &s : pl.bwd) {
+    use(s.psi_in);
+    use(s.psi_out);
+    use(s.lam_in);
+    use(s.lam_out);
+  }
+  if (pl.mps_k > 0 && !pl.mps_fused) use(pl.mps_out);
+  if (pl.mps_k > 0) use(pl.mps_lam);
+  if (pl.layer0_kernel) use(pl.layer0_lam);
+  pl.num_bufs = std::max(next, 2);
+}
+
+Plan make_plan(int n, int L, int sms, bool checkpoint, int analytic) {
   Plan pl = make_plan_full(n, L, sms, checkpoint);
   use_half_tiles(pl, sms);
   if (analytic >= 2) use_mps(pl, sms, analytic);
   if (pl.mps_k == 0 && analytic >= 1) use_layer0_kernel(pl, sms);
+  compact_buffers(pl);
   return pl;
 }
 
@@ -1460,7 +1491,8 @@ rsv_status run_in_workspace(int n, int L, double field, const double *d_params, 
 void setup_plan(rsv_backend *B, int mode) {
   if (mode != RSV_BACKWARD_AUTO && mode != RSV_BACKWARD_UNCOMPUTE && mode != RSV_BACKWARD_CHECKPOINT)
     invalid("backward mode must be RSV_BACKWARD_AUTO, _UNCOMPUTE or _CHECKPOINT");
-  const bool want = mode == RSV_BACKWARD_CHECKPOINT || (mode == RSV_BACKWARD_AUTO && checkpoint_fits(B->n, B->L));
+  const bool want = mode == RSV_BACKWARD_CHECKPOINT ||
+                    (mode == RSV_BACKWARD_AUTO && checkpoint_fits(B->n, B->L, B->analytic_layers));
   B->states.release();
   Plan pl = make_plan(B->n, B->L, B->sms, want, B->analytic_layers);
   B->state_len = size_t{1} << pl.phys;
@@ -1512,9 +1544,10 @@ void setup_plan(rsv_backend *B, int mode) {
 }
 
 Plan plan_for_mode(int n, int L, int mode) {
-  if (mode == RSV_BACKWARD_AUTO) return make_plan(n, L, 148, checkpoint_fits(n, L));
-  if (mode == RSV_BACKWARD_UNCOMPUTE) return make_plan(n, L, 148, false);
-  if (mode == RSV_BACKWARD_CHECKPOINT) return make_plan(n, L, 148, true);
+  if (mode == RSV_BACKWARD_AUTO)
+    return make_plan(n, L, 148, checkpoint_fits(n, L, kDefaultAnalyticLayers), kDefaultAnalyticLayers);
+  if (mode == RSV_BACKWARD_UNCOMPUTE) return make_plan(n, L, 148, false, kDefaultAnalyticLayers);
+  if (mode == RSV_BACKWARD_CHECKPOINT) return make_plan(n, L, 148, true, kDefaultAnalyticLayers);
   invalid("backward mode must be RSV_BACKWARD_AUTO, _UNCOMPUTE or _CHECKPOINT");
 }
 

@@ -38,10 +38,16 @@ def test_both_schedules_match_oracle(n, L, h):
 
 def test_auto_mode_and_buffers():
     eng = Engine(14, 3, 1.0)
+    eng.set_analytic_layers(0)  # every layer on tile passes
     info = eng.backward_mode()
     assert info["mode"] == "auto" and info["checkpoint"] and info["state_buffers"] == 2 * 2 + 1
     eng.set_backward_mode("uncompute")
     assert eng.backward_mode()["state_buffers"] == 3
+    # layers 0..2 as a matrix-product state: only chi and lambda remain
+    eng.set_analytic_layers(3)
+    assert eng.backward_mode()["state_buffers"] == 2
+    eng.set_backward_mode("auto")
+    assert eng.backward_mode()["checkpoint"] and eng.backward_mode()["state_buffers"] == 2
     assert Engine(12, 3, 1.0).backward_mode()["checkpoint"] is False  # one tile: in place
 
 

@@ -78,7 +78,9 @@ def test_large_plans_cover_every_wire_once(n, L):
     ck = plan_sim.parse_plan(plan_sim.describe_plan(n, L, plan_sim.CHECKPOINT))
     fits = ck["bufs"] * 16 * 2 ** n <= 96 * 2 ** 30
     assert auto["mode"] == ("checkpoint" if fits else "uncompute")
-    assert plan_sim.parse_plan(plan_sim.describe_plan(n, L, plan_sim.UNCOMPUTE))["bufs"] == 3
+    # uncompute: psi, lambda and the target of the inverse-ring scatter (not
+    # needed when the leading layers are one read of lambda)
+    assert plan_sim.parse_plan(plan_sim.describe_plan(n, L, plan_sim.UNCOMPUTE))["bufs"] in (2, 3)
 
 
 def check_large_plan(plan, n, L):
