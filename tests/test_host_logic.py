@@ -57,6 +57,7 @@ def test_ring_map_matches_oracle_closed_form():
 @pytest.mark.parametrize("n,L,h", [
     (2, 1, 0.7), (2, 3, 1.0), (3, 2, 1.1), (5, 4, 0.3), (8, 2, 1.0), (11, 2, 0.9),
     (12, 3, 1.0), (13, 1, 1.2), (13, 3, 0.8), (14, 2, 1.0), (16, 2, 2.0), (17, 2, 0.5),
+    (13, 4, 0.8), (14, 5, 1.1),
 ])
 def test_plan_executed_in_numpy_matches_oracle(n, L, h):
     rng = np.random.default_rng(100 + n * 10 + L)
@@ -98,11 +99,32 @@ def check_large_plan(plan, n, L):
                 key = (st["layer"], w)
                 assert key not in seen
                 seen[key] = st["pass_index"]
+    # buffer ids are compact: every id below bufs is used (at least two buffers)
+    used = {plan["energy"][0], plan["energy"][1]}
+    for st in plan["steps"]:
+        if st.get("kind") == "mps_fwd":
+            used.add(st["out"])
+            continue
+        used.update(b for b in (st["psi_in"], st["psi_out"], st["lam_in"], st["lam_out"]) if b >= 0)
+    if plan["mps"] is not None:
+        used.add(plan["mps"]["buf"])
+    if plan["layer0"] is not None:
+        used.add(plan["layer0"]["buf"])
+    assert used == set(range(max(len(used), 2))) and plan["bufs"] == max(len(used), 2)
     if plan["mps"] is not None:
         # the first K layers are one read of lambda on the matrix-product kernels
         K = plan["mps"]["K"]
         assert all(layer >= K for layer, _ in seen)
         assert 0 <= plan["mps"]["buf"] < plan["bufs"]
+        fwd = [st for st in plan["steps"] if st.get("kind") != "mps_fwd" and not st["bwd"]]
+        if K == 3 and L > K:
+            # the bond-4 state is evaluated by layer 3's first forward pass itself
+            assert not any(st.get("kind") == "mps_fwd" for st in plan["steps"])
+            assert fwd[0]["psi_load"] == "mpsP" and fwd[0]["layer"] == K
+        bwd = [st for st in plan["steps"] if st.get("kind") != "mps_fwd" and st["bwd"]]
+        if bwd:
+            # psi below layer K is never needed
+            assert bwd[-1]["psi_store"] == "none"
         for layer in range(K):
             for w in range(n):
                 seen[(layer, w)] = -1
