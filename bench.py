@@ -350,6 +350,12 @@ def adam_section(n, L, steps, seed, field=1.0):
     t.record()
     t.synchronize()
     dev_ms = s.elapsed_time(t) / reps
+    # the same Adam loop on the device: energy_and_grad + fused Adam step, one
+    # step captured as a CUDA graph and replayed (torch.optim.Adam's update)
+    from gpu_simulation_b200.training import run_adam_device
+
+    run_adam_device(eng, p0, 3, lr=0.05)  # warm-up (fresh optimiser state per call)
+    dev_adam = run_adam_device(eng, p0, steps, lr=0.05)
     eng.close()
     threads = oracle.set_num_threads(0)
     oracle.energy_and_grad(n, L, field, p0.reshape(-1))
@@ -363,6 +369,10 @@ def adam_section(n, L, steps, seed, field=1.0):
         "adam_steps_per_s": steps * 1000.0 / loop_ms, "ms_per_adam_step": loop_ms / steps,
         "final_energy": final,
         "energy_and_grad_per_s_device": 1000.0 / dev_ms, "ms_per_energy_and_grad_device": dev_ms,
+        "device_adam_graph": {"adam_steps_per_s": steps * 1000.0 / dev_adam["gpu_ms"],
+                              "ms_per_adam_step": dev_adam["gpu_ms"] / steps,
+                              "energy_at_last_step": float(dev_adam["energies"][-1]),
+                              "torch_loop_energy_at_last_step": final},
         "cpu_baseline": {"value": 1.0 / cpu_s, "unit": "energy_and_grad/s", "cores": threads, "kind": "port",
                          "sample": f"{creps} energy_and_grad calls on the CPU restatement (oracle/)"},
     }

@@ -240,6 +240,45 @@ cudaError_t adam_step(long long count, T *p, const T *g, T *m, T *v, T lr, T bet
   return cudaGetLastError();
 }
 
+// One Adam step of a device-resident VQE loop with torch.optim.Adam's update
+// (bias-corrected, no weight decay): m <- m + (1 - beta1)(g - m),
+// v <- beta2 v + (1 - beta2) g^2, p <- p - (lr / c1) m / (sqrt(v) / sqrt(c2) + eps)
+// with c_i = 1 - beta_i^t.  The step t is *counter + 1 (read on the device, so
+// one captured step can be replayed); the step's energy goes to
+// energy_hist[*counter] and *counter is incremented.  One CTA.
+__global__ void __launch_bounds__(kGdThreads) adam_vqe_step_kernel(long long count, double *__restrict__ p,
+                                                                  const double *__restrict__ g,
+                                                                  double *__restrict__ m, double *__restrict__ v,
+                                                                  double lr, double beta1, double beta2,
+                                                                  double eps, const double *__restrict__ energy,
+                                                                  double *__restrict__ energy_hist, int *counter) {
+  const int k = *counter;
+  const double t = static_cast<double>(k + 1);
+  const double c1 = 1.0 - pow(beta1, t), c2s = sqrt(1.0 - pow(beta2, t));
+  const double step = lr / c1;
+  for (long long i = threadIdx.x; i < count; i += kGdThreads) {
+    const double gi = g[i];
+    const double mi = m[i] + (1.0 - beta1) * (gi - m[i]);
+    const double vi = v[i] * beta2 + (1.0 - beta2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= step * (mi / (sqrt(vi) / c2s + eps));
+  }
+  __syncthreads();  // every thread has read *counter
+  if (threadIdx.x == 0) {
+    if (energy_hist) energy_hist[k] = *energy;
+    *counter = k + 1;
+  }
+}
+
+cudaError_t adam_vqe_step(long long count, double *p, const double *g, double *m, double *v, double lr,
+                          double beta1, double beta2, double eps, const double *energy, double *energy_hist,
+                          int *counter, cudaStream_t s) {
+  adam_vqe_step_kernel<<<1, kGdThreads, 0, s>>>(count, p, g, m, v, lr, beta1, beta2, eps, energy, energy_hist,
+                                                counter);
+  return cudaGetLastError();
+}
+
 cudaError_t gd_step(long long count, double *p, const double *g, double stepsize, const double *energy,
                     double *energy_hist, double *gnorm_hist, int *counter, cudaStream_t s) {
   gd_step_kernel<<<1, kGdThreads, 0, s>>>(count, p, g, stepsize, energy, energy_hist, gnorm_hist, counter);

@@ -19,6 +19,9 @@ cudaError_t mlp_mse(long long count, const float *out, const float *target, floa
                     float *partials, float *loss, cudaStream_t s);
 cudaError_t gd_step(long long count, double *p, const double *g, double stepsize, const double *energy,
                     double *energy_hist, double *gnorm_hist, int *counter, cudaStream_t s);
+cudaError_t adam_vqe_step(long long count, double *p, const double *g, double *m, double *v, double lr,
+                          double beta1, double beta2, double eps, const double *energy, double *energy_hist,
+                          int *counter, cudaStream_t s);
 template <typename T>
 cudaError_t adam_step(long long count, T *p, const T *g, T *m, T *v, T lr, T beta1, T beta2, T eps,
                       int step, cudaStream_t s);

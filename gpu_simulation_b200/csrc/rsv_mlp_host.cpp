@@ -207,4 +207,18 @@ rsv_status rsv_gd_step_f64(double *d_params, const double *d_grad, size_t count,
   });
 }
 
+rsv_status rsv_adam_vqe_step_f64(double *d_params, const double *d_grad, double *d_m, double *d_v, size_t count,
+                                 double lr, double beta1, double beta2, double eps, const double *d_energy,
+                                 double *d_energy_hist, int *d_step_counter, void *stream) {
+  return mlp_guarded([&] {
+    if (!d_params || !d_grad || !d_m || !d_v || !d_energy || !d_step_counter) throw ArgError("null device pointer");
+    if (!std::isfinite(lr) || !(beta1 >= 0.0 && beta1 < 1.0) || !(beta2 >= 0.0 && beta2 < 1.0) ||
+        !std::isfinite(eps))
+      throw ArgError("Adam needs a finite lr and eps and betas in [0, 1)");
+    cuda_check(adam_vqe_step(static_cast<long long>(count), d_params, d_grad, d_m, d_v, lr, beta1, beta2, eps,
+                             d_energy, d_energy_hist, d_step_counter, static_cast<cudaStream_t>(stream)),
+               "adam step");
+  });
+}
+
 }  // extern "C"

@@ -129,6 +129,72 @@ def run_gradient_descent_device(engine: Engine, params, steps: int, stepsize: fl
     )
 
 
+def run_adam_device(engine: Engine, params, steps: int, lr: float = 0.05, betas=(0.9, 0.999),
+                    eps: float = 1e-8, use_graph: bool = True) -> dict:
+    """``steps`` Adam steps with the angles resident on the GPU, the update of
+    ``torch.optim.Adam`` (bias-corrected, no weight decay) applied by one fused
+    kernel (``rsv_adam_vqe_step_f64``): the same trajectory as a torch Adam loop
+    over the autograd Function, without the per-step Python and optimiser
+    launches.  With ``use_graph`` one (energy_and_grad, Adam) step is captured
+    into a CUDA graph and replayed.  Returns the final angles (flat), the
+    energy evaluated at the start of every step, and the GPU time of the loop.
+    """
+    import torch
+
+    if steps < 1:
+        raise ValueError("steps must be at least 1.")
+    lib = load_library()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    p = torch.as_tensor(np.asarray(params, dtype=np.float64).reshape(-1)).to(dev).contiguous()
+    if p.numel() != engine.num_params:
+        raise ValueError("num_params does not match the circuit.")
+    g = torch.empty_like(p)
+    m = torch.zeros_like(p)
+    v = torch.zeros_like(p)
+    e = torch.empty(1, dtype=torch.float64, device=dev)
+    e_hist = torch.empty(steps, dtype=torch.float64, device=dev)
+    counter = torch.zeros(1, dtype=torch.int32, device=dev)
+    b1, b2 = float(betas[0]), float(betas[1])
+
+    def step(stream):
+        engine.energy_and_grad_device(p, e, g, stream=stream)
+        check(lib.rsv_adam_vqe_step_f64(p.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr(), p.numel(),
+                                        float(lr), b1, b2, float(eps), e.data_ptr(), e_hist.data_ptr(),
+                                        counter.data_ptr(), stream.cuda_stream))
+
+    # one evaluation outside the timed loop configures every kernel once
+    engine.energy_and_grad_device(p, e, g)
+    torch.cuda.synchronize(dev)
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    graph = None
+    if use_graph:
+        graph = torch.cuda.CUDAGraph()
+        side = torch.cuda.Stream(device=dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.graph(graph, stream=side):
+            step(side)
+        # capture records the launches without running them
+        a.record()
+        for _ in range(steps):
+            graph.replay()
+        b.record()
+    else:
+        s = torch.cuda.current_stream(dev)
+        a.record()
+        for _ in range(steps):
+            step(s)
+        b.record()
+    b.synchronize()
+    gpu_ms = a.elapsed_time(b)
+    if int(counter.item()) != steps:
+        raise RuntimeError(f"step counter {int(counter.item())} != {steps}")
+    out = {"params": p.cpu().numpy(), "energies": e_hist.cpu().numpy(), "gpu_ms": gpu_ms,
+           "cuda_graph": bool(use_graph)}
+    del graph
+    return out
+
+
 def run_standalone(num_qubits: int, layers: int, steps: int, stepsize: float, field: float = 1.0,
                    seed: int = 7, init_scale: float = 0.3, use_graph: bool = True) -> TrainingRunResult:
     """The reference's standalone workflow on this engine: seeded initial angles,

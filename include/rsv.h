@@ -357,6 +357,21 @@ rsv_status rsv_gd_step_f64(double *d_params, const double *d_grad, size_t count,
                            const double *d_energy, double *d_energy_hist, double *d_gnorm_hist,
                            int *d_step_counter, void *stream);
 
+/*
+ * One Adam step of a device-resident VQE loop, with torch.optim.Adam's update
+ * (bias-corrected, no weight decay; d_m and d_v zero before the first step):
+ * the step number is *d_step_counter + 1, read on the device; the step's
+ * energy (*d_energy) is stored at index *d_step_counter of d_energy_hist (may be
+ * NULL), then *d_step_counter is incremented, so one captured
+ * (energy_and_grad, adam step) pair can be replayed as a CUDA graph.  The
+ * reference's loop applies a host-side gradient step
+ * (ring_ising/workflows/common.py:23-25); this is the torch Adam loop of a
+ * Python caller moved onto the device.
+ */
+rsv_status rsv_adam_vqe_step_f64(double *d_params, const double *d_grad, double *d_m, double *d_v, size_t count,
+                                 double lr, double beta1, double beta2, double eps, const double *d_energy,
+                                 double *d_energy_hist, int *d_step_counter, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -47,3 +47,29 @@ def test_graph_replay_equals_launches_and_host_loop():
     np.testing.assert_allclose(rg.final_params, p, atol=1e-12, rtol=0)
     np.testing.assert_allclose([m.energy for m in rg.step_metrics], energies, atol=1e-12, rtol=0)
     assert all(m.grad_norm > 0 for m in rg.step_metrics)
+
+
+@pytest.mark.parametrize("n,L,use_graph", [(12, 3, True), (12, 3, False), (14, 2, True)])
+def test_device_adam_matches_torch_adam(n, L, use_graph):
+    # the fused device Adam loop follows torch.optim.Adam over the autograd Function
+    import torch
+
+    from gpu_simulation_b200 import ring_ising_energy
+    from gpu_simulation_b200.training import run_adam_device
+
+    steps, lr = 20, 0.05
+    p0 = np.random.default_rng(7).uniform(0.0, 2.0 * np.pi, (L, n, 2))
+    eng = Engine(n, L, 1.0)
+    x = torch.tensor(p0, device="cuda", requires_grad=True)
+    opt = torch.optim.Adam([x], lr=lr)
+    energies = []
+    for _ in range(steps):
+        opt.zero_grad()
+        e = ring_ising_energy(x, eng)
+        e.backward()
+        opt.step()
+        energies.append(float(e.item()))
+    out = run_adam_device(eng, p0, steps, lr=lr, use_graph=use_graph)
+    np.testing.assert_allclose(out["energies"], energies, atol=1e-9, rtol=0)
+    np.testing.assert_allclose(out["params"], x.detach().cpu().numpy().reshape(-1), atol=1e-9, rtol=0)
+    assert out["energies"][-1] < out["energies"][0]
