@@ -1,8 +1,8 @@
 // Batched energy and gradient of many independent ring-Ising circuits in one
 // persistent kernel launch (uneven qubit counts and depths).
 //
-// The reference has no batched mode (it is only proposed in its design notes,
-// SURVEY 2.5); this kernel runs thousands of circuits per launch:
+// The reference has no batched mode (it is only proposed in its design
+// notes); this kernel runs thousands of circuits per launch:
 //   * one CTA (512 threads) per circuit at a time; CTAs take circuits from an
 //     atomic work counter over a list sorted by decreasing cost;
 //   * every circuit runs the same pass plan the single-circuit engine uses for

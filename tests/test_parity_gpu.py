@@ -11,7 +11,7 @@ from gpu_simulation_b200 import Engine
 
 pytestmark = pytest.mark.gpu
 
-TOL = 1e-10  # absolute, energy and gradient (BASELINE north star)
+TOL = 1e-10  # absolute, energy and gradient
 
 CASES = [
     (2, 1, 0.7), (2, 2, 1.0), (3, 1, 1.0), (3, 3, 1.1), (4, 2, 1.0), (5, 4, 0.3), (6, 2, 1.1),
