@@ -200,3 +200,16 @@ def test_initial_params_follow_the_reference_recipe():
     p = make_initial_params(8, 2, 7, 0.3)
     assert p.shape == (2, 8, 2) and p.dtype == np.float64
     np.testing.assert_array_equal(p, 0.3 * np.random.default_rng(7).standard_normal((2, 8, 2)))
+
+
+def test_device_optimiser_steps_reject_bad_arguments_before_any_launch():
+    # argument checks of the device-resident update steps run on the host
+    lib = _lib.load_library()
+    fake = ctypes.c_void_p(16)  # never dereferenced: every call below fails its checks first
+    assert lib.rsv_adam_vqe_step_f64(None, fake, fake, fake, 4, 0.05, 0.9, 0.999, 1e-8, fake, None, fake,
+                                     None) == _lib.RSV_ERR_INVALID_ARGUMENT
+    assert lib.rsv_adam_vqe_step_f64(fake, fake, fake, fake, 4, float("nan"), 0.9, 0.999, 1e-8, fake, None,
+                                     fake, None) == _lib.RSV_ERR_INVALID_ARGUMENT
+    assert lib.rsv_adam_vqe_step_f64(fake, fake, fake, fake, 4, 0.05, 1.0, 0.999, 1e-8, fake, None, fake,
+                                     None) == _lib.RSV_ERR_INVALID_ARGUMENT
+    assert lib.rsv_gd_step_f64(fake, None, 4, 0.1, fake, None, None, fake, None) == _lib.RSV_ERR_INVALID_ARGUMENT
