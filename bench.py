@@ -402,6 +402,7 @@ def device_time(eng, n, L, field, steps, warmup, seed, timing=False):
     torch.cuda.synchronize()
     if timing:
         eng.set_launch_timing(True)
+    k0 = eng.kernel_launches()
     s, t = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     s.record()
     for _ in range(steps):
@@ -412,6 +413,7 @@ def device_time(eng, n, L, field, steps, warmup, seed, timing=False):
     if timing:
         eng.set_launch_timing(False)
         stats = eng.launch_stats()
+        stats["kernels_launched"] = eng.kernel_launches() - k0
     return s.elapsed_time(t) / steps, stats, float(e.item())
 
 
@@ -478,6 +480,7 @@ def main():
         "backward_pass": "backward (bwd_pass_kernel 12-bit tiles, bwd_half_kernel 11-bit tiles, mps_grad_kernel)",
         "forward_pass": "fwd_pass_kernel + mps_fwd_kernel", "energy": "energy_tile_kernel + energy_kernel",
     }
+    kernels_launched = int(stats.pop("kernels_launched"))
     kinds = {k: v for k, v in stats.items() if v["launches"]}
     dom = max(kinds, key=lambda k: kinds[k]["ms"])
     d = kinds[dom]
@@ -518,7 +521,7 @@ def main():
             / (ms_max * 1e-3) / 1e9 / peak,
         },
         "kernels": kinds,
-        "gpu_launches": int(sum(v["launches"] for v in kinds.values())),
+        "gpu_launches": kernels_launched,
         "e2e": {"value": world * 1000.0 / e2e_ms, "unit": UNIT, "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": n * L * 32, "d2h_bytes_per_step": (1 + 2 * n * L) * 8},
         "clocks": clocks,
@@ -531,6 +534,7 @@ def main():
             try:
                 e2 = Engine(ns, L, h)
                 ms_s, st_s, _ = device_time(e2, ns, L, h, max(3, args.steps // 2), 2, seed=7, timing=True)
+                st_s.pop("kernels_launched")
                 byt = sum(v["bytes"] for v in st_s.values())
                 tms = sum(v["ms"] for v in st_s.values())
                 sweep[f"n={ns}"] = {"ms_per_call": ms_s, "energy_and_grad_per_s": 1000.0 / ms_s,

@@ -42,6 +42,7 @@ _SIGNATURES = {
                                      ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
                                     ctypes.c_int),
     "rsv_set_launch_timing": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "rsv_kernel_launches": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "rsv_launch_stats": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
                          ctypes.c_int),
     "rsv_set_field": ([ctypes.c_void_p, ctypes.c_double], ctypes.c_int),

@@ -829,6 +829,8 @@ struct rsv_backend {
   // call records its value so that a deferred backward can check it.
   unsigned long long generation = 0;
   bool forward_only_state = false;
+  // kernels launched by this backend's calls (rsv_kernel_launches)
+  unsigned long long kernels_launched = 0;
   // launch timing (rsv_set_launch_timing)
   bool timing = false;
   struct Rec {
@@ -947,9 +949,11 @@ cudaEvent_t take_event(rsv_backend *B) {
   return e;
 }
 
-// Launch `body` and, when launch timing is on, bracket it with events.
+// Launch `body` (`kernels` kernel launches) and, when launch timing is on,
+// bracket it with events.
 template <typename F>
-void timed(rsv_backend *B, cudaStream_t st, int kind, double bytes, F &&body) {
+void timed(rsv_backend *B, cudaStream_t st, int kind, double bytes, F &&body, int kernels = 1) {
+  B->kernels_launched += static_cast<unsigned long long>(kernels);
   if (!B->timing) {
     body();
     return;
@@ -1001,14 +1005,14 @@ MpsParams mps_params(rsv_backend *B) {
 void run_forward(rsv_backend *B, cudaStream_t st) {
   if (B->plan.mps_k > 0 && B->plan.mps_fused) {
     const MpsParams Q = mps_params(B);
-    timed(B, st, 0, 0.0, [&] { check(launch_mps_tables(Q, st), "matrix-product tables launch"); });
+    timed(B, st, 0, 0.0, [&] { check(launch_mps_tables(Q, st), "matrix-product tables launch"); }, 2);
   } else if (B->plan.mps_k > 0) {
     const MpsParams Q = mps_params(B);
     timed(B, st, 1, 16.0 * static_cast<double>(u64{1} << B->n), [&] {
       check(launch_mps_tables(Q, st), "matrix-product tables launch");
       check(launch_mps_forward(Q, state_buf(B, B->plan.mps_out), B->plan.mps_scatter ? 1 : 0, B->plan.mps_fwd_grid, st),
             "matrix-product forward launch");
-    });
+    }, 3);
   }
   PassParams P;
   for (const auto &s : B->plan.fwd) {
@@ -1024,7 +1028,7 @@ void run_energy(rsv_backend *B, cudaStream_t st) {
     check(launch_energy(state_buf(B, B->plan.chi_buf), state_buf(B, B->plan.mu_buf), B->n, B->field,
                         u64{1} << B->n, B->energy_partials.p, B->energy_grid, B->sms, st),
           "energy launch");
-  });
+  }, energy_kernel_count(B->n));
 }
 
 Layer0Params layer0_params(rsv_backend *B) {
@@ -1056,7 +1060,7 @@ void run_backward(rsv_backend *B, cudaStream_t st) {
       check(launch_mps_grad(Q, state_buf(B, B->plan.mps_lam), B->plan.mps_load == kLoadGatherP ? 1 : 0,
                             B->plan.mps_grad_grid, st),
             "matrix-product gradient launch");
-    });
+    }, 3);
   }
 }
 
@@ -1842,6 +1846,14 @@ rsv_status rsv_set_launch_timing(rsv_backend *B, int enable) {
   return guarded([&] {
     if (B == nullptr) invalid("backend is null");
     B->timing = enable != 0;
+  });
+}
+
+rsv_status rsv_kernel_launches(rsv_backend *B, unsigned long long *count_out) {
+  return guarded([&] {
+    if (B == nullptr) invalid("backend is null");
+    if (count_out == nullptr) invalid("output pointer is null");
+    *count_out = B->kernels_launched;
   });
 }
 

@@ -391,6 +391,8 @@ cudaError_t launch_energy(const double2 *chi, double2 *mu, int n, double field, 
   return launch_energy_k<1>(count, grid, s, chi, mu, n, field, size, M, 1, partials);
 }
 
+int energy_kernel_count(int n) { return n < kEnergySplitQubits ? 1 : 2; }
+
 cudaError_t launch_finalize(const FinalizeParams &F, cudaStream_t s) {
   finalize_kernel<<<1, 256, 0, s>>>(F);
   return cudaGetLastError();

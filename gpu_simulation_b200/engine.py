@@ -120,6 +120,12 @@ class Engine:
         return {name: {"launches": int(counts[i]), "ms": float(ms[i]), "bytes": float(by[i])}
                 for i, name in enumerate(self.KINDS)}
 
+    def kernel_launches(self) -> int:
+        """Kernels launched by this engine's calls since it was created."""
+        out = ctypes.c_ulonglong()
+        check(self._lib.rsv_kernel_launches(self._h, ctypes.byref(out)))
+        return int(out.value)
+
     BACKWARD_MODES = {"auto": 0, "uncompute": 1, "checkpoint": 2}
 
     def set_backward_mode(self, mode: str) -> None:

@@ -175,6 +175,13 @@ rsv_status rsv_energy_and_grad_noalloc(int num_qubits, int num_layers, double fi
  * No reference counterpart.
  */
 #define RSV_NUM_KINDS 5
+
+/*
+ * Number of kernels the backend's calls have launched since it was created
+ * (every kernel of every call, with or without launch timing).
+ * No reference counterpart.
+ */
+rsv_status rsv_kernel_launches(rsv_backend *backend, unsigned long long *count_out);
 rsv_status rsv_set_launch_timing(rsv_backend *backend, int enable);
 rsv_status rsv_launch_stats(rsv_backend *backend, int *counts, double *total_ms,
                             double *total_bytes);
