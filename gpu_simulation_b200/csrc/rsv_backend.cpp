@@ -1426,8 +1426,7 @@ rsv_status run_in_workspace(int n, int L, double field, const double *d_params, 
     B.plan = make_plan_full(n, L, B.sms, false);
     B.num_bwd_passes = static_cast<int>(B.plan.bwd.size());
     B.state_len = size_t{1} << B.plan.phys;
-    B.energy_grid = static_cast<int>(std::min<u64>(std::max<u64>(1, (u64{1} << n) / 256),
-                                                   static_cast<u64>(B.sms) * 8));
+    B.energy_grid = energy_grid_size(n, B.sms);
     const size_t nl = static_cast<size_t>(n) * L;
     std::vector<int> tab;
     for (const auto &s : B.plan.bwd) tab.push_back(s.grid);
@@ -1642,8 +1641,7 @@ rsv_status rsv_create(int num_qubits, int num_layers, double field, const char *
     }
     B->coef.alloc(nl);
     B->ptab.alloc(static_cast<size_t>(num_layers) * 1024);
-    B->energy_grid = static_cast<int>(std::min<u64>(
-        std::max<u64>(1, (u64{1} << num_qubits) / 256), static_cast<u64>(B->sms) * 8));
+    B->energy_grid = energy_grid_size(num_qubits, B->sms);
     B->energy_partials.alloc(B->energy_grid);
     B->outputs.alloc(1 + B->num_params);
     B->rot.alloc(nl);

@@ -162,6 +162,10 @@ __global__ void rot_kernel(const double4 *__restrict__ coef, int n, int L, const
 // are near enough to come from L1/L2, and forms the energy.
 // ------------------------------------------------------------------------
 constexpr int kEnergyThreads = 256;
+// The split energy's grid-stride part runs 1024-thread CTAs (two per SM): a CTA
+// covers 1024 consecutive amplitudes per step, so the partners of the masks on
+// index bits up to 9 are ones the CTA has just read (L1), not L2 requests.
+constexpr int kEnergySplitThreads = 1024;
 constexpr int kEnergySplitQubits = 21;
 constexpr int kEnergyHighBits = 9;
 constexpr int kEnergyTileThreads = 256;
@@ -179,16 +183,16 @@ struct EnergyMasks {
 // diagonal included) when given, else the diagonal.  K is a template
 // parameter so that all K partner loads of an amplitude are issued before
 // the first is used.
-template <int K>
-__global__ void __launch_bounds__(kEnergyThreads) energy_kernel(const double2 *__restrict__ chi,
+template <int K, int THREADS>
+__global__ void __launch_bounds__(THREADS) energy_kernel(const double2 *__restrict__ chi,
                                                                  double2 *__restrict__ mu, int n,
                                                                  double field, u64 size,
                                                                  const EnergyMasks M, int with_mu_in,
                                                                  double *__restrict__ partials) {
-  __shared__ double red[kEnergyThreads / 32];
+  __shared__ double red[THREADS / 32];
   double e = 0.0;
-  const u64 stride = static_cast<u64>(gridDim.x) * kEnergyThreads;
-  for (u64 i = static_cast<u64>(blockIdx.x) * kEnergyThreads + threadIdx.x; i < size; i += stride) {
+  const u64 stride = static_cast<u64>(gridDim.x) * THREADS;
+  for (u64 i = static_cast<u64>(blockIdx.x) * THREADS + threadIdx.x; i < size; i += stride) {
     const double2 c = chi[i];
     double2 x = make_double2(0.0, 0.0);
 #pragma unroll
@@ -213,7 +217,7 @@ __global__ void __launch_bounds__(kEnergyThreads) energy_kernel(const double2 *_
   __syncthreads();
   if (threadIdx.x == 0) {
     double s = 0.0;
-    for (int i = 0; i < kEnergyThreads / 32; ++i) s += red[i];
+    for (int i = 0; i < THREADS / 32; ++i) s += red[i];
     partials[blockIdx.x] = s;
   }
 }
@@ -222,7 +226,11 @@ template <int K>
 cudaError_t launch_energy_k(int count, int grid, cudaStream_t s, const double2 *chi, double2 *mu, int n,
                             double field, u64 size, const EnergyMasks &M, int with_mu_in, double *partials) {
   if (count == K) {
-    energy_kernel<K><<<grid, kEnergyThreads, 0, s>>>(chi, mu, n, field, size, M, with_mu_in, partials);
+    if (with_mu_in)
+      energy_kernel<K, kEnergySplitThreads><<<grid, kEnergySplitThreads, 0, s>>>(chi, mu, n, field, size, M, 1,
+                                                                                 partials);
+    else
+      energy_kernel<K, kEnergyThreads><<<grid, kEnergyThreads, 0, s>>>(chi, mu, n, field, size, M, 0, partials);
     return cudaGetLastError();
   }
   if constexpr (K < kMaxQubits) {
@@ -392,6 +400,13 @@ cudaError_t launch_energy(const double2 *chi, double2 *mu, int n, double field, 
 }
 
 int energy_kernel_count(int n) { return n < kEnergySplitQubits ? 1 : 2; }
+
+int energy_grid_size(int n, int sms) {
+  const u64 size = u64{1} << n;
+  if (n >= kEnergySplitQubits)
+    return static_cast<int>(std::min<u64>(std::max<u64>(1, size / kEnergySplitThreads), static_cast<u64>(sms) * 2));
+  return static_cast<int>(std::min<u64>(std::max<u64>(1, size / kEnergyThreads), static_cast<u64>(sms) * 8));
+}
 
 cudaError_t launch_finalize(const FinalizeParams &F, cudaStream_t s) {
   finalize_kernel<<<1, 256, 0, s>>>(F);

@@ -25,6 +25,8 @@ cudaError_t launch_energy(const double2 *chi, double2 *mu, int n, double field,
                           unsigned long long size, double *partials, int grid, int sms, cudaStream_t s);
 // kernels launch_energy launches for n qubits (1, or 2 for the split energy)
 int energy_kernel_count(int n);
+// CTAs of the energy's grid-stride kernel (= its number of partials)
+int energy_grid_size(int n, int sms);
 cudaError_t launch_finalize(const FinalizeParams &F, cudaStream_t s);
 // layer-0 gradients in one read of lambda (n >= 13), and their final reduction
 // into grad_out[0 .. 2n)
