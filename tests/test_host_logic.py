@@ -213,3 +213,9 @@ def test_device_optimiser_steps_reject_bad_arguments_before_any_launch():
     assert lib.rsv_adam_vqe_step_f64(fake, fake, fake, fake, 4, 0.05, 1.0, 0.999, 1e-8, fake, None, fake,
                                      None) == _lib.RSV_ERR_INVALID_ARGUMENT
     assert lib.rsv_gd_step_f64(fake, None, 4, 0.1, fake, None, None, fake, None) == _lib.RSV_ERR_INVALID_ARGUMENT
+
+
+def test_kernel_launch_counter_rejects_null_arguments():
+    lib = _lib.load_library()
+    out = ctypes.c_ulonglong()
+    assert lib.rsv_kernel_launches(None, ctypes.byref(out)) == _lib.RSV_ERR_INVALID_ARGUMENT
