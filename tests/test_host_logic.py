@@ -219,3 +219,13 @@ def test_kernel_launch_counter_rejects_null_arguments():
     lib = _lib.load_library()
     out = ctypes.c_ulonglong()
     assert lib.rsv_kernel_launches(None, ctypes.byref(out)) == _lib.RSV_ERR_INVALID_ARGUMENT
+
+
+def test_plan_invariants_over_every_size():
+    # every wire once, compact buffer ids, the fused bond-4 source and no psi
+    # store below the matrix-product layers, for all multi-tile sizes
+    for n in range(13, 32):
+        for L in range(1, 7):
+            for mode in (plan_sim.AUTO, plan_sim.UNCOMPUTE, plan_sim.CHECKPOINT):
+                plan = plan_sim.parse_plan(plan_sim.describe_plan(n, L, mode))
+                check_large_plan(plan, n, L)
