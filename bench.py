@@ -15,9 +15,12 @@ through the public host API (host parameters in, host energy+gradient out,
 copies inside the timed region).  ``--impl reference`` times the CPU
 reference arm: the reference has no CPU implementation of this path, so the
 arm runs the repository's CPU restatement of it (oracle/, OpenMP, every host
-thread) on a bounded sample of the same workload.  With --gpus N > 1 (under
-torchrun) every rank evaluates its own independent circuit (replicas, weak
-scaling; the path has no exchange step).
+thread), one full energy_and_grad of the same n=28, L=4 circuit per step.
+Beside it the arm records the reference's own CUDA code, rebuilt for sm_100a
+from its sources (oracle/_ref), timed on the same GPU at n=28 and n=30, L=4
+(``reference_gpu``).  With --gpus N > 1 (under torchrun) every rank evaluates
+its own independent circuit (replicas, weak scaling; the path has no exchange
+step).
 
 Two further sections ride on the same JSON line: ``batch`` -- 4096 circuits
 of uneven size per step through the persistent batched kernel (one CUDA
@@ -66,6 +69,8 @@ def parse_args():
     ap.add_argument("--no-batch", action="store_true", help="skip the 4096-circuit batched section")
     ap.add_argument("--no-warmstart", action="store_true", help="skip the warm-start section")
     ap.add_argument("--no-small", action="store_true", help="skip the n=12 Adam and n=20 autograd sections")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="reference arm: skip timing the reference's sm_100a rebuild on the GPU")
     return ap.parse_args()
 
 
@@ -133,22 +138,52 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------- CPU baselines
-def cpu_sample(n, L, field, repeats=1):
-    """Time the oracle (CPU restatement, all host threads) on a bounded sample
-    of the workload: n_s = min(n, 24) qubits, same L; returns seconds/call at
-    n_s and the scale factor 2^(n - n_s) to the full workload."""
+def cpu_call(n, L, field, seed=7):
+    """One full energy_and_grad of the workload on the oracle (the CPU
+    restatement, every host thread); returns (seconds, threads, energy)."""
     import oracle
 
     threads = oracle.set_num_threads(0)
-    n_s = min(n, 24)
-    p = workload_params(n_s, L, 7)
-    oracle.energy_and_grad(n_s, L, field, p)  # warm (page faults, thread pool)
-    times = []
-    for _ in range(repeats):
-        t0 = time.perf_counter()
-        oracle.energy_and_grad(n_s, L, field, p)
-        times.append(time.perf_counter() - t0)
-    return min(times), float(2 ** (n - n_s)), threads, n_s
+    p = workload_params(n, L, seed)
+    t0 = time.perf_counter()
+    e, _ = oracle.energy_and_grad(n, L, field, p)
+    return time.perf_counter() - t0, threads, float(e)
+
+
+def reference_gpu_times(L, field, sizes=(28, 30), warmup=2, reps=5):
+    """The reference's own structured_adjoint CUDA code (its extension rebuilt
+    for sm_100a from its sources into oracle/_ref), timed on this GPU through
+    its public call energy_and_grad(params, True, False): host parameters in,
+    energy and gradient out, synchronous, so a wall-clock interval per call is
+    its end-to-end time.  Seed-7 angles as the workload."""
+    from tests.refmod import load_reference_module
+
+    ref = load_reference_module()
+    if ref is None:
+        return {"unavailable": "oracle/_ref was not built (make -C oracle ref)"}
+    import gc
+
+    out = {"what": "reference cpp/*.cu rebuilt for sm_100a (structured_adjoint, chunk width 8), "
+                   "same GPU, median ms per energy_and_grad call (host params in, host results out)"}
+    for n in sizes:
+        p = workload_params(n, L, 7)
+        try:
+            rb = ref.RingIsingCudaBackend(n, L, field, "structured_adjoint", 8, False)
+            for _ in range(warmup):
+                r = rb.energy_and_grad(p, True, False)
+            times = []
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                r = rb.energy_and_grad(p, True, False)
+                times.append(time.perf_counter() - t0)
+            ms = statistics.median(times) * 1e3
+            out[f"n={n}"] = {"ms_per_call": ms, "energy_and_grad_per_s": 1000.0 / ms,
+                             "energy": float(r["energy"]), "calls_timed": reps}
+            del rb, r
+            gc.collect()
+        except Exception as exc:  # report, do not hide
+            out[f"n={n}"] = {"error": str(exc)}
+    return out
 
 
 def run_reference_arm(args, rank, world):
@@ -156,14 +191,15 @@ def run_reference_arm(args, rank, world):
         return 0
     n, L = args.qubits, args.layers
     per_step = []
+    energy = None
     for i in range(args.warmup + args.steps):
-        t, scale, threads, n_s = cpu_sample(n, L, args.field)
+        t, threads, energy = cpu_call(n, L, args.field)
         if i >= args.warmup:
-            per_step.append(t * scale)
+            per_step.append(t)
     sec = statistics.median(per_step)
     value = 1.0 / sec
-    sample = (f"one energy_and_grad at n={n_s}, L={L} per step, scaled by 2^{n - n_s} to n={n} "
-              "(the CPU restatement is memory-bound and linear in 2^n)")
+    sample = (f"the full workload: one energy_and_grad at n={n}, L={L} per step on the CPU restatement "
+              f"(oracle/, {threads} threads); median of {args.steps} steps after {args.warmup} warm-up steps")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
@@ -173,9 +209,51 @@ def run_reference_arm(args, rank, world):
                    "num_qubits": n, "num_layers": L, "field": args.field, "parallelism": "replicas"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "energy": energy,
     }
+    if not args.no_reference_gpu:
+        line["reference_gpu"] = reference_gpu_times(L, args.field)
     print(json.dumps(line), flush=True)
     return 0
+
+
+def pennylane_baseline():
+    """PennyLane lightning.qubit with adjoint differentiation on the host
+    cores, the reported CPU baseline for the n=12, L=3 circuit, when PennyLane
+    is installed; otherwise the reason it is not measured."""
+    try:
+        import pennylane as qml  # noqa: F401
+    except Exception as exc:
+        return {"unavailable": f"pennylane is not installed on this box ({type(exc).__name__}: {exc}); "
+                               "the image has no network to install it"}
+    n, L = 12, 3
+    dev = qml.device("lightning.qubit", wires=n)
+    ham = qml.Hamiltonian([-1.0] * n + [-1.0] * n,
+                          [qml.PauliZ(i) @ qml.PauliZ((i + 1) % n) for i in range(n)]
+                          + [qml.PauliX(i) for i in range(n)])
+
+    @qml.qnode(dev, diff_method="adjoint")
+    def circuit(x):
+        for layer in range(L):
+            for w in range(n):
+                qml.RY(x[layer, w, 0], wires=w)
+                qml.RZ(x[layer, w, 1], wires=w)
+            for w in range(n):
+                qml.CNOT(wires=[w, (w + 1) % n])
+        return qml.expval(ham)
+
+    from pennylane import numpy as pnp
+
+    x = pnp.array(workload_params(n, L, 7).reshape(L, n, 2), requires_grad=True)
+    grad = qml.grad(circuit)
+    grad(x)
+    t0 = time.perf_counter()
+    reps = 5
+    for _ in range(reps):
+        grad(x)
+    sec = (time.perf_counter() - t0) / reps
+    return {"value": 1.0 / sec, "unit": "energy_and_grad/s", "cores": os.cpu_count(),
+            "workload": f"n={n} L={L} h=1, lightning.qubit adjoint, seed 7"}
 
 
 # ------------------------------------------------------- batched circuits
@@ -516,9 +594,6 @@ def main():
         "whole_call": {
             "algorithmic_bytes": whole_bytes, "achieved_gbs": whole_bytes / (total_ms * 1e-3) / 1e9,
             "frac_of_peak": whole_bytes / (total_ms * 1e-3) / 1e9 / peak,
-            "survey_formula_bytes": 16.0 * 2 ** n * (115 if (n + 7) // 8 == 4 else 93),
-            "survey_formula_frac": 16.0 * 2 ** n * (115 if (n + 7) // 8 == 4 else 93)
-            / (ms_max * 1e-3) / 1e9 / peak,
         },
         "kernels": kinds,
         "gpu_launches": kernels_launched,
@@ -557,12 +632,14 @@ def main():
         eng.set_analytic_layers(info["max_layers"])
         line["analytic_layers"] = alt
     if world == 1 and rank == 0 and not args.no_cpu:
-        t, scale, threads, n_s = cpu_sample(n, L, h)
+        t, threads, e_cpu = cpu_call(n, L, h)
         line["cpu_baseline"] = {
-            "value": 1.0 / (t * scale), "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"one energy_and_grad at n={n_s}, L={L} on the CPU restatement (oracle/), "
-                      f"{t:.2f} s, scaled by 2^{n - n_s} to n={n}",
+            "value": 1.0 / t, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"one full energy_and_grad at n={n}, L={L} (the workload itself) on the CPU "
+                      f"restatement (oracle/), {t:.2f} s, energy {e_cpu:.12f}",
         }
+    if world == 1 and rank == 0:
+        line["pennylane_lightning_qubit"] = pennylane_baseline()
     eng.close()
     if not args.no_batch:
         line["batch"] = batch_section(args, rank, world, dist, barrier, max_over_ranks)

@@ -15,6 +15,7 @@ LIB_PATH = _PKG / "librsv.so"
 
 RSV_OK = 0
 RSV_ERR_INVALID_ARGUMENT = 1
+RSV_ERR_STALE_STATE = 6
 
 # Every function declared in include/rsv.h, with its ctypes signature.
 _c_double_p = ctypes.POINTER(ctypes.c_double)

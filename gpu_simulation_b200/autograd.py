@@ -16,7 +16,7 @@ import ctypes
 
 import torch
 
-from ._lib import check
+from ._lib import RSV_ERR_STALE_STATE, check
 from .engine import Engine
 
 
@@ -47,10 +47,12 @@ class RingIsingEnergy(torch.autograd.Function):
         stream = torch.cuda.current_stream(flat.device)
         status = engine._lib.rsv_backward_device(engine._h, ctx.generation, grad.data_ptr(),
                                                  stream.cuda_stream)
-        if status != 0:
+        if status == RSV_ERR_STALE_STATE:
             # the engine's buffers were reused by another call: recompute
             scratch = torch.empty(1, dtype=torch.float64, device=flat.device)
             engine.energy_and_grad_device(flat, scratch, grad, stream)
+        else:
+            check(status)  # any other failure is raised, never retried
         return (grad * grad_output).reshape(ctx.shape), None
 
 

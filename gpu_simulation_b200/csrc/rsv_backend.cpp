@@ -1472,18 +1472,16 @@ rsv_status run_in_workspace(int n, int L, double field, const double *d_params, 
     B.tables.view(reinterpret_cast<int *>(tabs), tab.size());
     B.order.view(reinterpret_cast<int *>(ords), ord.size());
     B.outputs.view(reinterpret_cast<double *>(outs), 1 + num_params);
-    check(cudaMemcpyAsync(B.tables.p, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice, st),
-          "plan table upload");
-    check(cudaMemcpyAsync(B.order.p, ord.data(), ord.size() * sizeof(int), cudaMemcpyHostToDevice, st),
-          "order upload");
+    // the plan tables travel in kernel parameters (no pageable host copy)
+    check(launch_put_ints(tab.data(), tab.size(), B.tables.p, st), "plan table upload");
+    check(launch_put_ints(ord.data(), ord.size(), B.order.p, st), "order upload");
     // The workspace keeps the previous call's contents; for n < 12 the padding
     // amplitudes of the state buffers must start at zero.
     if (B.plan.phys > n)
       check(cudaMemsetAsync(B.states.p, 0, 3 * B.state_len * sizeof(double2), st), "state clear");
     check(launch_coef(d_params, B.coef.p, static_cast<int>(nl), st), "coef launch");
     run_all(&B, d_gradient_out != nullptr, d_energy_out, d_gradient_out, st);
-    // the host vectors above are consumed by the time cudaMemcpyAsync from
-    // pageable memory returns; nothing else outlives this call
+    // nothing enqueued above refers to host memory of this call
   });
 }
 
@@ -1722,7 +1720,8 @@ rsv_status rsv_backward_device(rsv_backend *B, unsigned long long generation,
     if (B == nullptr) invalid("backend is null");
     if (d_gradient_out == nullptr) invalid("d_gradient_out is null");
     if (!B->forward_only_state || generation != B->generation)
-      invalid("backward needs the state of the matching forward; the backend ran another call since");
+      throw Error(RSV_ERR_STALE_STATE,
+                  "backward needs the state of the matching forward; the backend ran another call since");
     cudaStream_t st = device_stream(stream);
     run_backward(B, st);
     // energy is rewritten with the same value into the outputs scratch slot

@@ -4,6 +4,7 @@
 #include <algorithm>
 
 #include "rsv_device.cuh"
+#include "rsv_launch.h"
 #include "rsv_types.h"
 
 namespace rsv {
@@ -343,6 +344,32 @@ __global__ void finalize_kernel(const FinalizeParams F) {
 // Launchers (host side, same translation unit)
 // ------------------------------------------------------------------------
 
+// Small host tables written to device memory by kernels whose parameters carry
+// the values: no copy from pageable host memory, nothing refers to host memory
+// after the launch returns.
+namespace {
+constexpr int kParamInts = 960;  // 3.8 KB of kernel parameters per launch
+struct IntChunk {
+  int count;
+  int v[kParamInts];
+};
+__global__ void put_ints_kernel(const IntChunk c, int *dst) {
+  for (int i = threadIdx.x; i < c.count; i += blockDim.x) dst[i] = c.v[i];
+}
+}  // namespace
+
+cudaError_t launch_put_ints(const int *src, size_t count, int *dst, cudaStream_t s) {
+  for (size_t off = 0; off < count; off += kParamInts) {
+    IntChunk c;
+    c.count = static_cast<int>(std::min<size_t>(kParamInts, count - off));
+    for (int i = 0; i < c.count; ++i) c.v[i] = src[off + i];
+    put_ints_kernel<<<1, 256, 0, s>>>(c, dst + off);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t launch_coef(const double *params, double4 *coef, int count, cudaStream_t s) {
   coef_kernel<<<(count + 127) / 128, 128, 0, s>>>(params, coef, count);
   return cudaGetLastError();
@@ -385,12 +412,10 @@ cudaError_t launch_energy(const double2 *chi, double2 *mu, int n, double field, 
     }
   }
   if (T.num_masks != kEnergyTileMasks) return cudaErrorInvalidValue;
-  static bool configured = false;
-  if (!configured) {
-    const cudaError_t e = cudaFuncSetAttribute(energy_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               static_cast<int>(kEnergyTileSmem));
+  static std::atomic<unsigned long long> configured{0};
+  {
+    const cudaError_t e = set_smem_limit_once(energy_tile_kernel, kEnergyTileSmem, configured);
     if (e != cudaSuccess) return e;
-    configured = true;
   }
   const int tgrid = static_cast<int>(std::min<u64>(T.num_tiles, static_cast<u64>(std::max(1, sms)) * 3));
   energy_tile_kernel<<<tgrid, kEnergyTileThreads, kEnergyTileSmem, s>>>(chi, mu, T);

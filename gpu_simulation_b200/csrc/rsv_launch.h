@@ -1,6 +1,7 @@
 // Host-callable launchers of the kernels in rsv_kernels.cu.
 #pragma once
 
+#include <atomic>
 #include <cstddef>
 #include <cuda_runtime.h>
 
@@ -8,7 +9,26 @@
 
 namespace rsv {
 
+// Raises kernel k's dynamic shared-memory limit to `bytes` on the current
+// device, once per device: the attribute belongs to the device, so a process
+// that uses several GPUs sets it on each.  `done` holds one bit per device
+// ordinal (ordinals >= 64 set the attribute on every call).  Safe to call from
+// several host threads.
+template <typename K>
+inline cudaError_t set_smem_limit_once(K k, size_t bytes, std::atomic<unsigned long long> &done) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = dev < 64 ? (1ull << dev) : 0ull;
+  if (bit != 0 && (done.load(std::memory_order_acquire) & bit) != 0) return cudaSuccess;
+  e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+  if (e == cudaSuccess && bit != 0) done.fetch_or(bit, std::memory_order_acq_rel);
+  return e;
+}
+
 cudaError_t launch_coef(const double *params, double4 *coef, int count, cudaStream_t s);
+// dst[0 .. count) = src[0 .. count) through kernel parameters (small tables)
+cudaError_t launch_put_ints(const int *src, size_t count, int *dst, cudaStream_t s);
 // prod holds 1 + partial.count tables of [4][256]
 cudaError_t launch_tables(const double4 *coef, int n, int L, double2 *ptab, double2 *prod,
                           const PartialMasks &partial, cudaStream_t s);

@@ -631,12 +631,10 @@ __global__ void __launch_bounds__(64) mps_finalize_kernel(const MpsParams Q, dou
 
 template <int D>
 cudaError_t launch_grad_d(const MpsParams &Q, const double2 *lam, int gather, int grid, cudaStream_t s) {
-  static bool configured = false;
-  if (!configured) {
-    const cudaError_t e = cudaFuncSetAttribute(mps_grad_kernel<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               static_cast<int>(mps_grad_smem<D>()));
+  static std::atomic<unsigned long long> configured{0};
+  {
+    const cudaError_t e = set_smem_limit_once(mps_grad_kernel<D>, mps_grad_smem<D>(), configured);
     if (e != cudaSuccess) return e;
-    configured = true;
   }
   mps_grad_kernel<D><<<grid, kMpsThreads, mps_grad_smem<D>(), s>>>(Q, lam, gather);
   cudaError_t e = cudaGetLastError();

@@ -448,12 +448,10 @@ __global__ void __launch_bounds__(kThreads, 2) fwd_pass_kernel(const PassParams 
 template <int PSRC, int LSRC, int PDST, int LDST, bool PHASE>
 cudaError_t launch_bwd(const PassParams &P, int grid, cudaStream_t s) {
   auto k = bwd_pass_kernel<PSRC, LSRC, PDST, LDST, PHASE>;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(kBwdSmem));
+  static std::atomic<unsigned long long> configured{0};
+  {
+    const cudaError_t e = set_smem_limit_once(k, kBwdSmem, configured);
     if (e != cudaSuccess) return e;
-    configured = true;
   }
   k<<<grid, bw::kT, kBwdSmem, s>>>(P);
   return cudaGetLastError();
@@ -463,11 +461,10 @@ template <int PSRC, int PDST, bool PHASE>
 cudaError_t launch_fwd(const PassParams &P, int grid, cudaStream_t s) {
   auto k = fwd_pass_kernel<PSRC, PDST, PHASE>;
   constexpr size_t smem = PSRC == kLoadMpsP ? kFwdMpsSmem : kFwdSmem;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  static std::atomic<unsigned long long> configured{0};
+  {
+    const cudaError_t e = set_smem_limit_once(k, smem, configured);
     if (e != cudaSuccess) return e;
-    configured = true;
   }
   k<<<grid, kThreads, smem, s>>>(P);
   return cudaGetLastError();

@@ -320,12 +320,10 @@ __global__ void __launch_bounds__(hw::kT, 2) bwd_half_kernel(const PassParams P)
 template <int PSRC, int LSRC, int PDST, int LDST, bool PHASE>
 cudaError_t launch_half(const PassParams &P, int grid, cudaStream_t s) {
   auto k = bwd_half_kernel<PSRC, LSRC, PDST, LDST, PHASE>;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(kHalfSmem));
+  static std::atomic<unsigned long long> configured{0};
+  {
+    const cudaError_t e = set_smem_limit_once(k, kHalfSmem, configured);
     if (e != cudaSuccess) return e;
-    configured = true;
   }
   k<<<grid, hw::kT, kHalfSmem, s>>>(P);
   return cudaGetLastError();

@@ -37,7 +37,11 @@ typedef enum rsv_status {
   RSV_ERR_CUDA = 2,
   RSV_ERR_OUT_OF_MEMORY = 3,
   RSV_ERR_UNSUPPORTED = 4,
-  RSV_ERR_INTERNAL = 5
+  RSV_ERR_INTERNAL = 5,
+  /* rsv_backward_device only: the backend ran another call after the
+   * forward whose generation was passed, so that forward's state is gone
+   * (a Python RuntimeError; the autograd Function recomputes on it). */
+  RSV_ERR_STALE_STATE = 6
 } rsv_status;
 
 typedef struct rsv_backend rsv_backend;
@@ -109,7 +113,8 @@ rsv_status rsv_energy_and_grad_device(rsv_backend *backend, const double *d_para
  * rsv_backward_device runs only the adjoint sweep and writes the gradient of
  * that same forward (d_gradient_out, device f64[num_params]).  *generation_out
  * (may be NULL) identifies the forward; rsv_backward_device fails with
- * RSV_ERR_INVALID_ARGUMENT if another call has run on the backend since.
+ * RSV_ERR_STALE_STATE if another call has run on the backend since (and with
+ * RSV_ERR_INVALID_ARGUMENT for a null pointer or backend).
  * No reference counterpart.
  */
 rsv_status rsv_forward_device(rsv_backend *backend, const double *d_params, size_t num_params,

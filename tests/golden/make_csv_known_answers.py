@@ -7,7 +7,8 @@ csv_known_answers.json: for each qubit count, the final energy after 20
 plain gradient-descent steps (stepsize 0.08, seed 7, init 0.3*N(0,1), h=1,
 L=2) from both of the reference's GPU strategies.
 
-Run in a checkout that has the reference at REF (default /root/reference):
+Run with the reference checkout at REF (default: a directory "reference"
+beside this repository's checkout):
     python tests/golden/make_csv_known_answers.py
 """
 
@@ -18,7 +19,7 @@ import json
 import os
 from pathlib import Path
 
-REF = Path(os.environ.get("REF", "/root/reference"))
+REF = Path(os.environ.get("REF", str(Path(__file__).resolve().parents[3] / "reference")))
 CSV = (
     REF
     / "ring_cx_pipeline_vs_original_structed_vs_inversecuQuantum"

@@ -88,3 +88,38 @@ def test_adam_steps_through_the_function_lower_the_energy():
         energies.append(e.item())
     assert energies[-1] < energies[0] - 1.0
     assert energies[-1] >= oracle.ground_energy_free_fermion(n, h) - 1e-9
+
+
+def test_backward_status_stale_state_recomputes_and_other_failures_raise():
+    import ctypes
+
+    import torch
+    from gpu_simulation_b200 import _lib, ring_ising_energy
+
+    n, L, h = 8, 2, 0.9
+    eng = Engine(n, L, h)
+    a = torch.tensor(np.random.default_rng(4).uniform(0, 2 * np.pi, 2 * n * L), device="cuda")
+    e = torch.empty(1, dtype=torch.float64, device="cuda")
+    g = torch.empty_like(a)
+    ga, gb = ctypes.c_ulonglong(), ctypes.c_ulonglong()
+    lib = eng._lib
+    _lib.check(lib.rsv_forward_device(eng._h, a.data_ptr(), a.numel(), e.data_ptr(), ctypes.byref(ga), None))
+    _lib.check(lib.rsv_forward_device(eng._h, a.data_ptr(), a.numel(), e.data_ptr(), ctypes.byref(gb), None))
+    # the first forward's state is gone: a dedicated status, not a bad argument
+    assert lib.rsv_backward_device(eng._h, ga.value, g.data_ptr(), None) == _lib.RSV_ERR_STALE_STATE
+    assert lib.rsv_backward_device(eng._h, gb.value, None, None) == _lib.RSV_ERR_INVALID_ARGUMENT
+    _lib.check(lib.rsv_backward_device(eng._h, gb.value, g.data_ptr(), None))
+
+    class FailingLib:
+        """The engine's library with a backward that reports a CUDA error."""
+
+        def __getattr__(self, name):
+            if name == "rsv_backward_device":
+                return lambda *args: 2  # RSV_ERR_CUDA
+            return getattr(lib, name)
+
+    eng._lib = FailingLib()
+    p = a.clone().requires_grad_(True)
+    with pytest.raises(RuntimeError):
+        ring_ising_energy(p, eng).backward()
+    eng._lib = lib

@@ -62,6 +62,39 @@ def test_noalloc_matches_regular_entry_point_on_consecutive_calls():
         np.testing.assert_allclose(g0, g1, atol=TOL, rtol=0)
 
 
+def test_noalloc_at_its_stated_limit_and_energy_only():
+    # n=16, L=64 is the largest circuit the fixed workspace takes (the largest
+    # carve of state buffers, tables and per-CTA records); then the same call
+    # for the energy alone (no gradient pointer), and a small circuit after it
+    import torch
+
+    lib = _lib.load_library()
+    for n, L, h, seed in ((16, 64, 0.8, 11), (16, 63, 1.3, 12), (13, 64, 1.0, 13), (3, 64, 0.6, 14)):
+        p = np.random.default_rng(seed).uniform(0, 2 * np.pi, 2 * n * L)
+        e0, g0 = _noalloc(n, L, h, p)
+        e1, g1 = _regular(n, L, h, p)
+        assert abs(e0 - e1) < TOL, (n, L, e0, e1)
+        np.testing.assert_allclose(g0, g1, atol=TOL, rtol=0)
+        dp = torch.tensor(p, device="cuda")
+        de = torch.full((1,), float("nan"), dtype=torch.float64, device="cuda")
+        _lib.check(lib.rsv_energy_and_grad_noalloc(n, L, h, dp.data_ptr(), dp.numel(), de.data_ptr(), None,
+                                                   torch.cuda.current_stream().cuda_stream))
+        torch.cuda.synchronize()
+        assert abs(de.item() - e1) < TOL, (n, L, de.item(), e1)
+
+
+def test_noalloc_every_size_up_to_the_limit():
+    # every qubit count up to the limit at a few depths, so every carve the
+    # workspace can be asked for is exercised
+    for n in range(2, 17):
+        for L in (1, 2, 5, 17, 64):
+            p = np.random.default_rng(100 * n + L).uniform(0, 2 * np.pi, 2 * n * L)
+            e0, g0 = _noalloc(n, L, 1.0, p)
+            e1, g1 = _regular(n, L, 1.0, p)
+            assert abs(e0 - e1) < TOL, (n, L, e0, e1)
+            np.testing.assert_allclose(g0, g1, atol=TOL, rtol=0)
+
+
 def test_noalloc_rejects_sizes_beyond_its_workspace():
     import torch
 
@@ -72,3 +105,8 @@ def test_noalloc_rejects_sizes_beyond_its_workspace():
     rc = lib.rsv_energy_and_grad_noalloc(n, L, 1.0, dp.data_ptr(), dp.numel(), de.data_ptr(), None, 0)
     assert rc == _lib.RSV_ERR_INVALID_ARGUMENT
     assert "num_qubits <= 16" in lib.rsv_last_error().decode()
+    n, L = 8, 65
+    dp = torch.zeros(2 * n * L, dtype=torch.float64, device="cuda")
+    rc = lib.rsv_energy_and_grad_noalloc(n, L, 1.0, dp.data_ptr(), dp.numel(), de.data_ptr(), None, 0)
+    assert rc == _lib.RSV_ERR_INVALID_ARGUMENT
+    assert "num_layers <= 64" in lib.rsv_last_error().decode()
