@@ -51,6 +51,8 @@ _SIGNATURES = {
                            ctypes.c_void_p], ctypes.c_int),
     "rsv_set_backward_mode": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "rsv_set_analytic_layers": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "rsv_set_kernels": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "rsv_kernels": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "rsv_analytic_layers": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
                             ctypes.c_int),
     "rsv_backward_mode": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),

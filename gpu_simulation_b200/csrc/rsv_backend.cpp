@@ -29,6 +29,7 @@
 #include "rsv_gate.h"
 #include "rsv_device.cuh"
 #include "rsv_launch.h"
+#include "rsv_tma.h"
 #include "rsv_types.h"
 
 namespace rsv {
@@ -147,6 +148,12 @@ std::vector<Tile> high_tiles(int n, int lo, int min_c = 2) {
   return out;
 }
 
+// Kernel of a backward pass: bwd_pass_kernel / bwd_half_kernel by tile size,
+// or the TMA-fed half-tile kernel (rsv_pass_tma.cu), which rotates its tile
+// bits in another order.
+constexpr int kKernelDefault = 0;
+constexpr int kKernelTma = 1;
+
 struct Step {
   bool bwd = false;
   int layer = 0;
@@ -158,6 +165,7 @@ struct Step {
   int pass_index = -1;  // backward partial record
   int prod_table = 0;   // analytic psi: 0 = full layer-0 state, j >= 1 = partial table j
   int grid = 1;
+  int kernel = kKernelDefault;  // backward: which kernel runs the pass (set once buffers exist)
 };
 
 struct Plan {
@@ -214,8 +222,9 @@ void record_theta(Plan &pl, const Step &s) {
 }
 
 // Backward passes whose gates all lie on tile bits 4..11 of a unit tile with
-// tile bits 0..3 = index bits 0..3 run on the 11-bit half tile (tile bit 3
-// moves to the coset) with two 256-thread CTAs per SM (rsv_pass_half.cu),
+// tile bits 0..3 = index bits 0..3 run on the 11-bit half tile (the highest
+// of the leading contiguous ungated tile bits moves to the coset) with two
+// 256-thread CTAs per SM (rsv_pass_half.cu),
 // for the load/store variants that kernel has, once the pass has at least
 // eight 12-bit tiles per SM (smaller states sit in L2, where the extra CTAs
 // only add launch cost: n = 20 ran 6% slower on half tiles).
@@ -310,12 +319,14 @@ void use_half_tiles(Plan &pl, int sms) {
     const Tile &t = s.tile;
     if (!t.unit || t.dims != 12 || !half_tile_variant(s)) continue;
     if (t.num_tiles < static_cast<u64>(8) * std::max(1, sms)) continue;
-    bool ok = true;
-    for (int b = 0; b < 4; ++b) ok = ok && t.gate_wire[b] < 0 && t.vec[b] == (u64{1} << b);
-    if (!ok) continue;
+    // c leading tile bits are the contiguous, ungated index bits 0..c-1 (c >= 4);
+    // the top one moves to the coset, so index bits 0..c-2 stay contiguous
+    int c = 0;
+    while (c < 12 && t.gate_wire[c] < 0 && t.vec[c] == (u64{1} << c)) ++c;
+    if (c < 4) continue;
     std::vector<int> bits, gates;
     for (int b = 0; b < 12; ++b) {
-      if (b == 3) continue;
+      if (b == c - 1) continue;
       int bit = 0;
       while (!((t.vec[b] >> bit) & 1)) ++bit;
       bits.push_back(bit);
@@ -633,27 +644,46 @@ Plan make_plan_full(int n, int L, int sms, bool checkpoint) {
 // gradient correction.  In checkpoint mode the first wire of every pass
 // carries kUndoPassStart (the gradient correction restarts there, see
 // rot_kernel).
-std::vector<int> undo_order(const Plan &pl) {
+// The wires of one layer in the order its backward passes undo them (with
+// kUndoPassStart on the first wire of every pass in the checkpoint schedule).
+std::vector<int> undo_order_layer(const Plan &pl, int layer) {
   // tile bits in the order the backward kernels rotate them: bwd_pass_kernel
-  // B0, B1, A1, A2 (rsv_pass.cu); bwd_half_kernel H0, H1, HA (rsv_pass_half.cu)
+  // B0, B1, A1, A2 (rsv_pass.cu); bwd_half_kernel H0, H1, HA (rsv_pass_half.cu);
+  // the TMA kernel P, Q (rsv_pass_tma.cu)
   static const int kBits[12] = {9, 10, 11, 6, 7, 8, 0, 1, 2, 3, 4, 5};
   static const int kBitsHalf[11] = {8, 9, 10, 5, 6, 7, 3, 4, 0, 1, 2};
   std::vector<int> ord;
   for (const auto &s : pl.bwd) {
-    if (s.layer != pl.L - 1) continue;
+    if (s.layer != layer) continue;
     bool start = pl.checkpoint;
-    for (int i = 0; i < s.tile.dims; ++i) {
-      const int w = s.tile.gate_wire[s.tile.dims == 12 ? kBits[i] : kBitsHalf[i]];
+    const int count = s.kernel == kKernelTma ? 8 : s.tile.dims;
+    for (int i = 0; i < count; ++i) {
+      const int b = s.kernel == kKernelTma ? kTmaRotationOrder[i] : (s.tile.dims == 12 ? kBits[i] : kBitsHalf[i]);
+      const int w = s.tile.gate_wire[b];
       if (w < 0) continue;
       ord.push_back(start ? (w | kUndoPassStart) : w);
       start = false;
     }
   }
-  if (ord.empty() && (pl.layer0_kernel || pl.mps_k > 0)) {
-    // one layer, computed by the layer-0 kernel: no gradient correction is used
+  if (ord.empty()) {
+    // a layer without passes (layer-0 or matrix-product kernels): no gradient correction is used
     for (int w = 0; w < pl.n; ++w) ord.push_back(w);
   }
   if (static_cast<int>(ord.size()) != pl.n) throw Error(RSV_ERR_INTERNAL, "undo order incomplete");
+  return ord;
+}
+
+// The last layer's undo order (every layer of the plans that the batched
+// kernel and the fixed-workspace entry point run has the same one).
+std::vector<int> undo_order(const Plan &pl) { return undo_order_layer(pl, pl.L - 1); }
+
+// Every layer's undo order, layer after layer ([L][n]).
+std::vector<int> undo_orders(const Plan &pl) {
+  std::vector<int> ord;
+  for (int l = 0; l < pl.L; ++l) {
+    const std::vector<int> o = undo_order_layer(pl, l);
+    ord.insert(ord.end(), o.begin(), o.end());
+  }
   return ord;
 }
 
@@ -801,6 +831,11 @@ struct rsv_backend {
   rsv::Plan plan;
   rsv::DevBuf<double2> states;  // plan.num_bufs state buffers of state_len amplitudes each
   int backward_mode = RSV_BACKWARD_AUTO;
+  // RSV_KERNELS_* flags (rsv_set_kernels): TMA-fed backward passes where eligible
+  int kernel_flags = RSV_KERNELS_TMA;
+  std::vector<rsv::TmaPass> tma;    // per backward step (used where step.kernel is kKernelTma)
+  rsv::DevBuf<int> pipeline_err;    // set by a TMA pass whose pipeline wait gave up
+  int tma_passes = 0;
   int analytic_layers = 3;  // rsv_set_analytic_layers (default: layers 0..2 as a matrix-product state)
   // gradient_strategy "inverse_walk_cuQuantum": gate-level kernels (rsv_gate.cu)
   bool gate_level = false;
@@ -1044,8 +1079,14 @@ Layer0Params layer0_params(rsv_backend *B) {
 
 void run_backward(rsv_backend *B, cudaStream_t st) {
   PassParams P;
-  for (const auto &s : B->plan.bwd) {
+  for (size_t i = 0; i < B->plan.bwd.size(); ++i) {
+    const Step &s = B->plan.bwd[i];
     fill_pass_params(B, s, P);
+    if (s.kernel == kKernelTma) {
+      timed(B, st, 3, pass_bytes(B, s),
+            [&] { check(launch_bwd_tma(P, B->tma[i], s.grid, st), "backward TMA pass launch"); });
+      continue;
+    }
     timed(B, st, 3, pass_bytes(B, s),
           [&] { check(launch_pass(P, true, s.grid, st), "backward pass launch"); });
   }
@@ -1080,6 +1121,7 @@ void run_finalize(rsv_backend *B, bool grad, double *energy_out, double *grad_ou
   F.theta_slot = B->tables.p + np + nl;
   F.phi_pass = B->tables.p + np + 2 * nl;
   F.gscale = B->gscale.p;
+  F.pipeline_err = B->tma_passes > 0 ? B->pipeline_err.p : nullptr;
   F.energy_out = energy_out;
   F.grad_out = grad ? grad_out : nullptr;
   timed(B, st, 4, 0.0, [&] { check(launch_finalize(F, st), "finalize launch"); });
@@ -1171,6 +1213,19 @@ void run_all(rsv_backend *B, bool grad, double *energy_out, double *grad_out, cu
   run_energy(B, st);
   if (grad) run_backward(B, st);
   run_finalize(B, grad, energy_out, grad_out, st);
+}
+
+// After a synchronised call: a NaN energy from a backend with TMA passes may
+// come from a pipeline wait that gave up (finalize_kernel writes NaN then);
+// report it as an error and clear the flag.
+void check_pipeline(rsv_backend *B, double energy) {
+  if (B->tma_passes == 0 || !std::isnan(energy)) return;
+  int flag = 0;
+  check(cudaMemcpy(&flag, B->pipeline_err.p, sizeof(int), cudaMemcpyDeviceToHost), "pipeline flag read");
+  if (flag == 0) return;
+  check(cudaMemset(B->pipeline_err.p, 0, sizeof(int)), "pipeline flag clear");
+  throw Error(RSV_ERR_CUDA, "a TMA backward pass gave up waiting for its pipeline (flag " +
+                                std::to_string(flag) + "); the results of this call are void");
 }
 
 // Synchronous host entry points: NULL selects the backend's own stream.
@@ -1433,7 +1488,7 @@ rsv_status run_in_workspace(int n, int L, double field, const double *d_params, 
     tab.insert(tab.end(), B.plan.theta_pass.begin(), B.plan.theta_pass.end());
     tab.insert(tab.end(), B.plan.theta_slot.begin(), B.plan.theta_slot.end());
     tab.insert(tab.end(), B.plan.phi_pass.begin(), B.plan.phi_pass.end());
-    const std::vector<int> ord = undo_order(B.plan);
+    const std::vector<int> ord = undo_orders(B.plan);
     // carve the workspace (256-byte aligned sections)
     unsigned char *base = static_cast<unsigned char *>(workspace);
     size_t off = 0;
@@ -1485,6 +1540,32 @@ rsv_status run_in_workspace(int n, int L, double field, const double *d_params, 
   });
 }
 
+// Put the eligible backward passes on the TMA-fed kernel (rsv_pass_tma.cu):
+// their tensor maps are encoded here, once per plan, over the backend's own
+// state buffers.  A pass whose maps the driver rejects keeps its default
+// kernel.  Two CTAs per SM.
+void assign_backward_kernels(rsv_backend *B) {
+  B->tma.assign(B->plan.bwd.size(), TmaPass{});
+  B->tma_passes = 0;
+  if (B->pipeline_err.p == nullptr) {
+    B->pipeline_err.alloc(1);
+    check(cudaMemset(B->pipeline_err.p, 0, sizeof(int)), "pipeline flag clear");
+  }
+  PassParams P;
+  for (size_t i = 0; i < B->plan.bwd.size(); ++i) {
+    Step &s = B->plan.bwd[i];
+    s.kernel = kKernelDefault;
+    if (!(B->kernel_flags & RSV_KERNELS_TMA)) continue;
+    fill_pass_params(B, s, P);
+    if (!make_tma_pass(P, B->pipeline_err.p, B->tma[i], nullptr)) continue;
+    s.kernel = kKernelTma;
+    s.grid = static_cast<int>(std::min<u64>(
+        s.tile.num_tiles, static_cast<u64>(bwd_tma_blocks_per_sm()) * static_cast<u64>(std::max(1, B->sms))));
+    if (s.grid > B->plan.max_grid) throw Error(RSV_ERR_INTERNAL, "TMA pass grid exceeds the partial records");
+    ++B->tma_passes;
+  }
+}
+
 // (Re)plan a backend for a backward schedule and allocate what depends on the
 // plan: the state buffers, the product tables, the partial records and the
 // plan tables.  A failed allocation of the checkpoint schedule falls back to
@@ -1528,6 +1609,7 @@ void setup_plan(rsv_backend *B, int mode) {
   }
   B->pass_partials.alloc(static_cast<size_t>(std::max(1, B->num_bwd_passes)) * B->plan.max_grid *
                          kPartialStride);
+  assign_backward_kernels(B);
   std::vector<int> tab;
   for (const auto &s : B->plan.bwd) tab.push_back(s.grid);
   tab.insert(tab.end(), B->plan.theta_pass.begin(), B->plan.theta_pass.end());
@@ -1536,7 +1618,7 @@ void setup_plan(rsv_backend *B, int mode) {
   B->tables.alloc(tab.size());
   check(cudaMemcpy(B->tables.p, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice),
         "plan table upload");
-  const std::vector<int> ord = undo_order(B->plan);
+  const std::vector<int> ord = undo_orders(B->plan);
   B->order.alloc(ord.size());
   check(cudaMemcpy(B->order.p, ord.data(), ord.size() * sizeof(int), cudaMemcpyHostToDevice),
         "order upload");
@@ -1682,6 +1764,7 @@ rsv_status rsv_energy_and_grad(rsv_backend *B, const double *params, size_t num_
                           cudaMemcpyDeviceToHost, st),
           "result download");
     check(cudaStreamSynchronize(st), "energy_and_grad");
+    check_pipeline(B, B->out_host.p[0]);
     *energy_out = B->out_host.p[0];
     if (grad) std::memcpy(gradient_out, B->out_host.p + 1, B->num_params * sizeof(double));
   });
@@ -1893,6 +1976,24 @@ rsv_status rsv_set_analytic_layers(rsv_backend *B, int max_layers) {
     check(cudaStreamSynchronize(B->stream), "backend synchronize");
     B->analytic_layers = max_layers;
     setup_plan(B, B->backward_mode);
+  });
+}
+
+rsv_status rsv_set_kernels(rsv_backend *B, int flags) {
+  return guarded([&] {
+    if (B == nullptr) invalid("backend is null");
+    if ((flags & ~RSV_KERNELS_TMA) != 0) invalid("unknown kernel flags");
+    check(cudaStreamSynchronize(B->stream), "backend synchronize");
+    B->kernel_flags = flags;
+    setup_plan(B, B->backward_mode);
+  });
+}
+
+rsv_status rsv_kernels(rsv_backend *B, int *flags_out, int *tma_passes_out) {
+  return guarded([&] {
+    if (B == nullptr) invalid("backend is null");
+    if (flags_out) *flags_out = B->kernel_flags;
+    if (tma_passes_out) *tma_passes_out = B->tma_passes;
   });
 }
 

@@ -94,7 +94,8 @@ __global__ void tables_kernel(const double4 *__restrict__ coef, int n, int L,
 //   theta of wire w: 1 / (prod of f over the wires of its layer still pending
 //                         when w is undone, w included)^2,
 //   phi of the layer: 1 / K_l^2.
-// order[n] is the undo order of the wires within a backward layer.  In the
+// order[layer * n .. layer * n + n) is the undo order of the wires within
+// backward layer `layer` (the kernels of a layer's passes fix it).  In the
 // checkpoint schedule psi is re-read from the forward pass's checkpoint at
 // every backward pass, so the correction restarts at each pass (entries with
 // kUndoPassStart):
@@ -106,6 +107,7 @@ __global__ void rot_kernel(const double4 *__restrict__ coef, int n, int L, const
                            double *__restrict__ gscale) {
   const int layer = blockIdx.x;
   if (layer >= L) return;
+  order += layer * n;
   for (int w = threadIdx.x; w < n; w += blockDim.x) {
     const double4 k = coef[layer * n + w];
     rot[layer * n + w] = (fabs(k.x) >= fabs(k.y)) ? make_double2(k.y / k.x, 1.0)
@@ -303,6 +305,14 @@ __global__ void __launch_bounds__(kEnergyTileThreads) energy_tile_kernel(const d
 __global__ void finalize_kernel(const FinalizeParams F) {
   __shared__ double red[32];
   const int t = threadIdx.x;
+  if (F.pipeline_err != nullptr && *F.pipeline_err != 0) {
+    // a backward pass did not complete: no result is better than a wrong one
+    const double nan = __longlong_as_double(0x7ff8000000000000ll);
+    if (t == 0) *F.energy_out = nan;
+    if (F.grad_out != nullptr)
+      for (int k = t; k < 2 * F.L * F.n; k += blockDim.x) F.grad_out[k] = nan;
+    return;
+  }
   double e = 0.0;
   for (int i = t; i < F.num_energy_partials; i += blockDim.x) e += F.energy_partials[i];
   e = warp_sum(e);

@@ -1,0 +1,54 @@
+// Backward tile passes fed by the Tensor Memory Accelerator (rsv_pass_tma.cu):
+// host-side description of one pass (tensor maps and tile coordinates) and
+// its launcher.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "rsv_types.h"
+
+namespace rsv {
+
+// Dimensions of a tensor map over a state buffer: every map here has rank 5
+// (unused trailing dimensions have extent 1).  Dimension 0 counts doubles
+// (two per amplitude) and covers index bits 0..2; each other dimension covers a
+// run of consecutive index bits.  A tile's coordinate in dimension d is
+// (cbase >> shift[d]) & mask[d], cbase being the tile's coset base (mask 0 for
+// the dimensions the box spans).
+constexpr int kTmaRank = 5;
+
+struct alignas(64) TmaPass {
+  CUtensorMap psi_map;   // psi loads: box = the 11-bit tile in tile-index order
+  CUtensorMap lam_map;   // lambda loads, same box
+  CUtensorMap out_map;   // lambda store: box dimensions ordered tile bits 0..2, 7..10, 3..6
+  int ld_shift[kTmaRank];
+  unsigned int ld_mask[kTmaRank];
+  int st_shift[kTmaRank];
+  unsigned int st_mask[kTmaRank];
+  int *err;              // device flag: set when a pipeline wait gives up
+};
+
+// Whether a backward pass has the shape and load/store variant of the TMA
+// kernel: 11-bit unit tile with tile bits 0..2 = index bits 0..2, increasing
+// index bits, gates only on tile bits 3..10, psi and lambda loaded in natural
+// order, lambda stored in natural order, psi not stored.  `why` (optional)
+// receives the reason when it does not.
+bool tma_pass_shape_ok(const PassParams &P, std::string *why);
+
+// Encodes the three tensor maps of the pass (needs a CUDA context on the
+// device that owns the buffers).  Returns false (with the reason) when the
+// pass is not eligible or the driver rejects a map; nothing is allocated.
+bool make_tma_pass(const PassParams &P, int *err, TmaPass &out, std::string *why);
+
+// The tile bits in the order the TMA kernel rotates them (undo order).
+constexpr int kTmaRotationOrder[8] = {7, 8, 9, 10, 3, 4, 5, 6};
+
+cudaError_t launch_bwd_tma(const PassParams &P, const TmaPass &T, int grid, cudaStream_t s);
+// blocks per SM the kernel is laid out for (its grid: that many per SM)
+int bwd_tma_blocks_per_sm();
+size_t bwd_tma_smem_bytes();
+
+}  // namespace rsv

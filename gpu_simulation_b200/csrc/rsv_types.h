@@ -123,6 +123,7 @@ struct FinalizeParams {
   const int *theta_slot;         // [L*n]
   const int *phi_pass;           // [L]
   const double *gscale;          // [2 L n] multiplier of every gradient sum
+  const int *pipeline_err;       // non-zero: a TMA pass gave up waiting; outputs become NaN (may be null)
   double *energy_out;
   double *grad_out;              // [2 L n] or null
 };

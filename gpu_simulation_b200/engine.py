@@ -153,6 +153,16 @@ class Engine:
         check(self._lib.rsv_analytic_layers(self._h, ctypes.byref(m), ctypes.byref(u)))
         return {"max_layers": m.value, "used": u.value}
 
+    def set_kernels(self, tma: bool = True) -> None:
+        """Backward passes on the TMA-fed kernel where eligible (default) or
+        all on the cp.async kernels; re-plans the backend."""
+        check(self._lib.rsv_set_kernels(self._h, 1 if tma else 0))
+
+    def kernels(self) -> dict:
+        f, t = ctypes.c_int(), ctypes.c_int()
+        check(self._lib.rsv_kernels(self._h, ctypes.byref(f), ctypes.byref(t)))
+        return {"tma": bool(f.value & 1), "tma_passes": t.value}
+
     def set_field(self, field: float) -> None:
         """Change the transverse field h (same circuit shape and buffers)."""
         check(self._lib.rsv_set_field(self._h, float(field)))

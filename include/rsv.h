@@ -230,6 +230,28 @@ rsv_status rsv_set_analytic_layers(rsv_backend *backend, int max_layers);
 rsv_status rsv_analytic_layers(rsv_backend *backend, int *max_layers_out, int *used_out);
 
 /*
+ * Kernel selection.  With RSV_KERNELS_TMA (the default) the backward passes on
+ * 11-bit tiles whose psi comes from a forward checkpoint and whose lambda is
+ * updated in place run on the TMA-fed kernel
+ * (gpu_simulation_b200/csrc/rsv_pass_tma.cu): a producer warp streams psi and
+ * lambda into a two-stage shared-memory ring with tensor copies and writes
+ * lambda back with tensor stores, four consumer warps rotate; mbarriers are
+ * the only synchronisation.  Its tensor maps are encoded when the backend is
+ * planned; a pass the driver cannot map keeps the cp.async kernel.  Flags 0
+ * keeps every pass on the cp.async kernels.  Results agree to rounding.
+ * rsv_set_kernels re-plans (synchronises the backend's stream); rsv_kernels
+ * reports the flags and how many backward passes of the plan are on the TMA
+ * kernel.  If a TMA pass ever gives up waiting for its pipeline (after 1.5 s),
+ * the call's energy and gradient are NaN and the synchronous entry points
+ * return RSV_ERR_CUDA.  No reference counterpart (the reference's backward
+ * kernels, cpp/ising_cuda_statevector_grad_kernels.cu:683-1326, stage with
+ * cuda::memcpy_async).
+ */
+#define RSV_KERNELS_TMA 1
+rsv_status rsv_set_kernels(rsv_backend *backend, int flags);
+rsv_status rsv_kernels(rsv_backend *backend, int *flags_out, int *tma_passes_out);
+
+/*
  * Batched complex128 GEMM on FP64 tensor cores (mma.sync f64; the dense_scan
  * product tree uses it): C[b] = A[b] B[b] for b < batch, every matrix dim x dim
  * row-major and the batches contiguous; dim < 32 or a multiple of 32.  Device
