@@ -656,9 +656,11 @@ std::vector<int> undo_order_layer(const Plan &pl, int layer) {
   for (const auto &s : pl.bwd) {
     if (s.layer != layer) continue;
     bool start = pl.checkpoint;
-    const int count = s.kernel == kKernelTma ? 8 : s.tile.dims;
+    const bool tma = s.kernel == kKernelTma;
+    const int count = tma ? (s.tile.dims == 12 ? 12 : 8) : s.tile.dims;
     for (int i = 0; i < count; ++i) {
-      const int b = s.kernel == kKernelTma ? kTmaRotationOrder[i] : (s.tile.dims == 12 ? kBits[i] : kBitsHalf[i]);
+      const int b = tma ? (s.tile.dims == 12 ? kTmaLowRotationOrder[i] : kTmaRotationOrder[i])
+                        : (s.tile.dims == 12 ? kBits[i] : kBitsHalf[i]);
       const int w = s.tile.gate_wire[b];
       if (w < 0) continue;
       ord.push_back(start ? (w | kUndoPassStart) : w);
@@ -1559,8 +1561,8 @@ void assign_backward_kernels(rsv_backend *B) {
     fill_pass_params(B, s, P);
     if (!make_tma_pass(P, B->pipeline_err.p, B->tma[i], nullptr)) continue;
     s.kernel = kKernelTma;
-    s.grid = static_cast<int>(std::min<u64>(
-        s.tile.num_tiles, static_cast<u64>(bwd_tma_blocks_per_sm()) * static_cast<u64>(std::max(1, B->sms))));
+    s.grid = static_cast<int>(std::min<u64>(s.tile.num_tiles, static_cast<u64>(bwd_tma_blocks_per_sm(B->tma[i].kind)) *
+                                                                   static_cast<u64>(std::max(1, B->sms))));
     if (s.grid > B->plan.max_grid) throw Error(RSV_ERR_INTERNAL, "TMA pass grid exceeds the partial records");
     ++B->tma_passes;
   }

@@ -420,6 +420,248 @@ __global__ void __launch_bounds__(tw::kThreads, 2)
   }
 }
 
+// ---------------------------------------------------------------------------
+// The 12-wire low pass: a unit tile over index bits 0..11 (4096 contiguous
+// amplitudes), every tile bit gated, psi from a checkpoint, lambda in place.
+// 8 warps x 16 registers, one block per SM.  Layouts (tile index t, 12 bits):
+//   LC: warps -> 5,6,7    lanes -> 0..4           registers -> 8..11
+//   LA: warps -> 9,10,11  lanes -> 3,4,5,6,8      registers -> 0,1,2,7
+//   LB: warps -> 9,10,11  lanes -> 0,1,2,7,8      registers -> 3..6
+// The one change of warp bits comes first: every warp reads LC from the
+// stage, rotates 8..11 and writes the result back to the same places; after
+// `xw` every warp reads LA (its own region, bits 9..11 = warp) and the stage
+// is free, so thread 0 loads the next tile there about a third into this
+// one.  LA -> LB is warp-local, through the warp's own region of the
+// exchange buffer X; lambda is stored from LB (lanes 0..2: whole 128-byte
+// lines).  Per tile, every warp:
+//   wait `fullp`, `fulll` -> read LC -> rotate 8..11 -> write back -> arrive
+//   `xw`, wait `xw` -> read LA -> arrive `sread` -> rotate 0,1,2,7 ->
+//   transpose psi, lambda to LB -> rotate 3..6 -> store lambda;
+// thread 0 besides: after `sread`, the tensor loads of the next tile.  All
+// shared buffers are in tile-index order under the 128-byte swizzle, which
+// keeps every access pattern above conflict-free.  Waits are bounded as in
+// bwd_tma_kernel.
+// ---------------------------------------------------------------------------
+namespace tl {
+constexpr int kWarps = 8;
+constexpr int kThreads = 32 * kWarps;
+constexpr int kR = 16;
+constexpr int kTile = 4096;
+constexpr unsigned kVecBytes = kTile * 16u;  // 64 KiB
+// stage psi at 0, stage lambda at 64 KiB, X at 128 KiB (from a 1024-aligned base)
+constexpr unsigned kSmemBytes = 3 * kVecBytes + 1024;
+
+__device__ __forceinline__ int tC(int l, int w, int r) { return (l & 31) | (w << 5) | (r << 8); }
+__device__ __forceinline__ int tA(int l, int w, int r) {
+  return (r & 7) | ((l & 15) << 3) | ((r >> 3) << 7) | ((l >> 4) << 8) | (w << 9);
+}
+__device__ __forceinline__ int tB(int l, int w, int r) {
+  return (l & 7) | (r << 3) | ((l >> 3) << 7) | (w << 9);
+}
+__device__ __forceinline__ int sw(int t) { return t ^ ((t >> 3) & 7); }
+
+// tile bit of register bit j in layout L (0: LC, 1: LA, 2: LB)
+template <int L>
+__host__ __device__ constexpr int rtb(int j) {
+  return L == 0 ? 8 + j : L == 1 ? (j < 3 ? j : 7) : 3 + j;
+}
+
+// as tw::gates16 for the register bits of layout L; acc[tile bit * kThreads]
+// is the thread's running theta sum (shared memory)
+template <int L>
+__device__ __forceinline__ void gates(const PassParams &P, const double2 *km_tb, double2 (&a)[kR],
+                                      double2 (&b)[kR], double *acc) {
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int tb = rtb<L>(j);
+    if (P.gate_wire[tb] < 0) continue;
+    const double2 km = km_tb[tb];
+    const double k = km.x;
+    double t0 = 0.0, t1v = 0.0;
+    const bool plus = km.y > 0.0;
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+      if (r & (1 << j)) continue;
+      const int r1 = r | (1 << j);
+      const double2 x0 = a[r], x1 = a[r1], y0 = b[r], y1 = b[r1];
+      double &t = ((r >> ((j + 1) & 3)) & 1) ? t1v : t0;
+      t = fma(y1.x, x0.x, t);
+      t = fma(y1.y, x0.y, t);
+      t = fma(-y0.x, x1.x, t);
+      t = fma(-y0.y, x1.y, t);
+      if (plus) {
+        a[r] = make_double2(fma(k, x1.x, x0.x), fma(k, x1.y, x0.y));
+        a[r1] = make_double2(fma(-k, x0.x, x1.x), fma(-k, x0.y, x1.y));
+        b[r] = make_double2(fma(k, y1.x, y0.x), fma(k, y1.y, y0.y));
+        b[r1] = make_double2(fma(-k, y0.x, y1.x), fma(-k, y0.y, y1.y));
+      } else {
+        a[r] = make_double2(fma(k, x0.x, x1.x), fma(k, x0.y, x1.y));
+        a[r1] = make_double2(fma(k, x1.x, -x0.x), fma(k, x1.y, -x0.y));
+        b[r] = make_double2(fma(k, y0.x, y1.x), fma(k, y0.y, y1.y));
+        b[r1] = make_double2(fma(k, y1.x, -y0.x), fma(k, y1.y, -y0.y));
+      }
+    }
+    acc[tb * kThreads] += t0 + t1v;
+  }
+}
+}  // namespace tl
+
+__global__ void __launch_bounds__(tl::kThreads, 1)
+    bwd_tma_low_kernel(const __grid_constant__ PassParams P, const __grid_constant__ TmaPass T) {
+  using namespace tl;
+  using tw::bulk_wait_all;
+  using tw::mbar_arrive;
+  using tw::mbar_expect_tx;
+  using tw::mbar_init;
+  using tw::mbar_wait;
+  using tw::smem_u32;
+  extern __shared__ unsigned char smem_raw[];
+  // fullp, fulll (tx), xw (8), sread (8): one phase per tile
+  __shared__ __align__(8) unsigned long long bars[4];
+  __shared__ double2 km_sm[12];
+  __shared__ double red[kWarps][12];
+  __shared__ double acc_sm[12 * kThreads];  // per thread: theta sums of tile bits 0..11
+  __shared__ volatile int abort_flag;
+
+  const unsigned raw = smem_u32(smem_raw);
+  const unsigned pad = (1024u - (raw & 1023u)) & 1023u;
+  unsigned char *smem = smem_raw + pad;
+  const unsigned sbase = raw + pad;
+  double2 *spsi = reinterpret_cast<double2 *>(smem);
+  double2 *slam = reinterpret_cast<double2 *>(smem + kVecBytes);
+  double2 *xbuf = reinterpret_cast<double2 *>(smem + 2 * kVecBytes);
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const unsigned fullp = smem_u32(&bars[0]), fulll = smem_u32(&bars[1]), xw = smem_u32(&bars[2]);
+  const unsigned sread = smem_u32(&bars[3]);
+  if (tid == 0) {
+    mbar_init(fullp, 1);
+    mbar_init(fulll, 1);
+    mbar_init(xw, kWarps);
+    mbar_init(sread, kWarps);
+    tw::fence_mbar_init();
+    abort_flag = 0;
+  }
+  if (tid < 12) {
+    const int w = P.gate_wire[tid];
+    km_sm[tid] = w >= 0 ? RSV_TABLE_LOAD(&P.rot[P.layer * P.n + w]) : make_double2(0.0, 1.0);
+  }
+#pragma unroll
+  for (int i = 0; i < 12; ++i) acc_sm[i * kThreads + tid] = 0.0;
+  __syncthreads();
+
+  const u32 num_tiles = static_cast<u32>(P.num_tiles);
+  const u32 first = blockIdx.x;
+  const int my_tiles = first < num_tiles ? static_cast<int>((num_tiles - 1 - first) / gridDim.x) + 1 : 0;
+  const bool leader = tid == 0;
+  int loads = 0;  // tile loads issued (phases of fullp and fulll started)
+  auto issue = [&](int j) {
+    int c[kTmaRank];
+    tw::coords(deposit(P, first + static_cast<u32>(j) * gridDim.x), T.ld_shift, T.ld_mask, c);
+    mbar_expect_tx(fullp, kVecBytes);
+    tw::tma_load(sbase, &T.psi_map, c, fullp);
+    mbar_expect_tx(fulll, kVecBytes);
+    tw::tma_load(sbase + kVecBytes, &T.lam_map, c, fulll);
+    ++loads;
+  };
+  if (leader && my_tiles > 0) issue(0);
+
+  double *acc = acc_sm + tid;
+  double2 *lam_out = P.lam_out;
+  int fail = 0;
+
+  for (int j = 0; j < my_tiles; ++j) {
+    if (abort_flag) break;
+    const unsigned par = static_cast<unsigned>(j) & 1u;
+    if (!mbar_wait(fullp, par) || !mbar_wait(fulll, par)) {
+      fail = 11;
+      break;
+    }
+    double2 a[kR], b[kR];
+    // LC: rotate tile bits 8..11 and write back in place
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+      const int t = sw(tC(lane, warp, r));
+      a[r] = spsi[t];
+      b[r] = slam[t];
+    }
+    gates<0>(P, km_sm, a, b, acc);
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+      const int t = sw(tC(lane, warp, r));
+      spsi[t] = a[r];
+      slam[t] = b[r];
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(xw);
+    if (!mbar_wait(xw, par)) {
+      fail = 12;
+      break;
+    }
+    // LA: the warp's own region; then the stage is free
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+      const int t = sw(tA(lane, warp, r));
+      a[r] = spsi[t];
+      b[r] = slam[t];
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(sread);
+    if (leader) {
+      if (!mbar_wait(sread, par)) {
+        fail = 13;
+        abort_flag = 1;
+      } else if (j + 1 < my_tiles) {
+        issue(j + 1);
+      }
+    }
+    __syncwarp();
+    if (abort_flag) break;
+    gates<1>(P, km_sm, a, b, acc);
+    // LA -> LB inside the warp's own region of X
+#pragma unroll
+    for (int r = 0; r < kR; ++r) xbuf[sw(tA(lane, warp, r))] = a[r];
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < kR; ++r) a[r] = xbuf[sw(tB(lane, warp, r))];
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < kR; ++r) xbuf[sw(tA(lane, warp, r))] = b[r];
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < kR; ++r) b[r] = xbuf[sw(tB(lane, warp, r))];
+    __syncwarp();
+    gates<2>(P, km_sm, a, b, acc);
+    const u32 cbase = deposit(P, first + static_cast<u32>(j) * gridDim.x);
+#pragma unroll
+    for (int r = 0; r < kR; ++r) __stcs(&lam_out[cbase | static_cast<u32>(tB(lane, warp, r))], b[r]);
+  }
+  if (fail) {
+    atomicExch(T.err, fail);
+    abort_flag = 1;
+  }
+  if (leader && abort_flag && loads > 0) {
+    // loads this block issued must land before the block exits
+    mbar_wait(fullp, static_cast<unsigned>(loads - 1) & 1u);
+    mbar_wait(fulll, static_cast<unsigned>(loads - 1) & 1u);
+  }
+  if (leader) bulk_wait_all();
+
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 12; ++i) {
+    const double s = warp_sum(acc[i * kThreads]);
+    if (lane == 0) red[warp][i] = s;
+  }
+  __syncthreads();
+  double *rec = P.partials + static_cast<size_t>(blockIdx.x) * kPartialStride;
+  if (tid < 12) {
+    double s = 0.0;
+    for (int ww = 0; ww < kWarps; ++ww) s += red[ww][tid];
+    rec[tid] = s;
+  }
+}
+
 // ------------------------------------------------------------------- host
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -507,7 +749,7 @@ bool encode(CUtensorMap &map, const void *base, int n, const std::vector<MapDim>
 bool map_dims(const PassParams &P, std::vector<MapDim> &ld, std::vector<MapDim> &st, std::string *why) {
   const int n = P.n;
   std::vector<int> tb_of(static_cast<size_t>(n), -1);
-  for (int b = 0; b < 11; ++b) tb_of[static_cast<size_t>(index_bit(P.vec[b]))] = b;
+  for (int b = 0; b < P.tile_bits; ++b) tb_of[static_cast<size_t>(index_bit(P.vec[b]))] = b;
   std::vector<MapDim> coset;
   for (int i = 3; i < n;) {
     const bool tile = tb_of[static_cast<size_t>(i)] >= 0;
@@ -537,7 +779,7 @@ bool map_dims(const PassParams &P, std::vector<MapDim> &ld, std::vector<MapDim> 
   }
   st.clear();
   st.push_back({0, 3, true});
-  {
+  if (P.tile_bits == 11) {
     std::vector<int> hi, lo;
     for (int b = 7; b <= 10; ++b) hi.push_back(index_bit(P.vec[b]));
     for (int b = 3; b <= 6; ++b) lo.push_back(index_bit(P.vec[b]));
@@ -559,13 +801,20 @@ bool tma_pass_shape_ok(const PassParams &P, std::string *why) {
     if (why) *why = m;
     return false;
   };
-  if (P.tile_bits != 11) return no("not an 11-bit tile");
   if (P.psi_load != kLoadNatural || P.lam_load != kLoadNatural || P.psi_store != kStoreNone ||
       P.lam_store != kStoreNatural)
     return no("load/store variant not on the TMA kernel");
   if (P.phase != P.phi_grad) return no("phase without phi sums");
   if (P.n < 14 || P.n > 31 || P.num_tiles > 0xFFFFFFFFull) return no("state size out of range");
   if (P.psi_in == nullptr || P.lam_in == nullptr || P.lam_out == nullptr) return no("missing buffer");
+  if (P.tile_bits == 12) {
+    if (P.phase) return no("low pass with the layer's phase");
+    for (int b = 0; b < 12; ++b)
+      if (P.vec[b] != (1ull << b)) return no("12-bit tile is not index bits 0..11");
+    std::vector<MapDim> ld, st;
+    return map_dims(P, ld, st, why);
+  }
+  if (P.tile_bits != 11) return no("not an 11- or 12-bit tile");
   int prev = -1;
   for (int b = 0; b < 11; ++b) {
     const unsigned long long v = P.vec[b];
@@ -591,8 +840,9 @@ bool make_tma_pass(const PassParams &P, int *err, TmaPass &out, std::string *why
   unsigned mk[kTmaRank];
   if (!encode(out.psi_map, P.psi_in, P.n, ld, out.ld_shift, out.ld_mask, why)) return false;
   if (!encode(out.lam_map, P.lam_in, P.n, ld, sh, mk, why)) return false;
-  if (!encode(out.out_map, P.lam_out, P.n, st, out.st_shift, out.st_mask, why)) return false;
+  if (P.tile_bits == 11 && !encode(out.out_map, P.lam_out, P.n, st, out.st_shift, out.st_mask, why)) return false;
   out.err = err;
+  out.kind = P.tile_bits == 12 ? kTmaLow : kTmaHalf;
   return true;
 }
 
@@ -609,10 +859,16 @@ cudaError_t configure_tma(K k, std::atomic<unsigned long long> &done) {
 }
 }  // namespace
 
-int bwd_tma_blocks_per_sm() { return 2; }
+int bwd_tma_blocks_per_sm(int kind) { return kind == kTmaLow ? 1 : 2; }
 
 cudaError_t launch_bwd_tma(const PassParams &P, const TmaPass &T, int grid, cudaStream_t s) {
-  static std::atomic<unsigned long long> cfg_phase{0}, cfg_plain{0};
+  static std::atomic<unsigned long long> cfg_phase{0}, cfg_plain{0}, cfg_low{0};
+  if (T.kind == kTmaLow) {
+    const cudaError_t e = set_smem_limit_once(bwd_tma_low_kernel, tl::kSmemBytes, cfg_low);
+    if (e != cudaSuccess) return e;
+    bwd_tma_low_kernel<<<grid, tl::kThreads, tl::kSmemBytes, s>>>(P, T);
+    return cudaGetLastError();
+  }
   if (P.phase) {
     const cudaError_t e = configure_tma(bwd_tma_kernel<true>, cfg_phase);
     if (e != cudaSuccess) return e;

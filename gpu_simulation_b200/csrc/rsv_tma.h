@@ -20,22 +20,30 @@ namespace rsv {
 // the dimensions the box spans).
 constexpr int kTmaRank = 5;
 
+// Kernels: kTmaHalf, an 11-bit tile with gates on tile bits 3..10 (the high
+// passes); kTmaLow, the 12-bit unit tile over index bits 0..11 with every bit
+// gated (the low pass).
+constexpr int kTmaHalf = 0;
+constexpr int kTmaLow = 1;
+
 struct alignas(64) TmaPass {
-  CUtensorMap psi_map;   // psi loads: box = the 11-bit tile in tile-index order
+  CUtensorMap psi_map;   // psi loads: box = the tile in tile-index order
   CUtensorMap lam_map;   // lambda loads, same box
-  CUtensorMap out_map;   // lambda store: box dimensions ordered tile bits 0..2, 7..10, 3..6
+  CUtensorMap out_map;   // kTmaHalf lambda store: box dimensions ordered tile bits 0..2, 7..10, 3..6
   int ld_shift[kTmaRank];
   unsigned int ld_mask[kTmaRank];
   int st_shift[kTmaRank];
   unsigned int st_mask[kTmaRank];
   int *err;              // device flag: set when a pipeline wait gives up
+  int kind;              // kTmaHalf or kTmaLow
 };
 
-// Whether a backward pass has the shape and load/store variant of the TMA
-// kernel: 11-bit unit tile with tile bits 0..2 = index bits 0..2, increasing
-// index bits, gates only on tile bits 3..10, psi and lambda loaded in natural
-// order, lambda stored in natural order, psi not stored.  `why` (optional)
-// receives the reason when it does not.
+// Whether a backward pass has the shape and load/store variant of a TMA
+// kernel: psi and lambda loaded in natural order, lambda stored in natural
+// order, psi not stored, and either (kTmaHalf) an 11-bit unit tile with tile
+// bits 0..2 = index bits 0..2, increasing index bits and gates only on tile
+// bits 3..10, or (kTmaLow) the 12-bit unit tile over index bits 0..11 without
+// the layer's phase.  `why` (optional) receives the reason when it does not.
 bool tma_pass_shape_ok(const PassParams &P, std::string *why);
 
 // Encodes the three tensor maps of the pass (needs a CUDA context on the
@@ -43,12 +51,13 @@ bool tma_pass_shape_ok(const PassParams &P, std::string *why);
 // pass is not eligible or the driver rejects a map; nothing is allocated.
 bool make_tma_pass(const PassParams &P, int *err, TmaPass &out, std::string *why);
 
-// The tile bits in the order the TMA kernel rotates them (undo order).
+// The tile bits in the order the TMA kernels rotate them (undo order).
 constexpr int kTmaRotationOrder[8] = {7, 8, 9, 10, 3, 4, 5, 6};
+constexpr int kTmaLowRotationOrder[12] = {8, 9, 10, 11, 0, 1, 2, 7, 3, 4, 5, 6};
 
 cudaError_t launch_bwd_tma(const PassParams &P, const TmaPass &T, int grid, cudaStream_t s);
-// blocks per SM the kernel is laid out for (its grid: that many per SM)
-int bwd_tma_blocks_per_sm();
+// blocks per SM the kernel of `kind` is laid out for (its grid: that many per SM)
+int bwd_tma_blocks_per_sm(int kind);
 size_t bwd_tma_smem_bytes();
 
 }  // namespace rsv
