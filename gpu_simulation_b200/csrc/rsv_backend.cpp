@@ -14,7 +14,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <sstream>
 #include <stdexcept>
@@ -119,8 +121,9 @@ Tile antipodal_tile(int n) {
 
 // Split wires [lo, n) into high tiles with `c` contiguous low bits each;
 // c is chosen to minimise the number of passes, then maximised (longer DRAM
-// segments).  Returns the tiles (gates on the split wires).
-std::vector<Tile> high_tiles(int n, int lo, int min_c = 2) {
+// segments), unless force_c (2..10) fixes it (the autotuner's candidates).
+// Returns the tiles (gates on the split wires).
+std::vector<Tile> high_tiles(int n, int lo, int min_c = 2, int force_c = 0) {
   std::vector<Tile> out;
   const int m = n - lo;
   if (m <= 0) return out;
@@ -134,6 +137,7 @@ std::vector<Tile> high_tiles(int n, int lo, int min_c = 2) {
       best_c = c;
     }
   }
+  if (force_c >= min_c && force_c <= std::min(10, lo)) best_c = force_c;
   const int g = 12 - best_c;
   for (int start = lo; start < n; start += g) {
     const int end = std::min(n, start + g);
@@ -200,13 +204,13 @@ struct Plan {
 // this budget.
 constexpr double kCheckpointBudgetBytes = 96.0 * (1ull << 30);
 
-Plan make_plan(int n, int L, int sms, bool checkpoint, int analytic);
+Plan make_plan(int n, int L, int sms, bool checkpoint, int analytic, int force_c = 0);
 
 // The checkpoint schedule is chosen automatically while its state buffers
 // (after the leading layers the analytic kernels replace) fit the budget.
-bool checkpoint_fits(int n, int L, int analytic) {
+bool checkpoint_fits(int n, int L, int analytic, int force_c = 0) {
   if (n <= kTileBits) return false;
-  const double bufs = static_cast<double>(make_plan(n, L, 148, true, analytic).num_bufs);
+  const double bufs = static_cast<double>(make_plan(n, L, 148, true, analytic, force_c).num_bufs);
   return bufs * 16.0 * static_cast<double>(u64{1} << n) <= kCheckpointBudgetBytes;
 }
 
@@ -453,7 +457,7 @@ Plan make_checkpoint_plan(Plan pl, const std::vector<Tile> &fwd_tiles, int fwd_c
 //     Reference counterpart: run_structured_backward_sweep
 //     (cpp/ising_cuda_structured_adjoint_modes.inc:188-307), which always
 //     un-computes psi.
-Plan make_plan_full(int n, int L, int sms, bool checkpoint);
+Plan make_plan_full(int n, int L, int sms, bool checkpoint, int force_c = 0);
 
 // Plans of the single-circuit engine (half tiles on the eligible backward
 // passes); the batched kernel and the fixed-workspace entry point use
@@ -492,8 +496,8 @@ void compact_buffers(Plan &pl) {
   pl.num_bufs = std::max(next, 2);
 }
 
-Plan make_plan(int n, int L, int sms, bool checkpoint, int analytic) {
-  Plan pl = make_plan_full(n, L, sms, checkpoint);
+Plan make_plan(int n, int L, int sms, bool checkpoint, int analytic, int force_c) {
+  Plan pl = make_plan_full(n, L, sms, checkpoint, force_c);
   use_half_tiles(pl, sms);
   if (analytic >= 2) use_mps(pl, sms, analytic);
   if (pl.mps_k == 0 && analytic >= 1) use_layer0_kernel(pl, sms);
@@ -501,7 +505,7 @@ Plan make_plan(int n, int L, int sms, bool checkpoint, int analytic) {
   return pl;
 }
 
-Plan make_plan_full(int n, int L, int sms, bool checkpoint) {
+Plan make_plan_full(int n, int L, int sms, bool checkpoint, int force_c) {
   Plan pl;
   pl.n = n;
   pl.L = L;
@@ -520,9 +524,9 @@ Plan make_plan_full(int n, int L, int sms, bool checkpoint) {
     fwd_tiles.push_back(unit_tile(pl.phys, all_bits, real_wires));
     bwd_tiles.push_back(unit_tile(pl.phys, all_bits, real_wires));
   } else {
-    fwd_tiles = high_tiles(n, 12);
+    fwd_tiles = high_tiles(n, 12, 2, force_c);
     fwd_tiles.insert(fwd_tiles.begin(), unit_tile(n, all_bits, all_bits));
-    bwd_tiles = high_tiles(n, 11);
+    bwd_tiles = high_tiles(n, 11, 2, force_c);
     std::reverse(bwd_tiles.begin(), bwd_tiles.end());  // highest wires first
     bwd_tiles.push_back(antipodal_tile(n));
   }
@@ -760,7 +764,8 @@ std::string describe(const Plan &pl) {
        << " psi:" << psi_src(s) << "(" << s.psi_in << ")->" << store_name(s.psi_store)
        << "(" << s.psi_out << ") lam:" << load_name(s.lam_load) << "(" << s.lam_in << ")->"
        << store_name(s.lam_store) << "(" << s.lam_out << ")" << (s.phase ? " phase" : "")
-       << (s.phi_grad ? " phi" : "") << " grid=" << s.grid << "\n";
+       << (s.phi_grad ? " phi" : "") << (s.kernel == kKernelTma ? " kernel=tma" : "") << " grid=" << s.grid
+       << "\n";
   if (pl.mps_k > 0)
     os << "mps K=" << pl.mps_k << " grad lam:" << load_name(pl.mps_load) << "(" << pl.mps_lam
        << ") grid=" << pl.mps_grad_grid << "\n";
@@ -835,6 +840,8 @@ struct rsv_backend {
   int backward_mode = RSV_BACKWARD_AUTO;
   // RSV_KERNELS_* flags (rsv_set_kernels): TMA-fed backward passes where eligible
   int kernel_flags = RSV_KERNELS_TMA;
+  int force_c = 0;  // contiguous low bits of the high tiles (0: the planner's choice)
+  std::string tune_report;  // the last rsv_autotune's candidates and choice
   std::vector<rsv::TmaPass> tma;    // per backward step (used where step.kernel is kKernelTma)
   rsv::DevBuf<int> pipeline_err;    // set by a TMA pass whose pipeline wait gave up
   int tma_passes = 0;
@@ -1576,16 +1583,16 @@ void setup_plan(rsv_backend *B, int mode) {
   if (mode != RSV_BACKWARD_AUTO && mode != RSV_BACKWARD_UNCOMPUTE && mode != RSV_BACKWARD_CHECKPOINT)
     invalid("backward mode must be RSV_BACKWARD_AUTO, _UNCOMPUTE or _CHECKPOINT");
   const bool want = mode == RSV_BACKWARD_CHECKPOINT ||
-                    (mode == RSV_BACKWARD_AUTO && checkpoint_fits(B->n, B->L, B->analytic_layers));
+                    (mode == RSV_BACKWARD_AUTO && checkpoint_fits(B->n, B->L, B->analytic_layers, B->force_c));
   B->states.release();
-  Plan pl = make_plan(B->n, B->L, B->sms, want, B->analytic_layers);
+  Plan pl = make_plan(B->n, B->L, B->sms, want, B->analytic_layers, B->force_c);
   B->state_len = size_t{1} << pl.phys;
   try {
     B->states.alloc(static_cast<size_t>(pl.num_bufs) * B->state_len);
   } catch (const Error &e) {
     if (mode != RSV_BACKWARD_AUTO || !pl.checkpoint || e.status != RSV_ERR_OUT_OF_MEMORY) throw;
     cudaGetLastError();  // clear the allocation failure
-    pl = make_plan(B->n, B->L, B->sms, false, B->analytic_layers);
+    pl = make_plan(B->n, B->L, B->sms, false, B->analytic_layers, B->force_c);
     B->states.alloc(static_cast<size_t>(pl.num_bufs) * B->state_len);
   }
   check(cudaMemset(B->states.p, 0, B->states.count * sizeof(double2)), "state memset");
@@ -1626,6 +1633,93 @@ void setup_plan(rsv_backend *B, int mode) {
         "order upload");
   ++B->generation;  // any state kept for a deferred backward is gone
   B->forward_only_state = false;
+}
+
+// ------------------------------------------------------------------------
+// Autotuner: times the plan candidates of a backend once per (device, n, L)
+// and keeps the fastest.  It replaces the reference's hand-written width rules
+// (cpp/ising_cuda_structured_adjoint_modes.inc:188-202,
+// cpp/ising_cuda_rotation_kernels.cu:562-575) by measurements.
+// ------------------------------------------------------------------------
+struct TuneChoice {
+  int mode = RSV_BACKWARD_AUTO, analytic = kDefaultAnalyticLayers, kernels = RSV_KERNELS_TMA, force_c = 0;
+  double ms = 0.0;
+};
+
+std::mutex g_tune_mutex;
+std::map<std::string, TuneChoice> g_tune_cache;
+
+std::string tune_key(const rsv_backend *B) {
+  cudaDeviceProp prop{};
+  check(cudaGetDeviceProperties(&prop, B->device), "cudaGetDeviceProperties");
+  return std::string(prop.name) + "/" + std::to_string(B->sms) + "/n" + std::to_string(B->n) + "/L" +
+         std::to_string(B->L);
+}
+
+void apply_choice(rsv_backend *B, const TuneChoice &c) {
+  B->analytic_layers = c.analytic;
+  B->kernel_flags = c.kernels;
+  B->force_c = c.force_c;
+  setup_plan(B, c.mode);
+}
+
+std::string choice_str(const rsv_backend *B, const TuneChoice &c) {
+  std::ostringstream os;
+  os << "mode=" << (B->plan.checkpoint ? "checkpoint" : "uncompute") << " analytic_layers=" << c.analytic
+     << " tma=" << ((c.kernels & RSV_KERNELS_TMA) ? 1 : 0) << " tma_passes=" << B->tma_passes
+     << " high_tile_c=" << (c.force_c ? std::to_string(c.force_c) : std::string("planner"));
+  return os.str();
+}
+
+// Mean milliseconds of one energy_and_grad of the current plan (one untimed call first).
+double time_plan(rsv_backend *B, const double *d_params, int repeats, cudaStream_t st) {
+  const int nl = B->n * B->L;
+  check(launch_coef(d_params, B->coef.p, nl, st), "coef launch");
+  run_all(B, true, B->outputs.p, B->outputs.p + 1, st);
+  cudaEvent_t a, b;
+  check(cudaEventCreate(&a), "cudaEventCreate");
+  check(cudaEventCreate(&b), "cudaEventCreate");
+  check(cudaEventRecord(a, st), "cudaEventRecord");
+  for (int r = 0; r < repeats; ++r) {
+    check(launch_coef(d_params, B->coef.p, nl, st), "coef launch");
+    run_all(B, true, B->outputs.p, B->outputs.p + 1, st);
+  }
+  check(cudaEventRecord(b, st), "cudaEventRecord");
+  check(cudaEventSynchronize(b), "autotune synchronize");
+  float ms = 0.f;
+  check(cudaEventElapsedTime(&ms, a, b), "cudaEventElapsedTime");
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return static_cast<double>(ms) / repeats;
+}
+
+// The candidates: both backward schedules (checkpoint only where it fits),
+// three or two analytic leading layers, the TMA kernels on or off, and every
+// contiguous run length c of the high tiles that gives the fewest passes.
+std::vector<TuneChoice> tune_candidates(const rsv_backend *B) {
+  std::vector<TuneChoice> out;
+  std::vector<int> cs = {0};
+  if (B->n > 12) {
+    auto passes = [&](int c) { return static_cast<int>(high_tiles(B->n, 12, 2, c).size()); };
+    const int best = passes(0);
+    for (int c = 2; c <= 10; ++c)
+      if (c <= 12 && passes(c) == best) cs.push_back(c);
+  }
+  std::vector<int> analytic = {B->analytic_layers};
+  if (B->n >= 13 && B->L >= 2) analytic = {3, 2};
+  for (int an : analytic)
+    for (int c : cs)
+      for (int mode : {RSV_BACKWARD_CHECKPOINT, RSV_BACKWARD_UNCOMPUTE})
+        for (int k : {RSV_KERNELS_TMA, 0}) {
+          if (mode == RSV_BACKWARD_CHECKPOINT && !checkpoint_fits(B->n, B->L, an, c)) continue;
+          TuneChoice t;
+          t.mode = mode;
+          t.analytic = an;
+          t.kernels = k;
+          t.force_c = c;
+          out.push_back(t);
+        }
+  return out;
 }
 
 Plan plan_for_mode(int n, int L, int mode) {
@@ -1996,6 +2090,91 @@ rsv_status rsv_kernels(rsv_backend *B, int *flags_out, int *tma_passes_out) {
     if (B == nullptr) invalid("backend is null");
     if (flags_out) *flags_out = B->kernel_flags;
     if (tma_passes_out) *tma_passes_out = B->tma_passes;
+  });
+}
+
+rsv_status rsv_autotune(rsv_backend *B, const double *d_params, size_t num_params, int repeats, int flags,
+                        void *stream) {
+  return guarded([&] {
+    validate_params(B, d_params, num_params);
+    if (repeats < 1 || repeats > 1000) invalid("repeats must be in [1, 1000]");
+    if ((flags & ~RSV_AUTOTUNE_FORCE) != 0) invalid("unknown autotune flags");
+    if (B->gate_level || B->dense) invalid("the autotuner plans the structured_adjoint strategy only");
+    cudaStream_t st = device_stream(stream);
+    check(cudaStreamSynchronize(B->stream), "backend synchronize");
+    const std::string key = tune_key(B);
+    {
+      std::lock_guard<std::mutex> lock(g_tune_mutex);
+      auto it = g_tune_cache.find(key);
+      if (it != g_tune_cache.end() && !(flags & RSV_AUTOTUNE_FORCE)) {
+        apply_choice(B, it->second);
+        B->tune_report = "cached " + key + ": " + choice_str(B, it->second) + " " +
+                         std::to_string(it->second.ms) + " ms\n";
+        return;
+      }
+    }
+    std::ostringstream rep;
+    const TuneChoice before{B->backward_mode, B->analytic_layers, B->kernel_flags, B->force_c, 0.0};
+    TuneChoice best;
+    best.ms = 1e300;
+    std::vector<std::string> seen;
+    // every candidate computes the same energy and gradient: the largest
+    // deviation from the first candidate's outputs is reported
+    std::vector<double> ref_out, cur_out(1 + B->num_params);
+    double spread = 0.0;
+    for (TuneChoice c : tune_candidates(B)) {
+      try {
+        apply_choice(B, c);
+      } catch (const Error &e) {
+        if (e.status != RSV_ERR_OUT_OF_MEMORY) throw;
+        cudaGetLastError();
+        rep << "skipped (out of memory): " << choice_str(B, c) << "\n";
+        continue;
+      }
+      // the same launches under another name are timed once
+      std::string sig = describe(B->plan);
+      if (std::find(seen.begin(), seen.end(), sig) != seen.end()) continue;
+      seen.push_back(sig);
+      c.ms = time_plan(B, d_params, repeats, st);
+      check(cudaMemcpy(cur_out.data(), B->outputs.p, cur_out.size() * sizeof(double), cudaMemcpyDeviceToHost),
+            "autotune result read");
+      if (ref_out.empty()) {
+        ref_out = cur_out;
+      } else {
+        for (size_t k = 0; k < cur_out.size(); ++k) spread = std::max(spread, std::fabs(cur_out[k] - ref_out[k]));
+      }
+      rep << "candidate " << choice_str(B, c) << ": " << c.ms << " ms\n";
+      if (c.ms < best.ms) best = c;
+    }
+    if (best.ms >= 1e300) {
+      apply_choice(B, before);
+      throw Error(RSV_ERR_INTERNAL, "no autotune candidate could be planned");
+    }
+    apply_choice(B, best);
+    rep << "largest difference between candidates (energy, gradient): " << spread << "\n";
+    rep << "chosen " << choice_str(B, best) << ": " << best.ms << " ms\n";
+    B->tune_report = rep.str();
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[key] = best;
+  });
+}
+
+rsv_status rsv_describe_backend(rsv_backend *B, char *buf, size_t buf_size, size_t *length_out) {
+  return guarded([&] {
+    if (B == nullptr) invalid("backend is null");
+    std::ostringstream os;
+    os << "analytic_layers=" << B->analytic_layers << " kernels=" << B->kernel_flags
+       << " high_tile_c=" << (B->force_c ? std::to_string(B->force_c) : std::string("planner"))
+       << " tma_passes=" << B->tma_passes << "\n"
+       << describe(B->plan);
+    if (!B->tune_report.empty()) os << "autotune:\n" << B->tune_report;
+    const std::string s = os.str();
+    if (length_out) *length_out = s.size();
+    if (buf && buf_size) {
+      const size_t k = std::min(buf_size - 1, s.size());
+      std::memcpy(buf, s.data(), k);
+      buf[k] = '\0';
+    }
   });
 }
 

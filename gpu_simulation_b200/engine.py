@@ -163,6 +163,27 @@ class Engine:
         check(self._lib.rsv_kernels(self._h, ctypes.byref(f), ctypes.byref(t)))
         return {"tma": bool(f.value & 1), "tma_passes": t.value}
 
+    def autotune(self, params, repeats: int = 3, force: bool = False) -> str:
+        """Time the plan candidates on these parameters (host array or CUDA
+        tensor) and keep the fastest (cached per device and shape for the
+        process); returns the candidates and the choice as text."""
+        import torch
+
+        p = params if isinstance(params, torch.Tensor) else torch.tensor(np.asarray(params, dtype=np.float64))
+        p = p.to(device="cuda", dtype=torch.float64).reshape(-1).contiguous()
+        check(self._lib.rsv_autotune(self._h, p.data_ptr(), p.numel(), int(repeats), 1 if force else 0,
+                                     torch.cuda.current_stream().cuda_stream))
+        text = self.describe()
+        return text[text.index("autotune:"):] if "autotune:" in text else ""
+
+    def describe(self) -> str:
+        """The current plan (one line per kernel launch) and the last autotune report."""
+        n = ctypes.c_size_t()
+        check(self._lib.rsv_describe_backend(self._h, None, 0, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value + 1)
+        check(self._lib.rsv_describe_backend(self._h, buf, n.value + 1, ctypes.byref(n)))
+        return buf.value.decode()
+
     def set_field(self, field: float) -> None:
         """Change the transverse field h (same circuit shape and buffers)."""
         check(self._lib.rsv_set_field(self._h, float(field)))

@@ -252,6 +252,28 @@ rsv_status rsv_set_kernels(rsv_backend *backend, int flags);
 rsv_status rsv_kernels(rsv_backend *backend, int *flags_out, int *tma_passes_out);
 
 /*
+ * Autotuner.  Times every plan candidate of the backend's circuit -- backward
+ * schedule (checkpoint where its buffers fit, uncompute), three or two
+ * analytic leading layers, the TMA kernels on or off, and each contiguous run
+ * length of the high tiles that keeps the fewest passes -- with `repeats`
+ * energy_and_grad calls on the device parameters d_params (after one untimed
+ * call), and re-plans the backend with the fastest.  The choice is cached per
+ * (device, num_qubits, num_layers) for the process: a later call for the same
+ * shape applies it without timing unless flags has RSV_AUTOTUNE_FORCE.
+ * Synchronous; reallocates the state buffers while it tries candidates.
+ * rsv_describe_backend returns the backend's current plan (one line per
+ * kernel launch, with the kernel of each backward pass) and the last
+ * autotune's candidates and choice as text (length in *length_out; at most
+ * buf_size bytes written including the NUL).  Replaces the reference's
+ * hand-written width rules (cpp/ising_cuda_structured_adjoint_modes.inc:188-202,
+ * cpp/ising_cuda_rotation_kernels.cu:562-575).
+ */
+#define RSV_AUTOTUNE_FORCE 1
+rsv_status rsv_autotune(rsv_backend *backend, const double *d_params, size_t num_params, int repeats,
+                        int flags, void *stream);
+rsv_status rsv_describe_backend(rsv_backend *backend, char *buf, size_t buf_size, size_t *length_out);
+
+/*
  * Batched complex128 GEMM on FP64 tensor cores (mma.sync f64; the dense_scan
  * product tree uses it): C[b] = A[b] B[b] for b < batch, every matrix dim x dim
  * row-major and the batches contiguous; dim < 32 or a multiple of 32.  Device
