@@ -52,6 +52,9 @@ _SIGNATURES = {
     "rsv_set_backward_mode": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "rsv_set_analytic_layers": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "rsv_set_kernels": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "rsv_batch_set_cluster": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "rsv_batch_cluster": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                           ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "rsv_autotune": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
                       ctypes.c_void_p], ctypes.c_int),
     "rsv_describe_backend": ([ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)],

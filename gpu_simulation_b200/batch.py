@@ -155,6 +155,17 @@ class BatchEngine:
     def set_active_slots(self, slots: int) -> None:
         check(self._lib.rsv_batch_set_active_slots(self._h, int(slots)))
 
+    def set_cluster(self, cluster: int) -> None:
+        """CTAs per thread-block cluster (1, 2, 4 or 8): a large circuit is
+        spread over up to this many SMs, and the cluster's CTAs add their
+        sums through distributed shared memory."""
+        check(self._lib.rsv_batch_set_cluster(self._h, int(cluster)))
+
+    def cluster(self) -> dict:
+        c, g, m = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(self._lib.rsv_batch_cluster(self._h, ctypes.byref(c), ctypes.byref(g), ctypes.byref(m)))
+        return {"cluster": c.value, "groups": g.value, "max_active_clusters": m.value}
+
     def device_bytes(self) -> int:
         v = ctypes.c_size_t()
         check(self._lib.rsv_batch_info(self._h, None, None, None, ctypes.byref(v)))
@@ -210,18 +221,29 @@ class BatchEngine:
         return graph
 
     def autotune(self, params, energy_out, grad_out=None, candidates=None, repeats: int = 3) -> dict:
-        """Time the batch at several numbers of circuits in flight and keep the
-        fastest (fewer slots keep the working set of large circuits in L2;
-        more slots keep every SM busy).  Returns {slots: ms} and sets the best."""
+        """Time the batch for each cluster size (1, 2, 4, 8 CTAs) and a few
+        numbers of CTAs in flight, and keep the fastest (bigger clusters spread
+        large circuits over more SMs and keep fewer of them, and their states,
+        in flight; more CTAs keep every SM busy).  Returns
+        {"cluster x CTAs": ms} and sets the best."""
         import torch
 
         full = self.max_slots
         if candidates is None:
-            candidates = sorted({max(1, full * k // 8) for k in (2, 3, 4, 5, 6, 7, 8)})
+            candidates = []
+            for c in (1, 2, 4, 8):
+                if c > full:
+                    continue
+                for k in sorted({max(c, (full * f // 4) // c * c) for f in (2, 3, 4)}):
+                    candidates.append((c, k))
         times = {}
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
-        for k in candidates:
+        for c, k in candidates:
+            try:
+                self.set_cluster(c)
+            except ValueError:
+                continue  # no cluster of this size fits
             self.set_active_slots(k)
             self.run_device(params, energy_out, grad_out)
             a.record()
@@ -229,7 +251,8 @@ class BatchEngine:
                 self.run_device(params, energy_out, grad_out)
             b.record()
             b.synchronize()
-            times[int(k)] = a.elapsed_time(b) / repeats
+            times[(c, int(k))] = a.elapsed_time(b) / repeats
         best = min(times, key=times.get)
-        self.set_active_slots(best)
-        return times
+        self.set_cluster(best[0])
+        self.set_active_slots(best[1])
+        return {f"{c}x{k}": ms for (c, k), ms in times.items()}

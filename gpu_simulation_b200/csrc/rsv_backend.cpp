@@ -1340,8 +1340,14 @@ struct rsv_batch {
   // current circuits
   int count = 0;
   size_t num_params = 0;
+  std::vector<rsv::BatchCircuit> circuits;
+  std::vector<double> circuit_cost;
   rsv::DevBuf<rsv::BatchCircuit> d_circuits;
   rsv::DevBuf<int> d_order;
+  // thread-block clusters: CTAs per cluster and the work groups for that size
+  int cluster = 8;
+  int num_groups = 0;
+  rsv::DevBuf<rsv::BatchGroup> d_groups;
   rsv::DevBuf<int> d_counter;
   cudaStream_t stream = nullptr;
 };
@@ -1388,6 +1394,42 @@ void upload(DevBuf<T> &d, const std::vector<T> &h, cudaStream_t st, const char *
     check(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st), what);
 }
 
+// Work groups for the current cluster size: circuits sorted longest first
+// (LPT; ties kept together by plan), then runs of the same plan cut into
+// groups of cluster / per circuits, per = min(cluster, tiles per pass) CTAs
+// each.  Uploads the order and the groups (synchronous).
+void batch_group(rsv_batch *Bt) {
+  const int count = Bt->count;
+  std::vector<int> order(static_cast<size_t>(count));
+  for (int c = 0; c < count; ++c) order[static_cast<size_t>(c)] = c;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    const double ca = Bt->circuit_cost[static_cast<size_t>(a)], cb = Bt->circuit_cost[static_cast<size_t>(b)];
+    if (ca != cb) return ca > cb;
+    return Bt->circuits[static_cast<size_t>(a)].plan < Bt->circuits[static_cast<size_t>(b)].plan;
+  });
+  std::vector<BatchGroup> groups;
+  for (int i = 0; i < count;) {
+    const BatchCircuit &C = Bt->circuits[static_cast<size_t>(order[static_cast<size_t>(i)])];
+    const int tiles = 1 << std::max(0, C.n - kTileBits);
+    BatchGroup g{};
+    g.first = i;
+    g.per = std::min(Bt->cluster, tiles);
+    const int cap = Bt->cluster / g.per;
+    int k = i;
+    while (k < count && k - i < cap &&
+           Bt->circuits[static_cast<size_t>(order[static_cast<size_t>(k)])].plan == C.plan)
+      ++k;
+    g.count = k - i;
+    groups.push_back(g);
+    i = k;
+  }
+  cudaStream_t st = Bt->stream;
+  upload(Bt->d_order, order, st, "batch order upload");
+  upload(Bt->d_groups, groups, st, "batch group upload");
+  check(cudaStreamSynchronize(st), "batch upload");
+  Bt->num_groups = static_cast<int>(groups.size());
+}
+
 void batch_set_circuits(rsv_batch *Bt, int count, const int *ns, const int *Ls, const double *hs) {
   if (count < 0) invalid("count must be non-negative");
   if (count > 0 && (ns == nullptr || Ls == nullptr || hs == nullptr)) invalid("null circuit array");
@@ -1414,12 +1456,6 @@ void batch_set_circuits(rsv_batch *Bt, int count, const int *ns, const int *Ls, 
         Bt->plan_cost[static_cast<size_t>(C.plan)] * static_cast<double>(u64{1} << std::max(n, kTileBits));
     off += static_cast<size_t>(2) * n * L;
   }
-  // Longest first (LPT): the persistent CTAs take circuits in this order.
-  std::vector<int> order(static_cast<size_t>(count));
-  for (int c = 0; c < count; ++c) order[static_cast<size_t>(c)] = c;
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-    return cost[static_cast<size_t>(a)] > cost[static_cast<size_t>(b)];
-  });
   cudaStream_t st = Bt->stream;
   if (Bt->dirty) {
     upload(Bt->d_plans, Bt->plans, st, "batch plan upload");
@@ -1429,10 +1465,11 @@ void batch_set_circuits(rsv_batch *Bt, int count, const int *ns, const int *Ls, 
     Bt->dirty = false;
   }
   upload(Bt->d_circuits, circ, st, "batch circuit upload");
-  upload(Bt->d_order, order, st, "batch order upload");
-  check(cudaStreamSynchronize(st), "batch upload");
+  Bt->circuits = std::move(circ);
+  Bt->circuit_cost = std::move(cost);
   Bt->count = count;
   Bt->num_params = off;
+  batch_group(Bt);
 }
 
 void batch_run(rsv_batch *Bt, const double *d_params, double *d_energy, double *d_grad,
@@ -1443,6 +1480,8 @@ void batch_run(rsv_batch *Bt, const double *d_params, double *d_energy, double *
   A.count = Bt->count;
   A.circuits = Bt->d_circuits.p;
   A.order = Bt->d_order.p;
+  A.groups = Bt->d_groups.p;
+  A.num_groups = Bt->num_groups;
   A.counter = Bt->d_counter.p;
   A.plans = Bt->d_plans.p;
   A.steps = Bt->d_steps.p;
@@ -1454,8 +1493,12 @@ void batch_run(rsv_batch *Bt, const double *d_params, double *d_energy, double *
   A.scratch = Bt->scratch.p;
   A.slot_bytes = Bt->slot_bytes;
   A.state_bytes = Bt->state_bytes;
+  // CTAs: the active slots, rounded down to whole clusters, no more than the groups need
+  const int C = Bt->cluster;
+  const int grid = std::max(C, (std::min(Bt->active_slots, Bt->num_groups * C) / C) * C);
+  if (grid > Bt->slots) invalid("fewer scratch slots than one thread-block cluster");
   check(cudaMemsetAsync(Bt->d_counter.p, 0, sizeof(int), st), "batch counter reset");
-  check(launch_batch(A, std::min(Bt->count, Bt->active_slots), st), "batch launch");
+  check(launch_batch(A, grid, C, st), "batch launch");
 }
 
 }  // namespace
@@ -2243,6 +2286,10 @@ rsv_status rsv_batch_create(int max_qubits, int slots, rsv_batch **out) {
     Bt->max_qubits = max_qubits;
     Bt->slots = slots > 0 ? slots : Bt->sms;
     Bt->active_slots = Bt->slots;
+    // the largest cluster (8, 4, 2, 1) that the slots and the device hold
+    Bt->cluster = 8;
+    while (Bt->cluster > 1 && (Bt->cluster > Bt->slots || batch_max_active_clusters(Bt->cluster) < 1))
+      Bt->cluster /= 2;
     Bt->state_bytes = sizeof(double2) << std::max(max_qubits, kTileBits);
     Bt->slot_bytes = (3 * Bt->state_bytes + batch_slot_table_bytes() + 255) & ~size_t{255};
     Bt->scratch.alloc(Bt->slot_bytes * static_cast<size_t>(Bt->slots));
@@ -2286,6 +2333,27 @@ rsv_status rsv_batch_set_active_slots(rsv_batch *batch, int slots) {
     if (slots < 1 || slots > batch->slots)
       invalid("slots must be in [1, " + std::to_string(batch->slots) + "]");
     batch->active_slots = slots;
+  });
+}
+
+rsv_status rsv_batch_set_cluster(rsv_batch *batch, int cluster) {
+  return guarded([&] {
+    if (batch == nullptr) invalid("batch is null");
+    if (cluster != 1 && cluster != 2 && cluster != 4 && cluster != 8) invalid("cluster must be 1, 2, 4 or 8");
+    if (cluster > batch->slots) invalid("cluster exceeds the scratch slots");
+    if (batch_max_active_clusters(cluster) < 1) invalid("no cluster of this size fits on the device");
+    check(cudaStreamSynchronize(batch->stream), "batch synchronize");
+    batch->cluster = cluster;
+    batch_group(batch);
+  });
+}
+
+rsv_status rsv_batch_cluster(rsv_batch *batch, int *cluster_out, int *groups_out, int *max_active_clusters_out) {
+  return guarded([&] {
+    if (batch == nullptr) invalid("batch is null");
+    if (cluster_out) *cluster_out = batch->cluster;
+    if (groups_out) *groups_out = batch->num_groups;
+    if (max_active_clusters_out) *max_active_clusters_out = batch_max_active_clusters(batch->cluster);
   });
 }
 

@@ -3,11 +3,18 @@
 //
 // The reference has no batched mode (it is only proposed in its design
 // notes); this kernel runs thousands of circuits per launch:
-//   * one CTA (512 threads) per circuit at a time; CTAs take circuits from an
-//     atomic work counter over a list sorted by decreasing cost;
+//   * the CTAs (512 threads each) form thread-block clusters of 1, 2, 4 or 8;
+//     a cluster takes a group of circuits of the same (n, L) from an atomic
+//     work counter over a list sorted by decreasing cost, and spreads each
+//     circuit over per = min(cluster size, tiles per pass) of its CTAs: every
+//     pass's tiles are split between them, a cluster barrier separates the
+//     passes, and the per-CTA energy and gradient sums are added in fixed
+//     order through distributed shared memory (DSMEM) -- so a 16-qubit
+//     circuit runs on 8 SMs at once and only a few large circuits are in
+//     flight, whose states then stay in L2;
 //   * every circuit runs the same pass plan the single-circuit engine uses for
 //     its (n, L) (built on the host, uploaded once), tile by tile on the
-//     CTA's own scratch slot, which stays in L2 for small circuits;
+//     scratch slot of its first CTA;
 //   * a tile is 4096 amplitudes, 8 per thread, in the layout families of the
 //     backward pass kernel (rsv_tile.cuh); the next tile of the same pass is
 //     prefetched with cp.async;
@@ -15,6 +22,8 @@
 //     by the CTA itself; gradient sums are reduced on chip and written once
 //     per circuit, so no cross-CTA reduction is needed and results are
 //     deterministic.
+#include <cooperative_groups.h>
+
 #include "rsv_batch.h"
 
 // the per-circuit tables are written by this kernel, in the slot it reuses
@@ -86,13 +95,15 @@ struct Shared {
   double theta[kBatchMaxLayers * kBatchMaxQubits];
   double phi_b[kBatchMaxLayers * kBatchMaxQubits];
   double phi_tot[kBatchMaxLayers];
-  double energy;
+  double energy;       // this CTA's part of the circuit's energy
+  int item;            // work item taken by the cluster's rank 0 (read through DSMEM)
   int next;
 };
 
-// One pass (forward or backward) of one circuit, all of its tiles.
+// One pass (forward or backward) of one circuit: tiles q, q + per, q + 2 per, ...
 template <bool BWD>
-__device__ void run_pass(const PassParams &P, Shared &S, int lane, int warp, double (&acc)[12]) {
+__device__ void run_pass(const PassParams &P, Shared &S, int lane, int warp, double (&acc)[12], u32 q,
+                         u32 per) {
   const int n = P.n;
   double2 *wbuf = S.trans + warp * 256;
   const bool has_lo = P.gate_wire[0] >= 0 || P.gate_wire[1] >= 0 || P.gate_wire[2] >= 0;
@@ -130,9 +141,9 @@ __device__ void run_pass(const PassParams &P, Shared &S, int lane, int warp, dou
     }
     cp_async_commit();
   };
-  if (staged) issue(0);
+  if (staged && q < num_tiles) issue(q);
 
-  for (u32 tile = 0; tile < num_tiles; ++tile) {
+  for (u32 tile = q; tile < num_tiles; tile += per) {
     const u32 cbase = deposit(P, tile);
     double2 a[kR], b[kR];
     if (staged) {
@@ -168,14 +179,14 @@ __device__ void run_pass(const PassParams &P, Shared &S, int lane, int warp, dou
     if (has_lo) {
       if (BWD) cta_transpose_pair<B1, A1>(S.stage_a, S.stage_b, lane, warp, a, b);
       else cta_transpose<B1, A1>(S.stage_a, lane, warp, a);
-      if (staged && tile + 1 < num_tiles) issue(tile + 1);
+      if (staged && tile + per < num_tiles) issue(tile + per);
       if (BWD) gates<A1>(P, S.km, a, b, acc); else fgates<A1>(P, S.km, a);
       warp_transpose<A1, A2>(wbuf, lane, warp, a);
       if (BWD) warp_transpose<A1, A2>(wbuf, lane, warp, b);
     } else {
       if (BWD) cta_transpose_pair<B1, A2>(S.stage_a, S.stage_b, lane, warp, a, b);
       else cta_transpose<B1, A2>(S.stage_a, lane, warp, a);
-      if (staged && tile + 1 < num_tiles) issue(tile + 1);
+      if (staged && tile + per < num_tiles) issue(tile + per);
     }
     if (BWD) gates<A2>(P, S.km, a, b, acc); else fgates<A2>(P, S.km, a);
 
@@ -197,14 +208,15 @@ __device__ void run_pass(const PassParams &P, Shared &S, int lane, int warp, dou
   __syncthreads();  // the pass's global writes are visible to the next pass
 }
 
-// lambda = P^T H P chi and the energy, one CTA (rsv_kernels.cu energy_kernel).
-__device__ double run_energy(const double2 *chi, double2 *mu, int n, double field, Shared &S) {
+// lambda = P^T H P chi and this CTA's part of the energy (amplitudes
+// q * blockDim + k * per * blockDim + thread), as rsv_kernels.cu energy_kernel.
+__device__ double run_energy(const double2 *chi, double2 *mu, int n, double field, Shared &S, u32 q, u32 per) {
   u64 masks[kBatchMaxQubits];
 #pragma unroll
   for (int w = 0; w < kBatchMaxQubits; ++w) masks[w] = (w < n) ? ring_pinv(u64{1} << w, n) : 0;
   double e = 0.0;
   const u32 size = 1u << n;
-  for (u32 i = threadIdx.x; i < size; i += blockDim.x) {
+  for (u32 i = q * blockDim.x + threadIdx.x; i < size; i += per * blockDim.x) {
     const double2 c = chi[i];
     const double d = diag_after_ring(i, n);
     double2 x = make_double2(0.0, 0.0);
@@ -231,97 +243,118 @@ __device__ double run_energy(const double2 *chi, double2 *mu, int n, double fiel
 }
 
 __global__ void __launch_bounds__(kBatchThreads, 1) batch_kernel(const BatchArgs A) {
+  namespace cg = cooperative_groups;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Shared &S = *reinterpret_cast<Shared *>(smem_raw);
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  unsigned char *slot = A.scratch + static_cast<size_t>(blockIdx.x) * A.slot_bytes;
-  double2 *bufs[3];
-  for (int i = 0; i < 3; ++i) bufs[i] = reinterpret_cast<double2 *>(slot + i * A.state_bytes);
-  double4 *coef = reinterpret_cast<double4 *>(slot + 3 * A.state_bytes);
-  double2 *rot = reinterpret_cast<double2 *>(coef + kBatchMaxLayers * kBatchMaxQubits);
-  double *lscale = reinterpret_cast<double *>(rot + kBatchMaxLayers * kBatchMaxQubits);
-  double *gscale = lscale + kBatchMaxLayers;
-  double2 *ptab = reinterpret_cast<double2 *>(gscale + 2 * kBatchMaxLayers * kBatchMaxQubits);
-  double2 *prod = ptab + kBatchMaxLayers * 1024;
+  cg::cluster_group cl = cg::this_cluster();
+  const int crank = static_cast<int>(cl.block_rank());
+  const int csize = static_cast<int>(cl.num_blocks());
+  const int cbase = static_cast<int>(blockIdx.x) - crank;  // the cluster's CTAs are consecutive
 
   for (;;) {
-    if (threadIdx.x == 0) S.next = atomicAdd(A.counter, 1);
-    __syncthreads();
-    const int idx = S.next;
-    __syncthreads();
-    if (idx >= A.count) break;
-    const BatchCircuit C = A.circuits[A.order[idx]];
+    // rank 0 takes the cluster's next group; every CTA reads it through DSMEM
+    if (crank == 0 && threadIdx.x == 0) S.item = atomicAdd(A.counter, 1);
+    cl.sync();
+    if (threadIdx.x == 0) S.next = *cl.map_shared_rank(&S.item, 0);
+    // every CTA has read rank 0's item before any moves on (or exits: the
+    // shared memory of an exited CTA must not be read)
+    cl.sync();
+    const int item = S.next;
+    if (item >= A.num_groups) break;
+    const BatchGroup G = A.groups[item];
+    const int per = G.per;
+    const int sub = crank / per, q = crank % per;
+    const bool active = sub < G.count;
+    // every CTA of the cluster walks the same plan (inactive ones only keep
+    // the barriers), so all take the same cluster barriers
+    const BatchCircuit C = A.circuits[A.order[G.first + (active ? sub : 0)]];
     const BatchPlan &PL = A.plans[C.plan];
     const int n = C.n, L = C.L;
     const double *params = A.params + C.param_off;
     const int nl = n * L;
+    // the circuit's state buffers and tables: the slot of its first CTA
+    unsigned char *slot = A.scratch + static_cast<size_t>(cbase + sub * per) * A.slot_bytes;
+    double2 *bufs[3];
+    for (int i = 0; i < 3; ++i) bufs[i] = reinterpret_cast<double2 *>(slot + i * A.state_bytes);
+    double4 *coef = reinterpret_cast<double4 *>(slot + 3 * A.state_bytes);
+    double2 *rot = reinterpret_cast<double2 *>(coef + kBatchMaxLayers * kBatchMaxQubits);
+    double *lscale = reinterpret_cast<double *>(rot + kBatchMaxLayers * kBatchMaxQubits);
+    double *gscale = lscale + kBatchMaxLayers;
+    double2 *ptab = reinterpret_cast<double2 *>(gscale + 2 * kBatchMaxLayers * kBatchMaxQubits);
+    double2 *prod = ptab + kBatchMaxLayers * 1024;
 
-    // ---- per-circuit tables (coef_kernel, tables_kernel, rot_kernel) ----
-    for (int k = threadIdx.x; k < nl; k += blockDim.x) {
-      double st, ct, sp, cp;
-      sincos(params[2 * k] * 0.5, &st, &ct);
-      sincos(params[2 * k + 1] * 0.5, &sp, &cp);
-      coef[k] = make_double4(ct, st, cp, sp);
-      rot[k] = (fabs(ct) >= fabs(st)) ? make_double2(st / ct, 1.0) : make_double2(ct / st, -1.0);
-    }
     for (int k = threadIdx.x; k < nl; k += blockDim.x) S.theta[k] = 0.0, S.phi_b[k] = 0.0;
-    // zero-padded layout below 12 qubits: the slot holds another circuit's
-    // data, and the padding amplitudes must read as zero
-    if (n < kTileBits)
-      for (int i = threadIdx.x; i < 3 * kTileSize; i += blockDim.x)
-        bufs[i / kTileSize][i % kTileSize] = make_double2(0.0, 0.0);
     if (threadIdx.x < kBatchMaxLayers) S.phi_tot[threadIdx.x] = 0.0;
-    __syncthreads();
-    // phase tables (tables_kernel): only the entries an index of the
-    // (zero-padded, max(n,12)-bit) state can reach; wires >= n contribute 1 to
-    // the RZ phase and the factor of |0> to the product state
-    const int phys = n > kTileBits ? n : kTileBits;
-    for (int e = threadIdx.x; e < (L + 1) * 1024; e += blockDim.x) {
-      const int layer = e / 1024, byte = (e / 256) % 4, v = e % 256;
-      if ((v >> max(0, phys - byte * 8)) != 0) continue;  // table4 reads entry 0 of every byte
-      double2 accv = make_double2(1.0, 0.0);
-      for (int j = 0; j < 8; ++j) {
-        const int w = byte * 8 + j;
-        const bool one = (v >> j) & 1;
-        double2 f;
-        if (w >= n) {
-          f = (layer < L || !one) ? make_double2(1.0, 0.0) : make_double2(0.0, 0.0);
-        } else {
-          const double4 k = coef[(layer < L ? layer : 0) * n + w];
-          if (layer < L) f = one ? make_double2(k.z, k.w) : make_double2(k.z, -k.w);
-          else f = one ? make_double2(k.y * k.z, k.y * k.w) : make_double2(k.x * k.z, -k.x * k.w);
+    if (active && q == 0) {
+      // ---- per-circuit tables (coef_kernel, tables_kernel, rot_kernel) ----
+      for (int k = threadIdx.x; k < nl; k += blockDim.x) {
+        double st, ct, sp, cp;
+        sincos(params[2 * k] * 0.5, &st, &ct);
+        sincos(params[2 * k + 1] * 0.5, &sp, &cp);
+        coef[k] = make_double4(ct, st, cp, sp);
+        rot[k] = (fabs(ct) >= fabs(st)) ? make_double2(st / ct, 1.0) : make_double2(ct / st, -1.0);
+      }
+      // zero-padded layout below 12 qubits: the slot holds another circuit's
+      // data, and the padding amplitudes must read as zero
+      if (n < kTileBits)
+        for (int i = threadIdx.x; i < 3 * kTileSize; i += blockDim.x)
+          bufs[i / kTileSize][i % kTileSize] = make_double2(0.0, 0.0);
+      __syncthreads();
+      // phase tables (tables_kernel): only the entries an index of the
+      // (zero-padded, max(n,12)-bit) state can reach; wires >= n contribute 1 to
+      // the RZ phase and the factor of |0> to the product state
+      const int phys = n > kTileBits ? n : kTileBits;
+      for (int e = threadIdx.x; e < (L + 1) * 1024; e += blockDim.x) {
+        const int layer = e / 1024, byte = (e / 256) % 4, v = e % 256;
+        if ((v >> max(0, phys - byte * 8)) != 0) continue;  // table4 reads entry 0 of every byte
+        double2 accv = make_double2(1.0, 0.0);
+        for (int j = 0; j < 8; ++j) {
+          const int w = byte * 8 + j;
+          const bool one = (v >> j) & 1;
+          double2 f;
+          if (w >= n) {
+            f = (layer < L || !one) ? make_double2(1.0, 0.0) : make_double2(0.0, 0.0);
+          } else {
+            const double4 k = coef[(layer < L ? layer : 0) * n + w];
+            if (layer < L) f = one ? make_double2(k.z, k.w) : make_double2(k.z, -k.w);
+            else f = one ? make_double2(k.y * k.z, k.y * k.w) : make_double2(k.x * k.z, -k.x * k.w);
+          }
+          accv = cmul(accv, f);
         }
-        accv = cmul(accv, f);
+        if (layer < L) ptab[layer * 1024 + byte * 256 + v] = accv;
+        else prod[byte * 256 + v] = accv;
       }
-      if (layer < L) ptab[layer * 1024 + byte * 256 + v] = accv;
-      else prod[byte * 256 + v] = accv;
-    }
-    if (threadIdx.x < L) {
-      const int layer = threadIdx.x;
-      auto factor = [&](int w) {
-        const double4 k = coef[layer * n + w];
-        return (fabs(k.x) >= fabs(k.y)) ? k.x : k.y;
-      };
-      double K = 1.0;
-      for (int w = 0; w < n; ++w) K *= factor(w);
-      lscale[layer] = K;
-      double pending = K;
-      for (int i = 0; i < n; ++i) {
-        const int w = A.undo[PL.undo_off + i];
-        gscale[2 * (layer * n + w)] = 1.0 / (pending * pending);
-        gscale[2 * (layer * n + w) + 1] = 1.0 / (K * K);
-        pending /= factor(w);
+      if (threadIdx.x < L) {
+        const int layer = threadIdx.x;
+        auto factor = [&](int w) {
+          const double4 k = coef[layer * n + w];
+          return (fabs(k.x) >= fabs(k.y)) ? k.x : k.y;
+        };
+        double K = 1.0;
+        for (int w = 0; w < n; ++w) K *= factor(w);
+        lscale[layer] = K;
+        double pending = K;
+        for (int i = 0; i < n; ++i) {
+          const int w = A.undo[PL.undo_off + i];
+          gscale[2 * (layer * n + w)] = 1.0 / (pending * pending);
+          gscale[2 * (layer * n + w) + 1] = 1.0 / (K * K);
+          pending /= factor(w);
+        }
       }
+      __threadfence();
     }
     __syncthreads();
+    cl.sync();  // the tables are visible to the circuit's other CTAs
 
     // ---- the plan ----
-    double energy = 0.0;
     for (int si = 0; si < PL.num_steps; ++si) {
       const BatchStep &st = A.steps[PL.first_step + si];
       if (st.kind == kBatchEnergy) {
-        energy = run_energy(bufs[st.psi_in], bufs[st.psi_out], n, C.h, S);
+        if (active) S.energy = run_energy(bufs[st.psi_in], bufs[st.psi_out], n, C.h, S, q, per);
+        __threadfence();
+        cl.sync();
         if (A.grad_out == nullptr) break;  // energies only: skip the backward sweep
         continue;
       }
@@ -356,45 +389,63 @@ __global__ void __launch_bounds__(kBatchThreads, 1) batch_kernel(const BatchArgs
           S.km[b] = T.gate_wire[b] >= 0 ? rot[st.layer * n + T.gate_wire[b]] : make_double2(0.0, 1.0);
       }
       __syncthreads();
-      const PassParams &P = S.P;
-      double acc[12];
+      if (active) {
+        const PassParams &P = S.P;
+        double acc[12];
 #pragma unroll
-      for (int i = 0; i < 12; ++i) acc[i] = 0.0;
-      if (st.kind == kBatchForward) {
-        run_pass<false>(P, S, lane, warp, acc);
-      } else {
-        run_pass<true>(P, S, lane, warp, acc);
-        // theta sums of this pass into the circuit's accumulators
+        for (int i = 0; i < 12; ++i) acc[i] = 0.0;
+        if (st.kind == kBatchForward) {
+          run_pass<false>(P, S, lane, warp, acc, static_cast<u32>(q), static_cast<u32>(per));
+        } else {
+          run_pass<true>(P, S, lane, warp, acc, static_cast<u32>(q), static_cast<u32>(per));
+          // this CTA's theta sums of the pass into its accumulators
 #pragma unroll
-        for (int i = 0; i < 12; ++i) {
-          const double s = warp_sum(acc[i]);
-          if (lane == 0) S.red[warp][i] = s;
+          for (int i = 0; i < 12; ++i) {
+            const double s = warp_sum(acc[i]);
+            if (lane == 0) S.red[warp][i] = s;
+          }
+          __syncthreads();
+          if (threadIdx.x < 12 && T.gate_wire[threadIdx.x] >= 0) {
+            double s = 0.0;
+            for (int ww = 0; ww < 16; ++ww) s += S.red[ww][threadIdx.x];
+            S.theta[st.layer * n + T.gate_wire[threadIdx.x]] += s;
+          }
+          if (st.phase) {
+            if (threadIdx.x < n) S.phi_b[st.layer * n + threadIdx.x] = S.phi_sm[threadIdx.x];
+            if (threadIdx.x == 32) S.phi_tot[st.layer] = S.phi_sm[32];
+          }
+          __syncthreads();
         }
-        __syncthreads();
-        if (threadIdx.x < 12 && T.gate_wire[threadIdx.x] >= 0) {
-          double s = 0.0;
-          for (int ww = 0; ww < 16; ++ww) s += S.red[ww][threadIdx.x];
-          S.theta[st.layer * n + T.gate_wire[threadIdx.x]] += s;
-        }
-        if (st.phase) {
-          if (threadIdx.x < n) S.phi_b[st.layer * n + threadIdx.x] = S.phi_sm[threadIdx.x];
-          if (threadIdx.x == 32) S.phi_tot[st.layer] = S.phi_sm[32];
-        }
-        __syncthreads();
       }
+      __threadfence();
+      cl.sync();  // the pass's global writes are visible to the circuit's CTAs
     }
 
-    // ---- outputs ----
-    if (threadIdx.x == 0) A.energy_out[C.index] = energy;
-    if (A.grad_out != nullptr) {
-      double *g = A.grad_out + C.param_off;
-      for (int k = threadIdx.x; k < nl; k += blockDim.x) {
-        const int layer = k / n, w = k % n;
-        g[2 * k] = S.theta[k] * gscale[2 * k];
-        g[2 * k + 1] = (S.phi_tot[layer] - 2.0 * S.phi_b[k]) * gscale[2 * k + 1];
+    // ---- outputs: the first CTA of a circuit adds its CTAs' parts in order ----
+    if (active && q == 0) {
+      const int lead = sub * per;
+      if (threadIdx.x == 0) {
+        double e = 0.0;
+        for (int j = 0; j < per; ++j) e += *cl.map_shared_rank(&S.energy, lead + j);
+        A.energy_out[C.index] = e;
+      }
+      if (A.grad_out != nullptr) {
+        double *g = A.grad_out + C.param_off;
+        for (int k = threadIdx.x; k < nl; k += blockDim.x) {
+          const int layer = k / n;
+          double th = 0.0, pb = 0.0, pt = 0.0;
+          for (int j = 0; j < per; ++j) {
+            th += cl.map_shared_rank(S.theta, lead + j)[k];
+            pb += cl.map_shared_rank(S.phi_b, lead + j)[k];
+            pt += cl.map_shared_rank(S.phi_tot, lead + j)[layer];
+          }
+          g[2 * k] = th * gscale[2 * k];
+          g[2 * k + 1] = (pt - 2.0 * pb) * gscale[2 * k + 1];
+        }
       }
     }
     __syncthreads();
+    cl.sync();  // the parts stay in place until they are read
   }
 }
 
@@ -412,9 +463,41 @@ cudaError_t configure_batch_kernel() {
                               static_cast<int>(sizeof(Shared)));
 }
 
-cudaError_t launch_batch(const BatchArgs &A, int grid, cudaStream_t s) {
-  batch_kernel<<<grid, kBatchThreads, sizeof(Shared), s>>>(A);
-  return cudaGetLastError();
+cudaError_t launch_batch(const BatchArgs &A, int grid, int cluster, cudaStream_t s) {
+  if (cluster < 1 || cluster > 8 || grid % cluster != 0) return cudaErrorInvalidValue;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(static_cast<unsigned>(grid));
+  cfg.blockDim = dim3(kBatchThreads);
+  cfg.dynamicSmemBytes = sizeof(Shared);
+  cfg.stream = s;
+  cudaLaunchAttribute attr{};
+  attr.id = cudaLaunchAttributeClusterDimension;
+  attr.val.clusterDim.x = static_cast<unsigned>(cluster);
+  attr.val.clusterDim.y = 1;
+  attr.val.clusterDim.z = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, batch_kernel, A);
+}
+
+int batch_max_active_clusters(int cluster) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(static_cast<unsigned>(cluster));
+  cfg.blockDim = dim3(kBatchThreads);
+  cfg.dynamicSmemBytes = sizeof(Shared);
+  cudaLaunchAttribute attr{};
+  attr.id = cudaLaunchAttributeClusterDimension;
+  attr.val.clusterDim.x = static_cast<unsigned>(cluster);
+  attr.val.clusterDim.y = 1;
+  attr.val.clusterDim.z = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  int num = 0;
+  if (cudaOccupancyMaxActiveClusters(&num, batch_kernel, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return num;
 }
 
 }  // namespace rsv

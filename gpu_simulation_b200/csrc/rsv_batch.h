@@ -48,10 +48,21 @@ struct BatchCircuit {
   int index;            // position in the caller's list (energy output slot)
 };
 
+// A work item of one thread-block cluster: `count` circuits of the same plan
+// (order[first .. first + count)), each spread over `per` CTAs of the cluster
+// (per = min(cluster size, tiles per pass)); count * per <= cluster size.
+struct BatchGroup {
+  int first;
+  int count;
+  int per;
+};
+
 struct BatchArgs {
   int count;
   const BatchCircuit *circuits;
-  const int *order;     // circuits in decreasing cost
+  const int *order;     // circuits in decreasing cost, circuits of a group adjacent
+  const BatchGroup *groups;
+  int num_groups;
   int *counter;         // work counter, zero at launch
   const BatchPlan *plans;
   const BatchStep *steps;
@@ -68,6 +79,9 @@ struct BatchArgs {
 size_t batch_smem_bytes();
 size_t batch_slot_table_bytes();
 cudaError_t configure_batch_kernel();
-cudaError_t launch_batch(const BatchArgs &A, int grid, cudaStream_t s);
+// grid: a multiple of `cluster` (1, 2, 4 or 8 CTAs per thread-block cluster)
+cudaError_t launch_batch(const BatchArgs &A, int grid, int cluster, cudaStream_t s);
+// clusters of `cluster` CTAs that can be resident at once (0 if none)
+int batch_max_active_clusters(int cluster);
 
 }  // namespace rsv

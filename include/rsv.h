@@ -349,9 +349,26 @@ rsv_status rsv_batch_set_circuits(rsv_batch *batch, int count, const int *num_qu
 rsv_status rsv_batch_info(rsv_batch *batch, int *count, size_t *num_params, int *slots,
                           size_t *device_bytes);
 
-/* Circuits in flight for the following runs (1..the slots given at creation);
- * used by the autotuner (gpu_simulation_b200.batch). */
+/* CTAs in flight for the following runs (1..the slots given at creation;
+ * rounded down to whole clusters); used by the autotuner
+ * (gpu_simulation_b200.batch). */
 rsv_status rsv_batch_set_active_slots(rsv_batch *batch, int slots);
+
+/*
+ * Thread-block clusters of the batched kernel: 1, 2, 4 or 8 CTAs (default 8).
+ * A cluster takes a group of circuits of the same (num_qubits, num_layers) and
+ * spreads each over min(cluster, 2^max(0, num_qubits - 12)) of its CTAs,
+ * which split every pass's 4096-amplitude tiles, meet at a cluster barrier
+ * between passes and add their energy and gradient sums in fixed order
+ * through distributed shared memory.  Results are deterministic for a given
+ * cluster size and agree across sizes to rounding.  rsv_batch_set_cluster
+ * re-groups the current circuits (synchronous); rsv_batch_cluster reports the
+ * size, the number of work groups and how many clusters of that size the
+ * device holds at once.  No reference counterpart.
+ */
+rsv_status rsv_batch_set_cluster(rsv_batch *batch, int cluster);
+rsv_status rsv_batch_cluster(rsv_batch *batch, int *cluster_out, int *groups_out,
+                             int *max_active_clusters_out);
 
 rsv_status rsv_batch_run_device(rsv_batch *batch, const double *d_params, double *d_energy_out,
                                 double *d_gradient_out, void *stream);

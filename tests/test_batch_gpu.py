@@ -142,3 +142,27 @@ def test_invalid_arguments():
         BatchEngine(max_qubits=17)
     e, g = eng.energy_and_grad([], [], [], np.zeros(0))
     assert e.size == 0 and g.size == 0
+
+
+def test_cluster_sizes_agree():
+    # circuits spread over 1, 2, 4 or 8 CTAs of a thread-block cluster (tiles
+    # split between them, sums added through distributed shared memory) give
+    # the same energies and gradients to rounding, each matching the oracle
+    ns, ls, hs, params = mixed_batch(seed=21)
+    eng = BatchEngine()
+    info = eng.cluster()
+    assert info["cluster"] in (1, 2, 4, 8) and info["max_active_clusters"] >= 1
+    results = {}
+    for c in (1, 2, 4, 8):
+        eng.set_cluster(c)
+        assert eng.cluster()["cluster"] == c
+        results[c] = eng.energy_and_grad(ns, ls, hs, params)
+        e2, g2 = eng.energy_and_grad(ns, ls, hs, params)
+        assert np.array_equal(results[c][0], e2) and np.array_equal(results[c][1], g2)
+    for c in (2, 4, 8):
+        np.testing.assert_allclose(results[c][0], results[1][0], atol=1e-12, rtol=0)
+        np.testing.assert_allclose(results[c][1], results[1][1], atol=1e-12, rtol=0)
+    e, g = results[8]
+    check_against_oracle(ns, ls, hs, params, e, g, range(ns.size))
+    with pytest.raises(ValueError):
+        eng.set_cluster(3)

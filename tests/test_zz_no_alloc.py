@@ -110,3 +110,21 @@ def test_noalloc_rejects_sizes_beyond_its_workspace():
     rc = lib.rsv_energy_and_grad_noalloc(n, L, 1.0, dp.data_ptr(), dp.numel(), de.data_ptr(), None, 0)
     assert rc == _lib.RSV_ERR_INVALID_ARGUMENT
     assert "num_layers <= 64" in lib.rsv_last_error().decode()
+
+
+def test_noalloc_on_every_visible_device():
+    # the workspace address and the kernels' shared-memory limits are set up
+    # per device: a call on each visible GPU in turn must match the regular
+    # entry point on that GPU (skipped with one GPU)
+    import torch
+
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two visible GPUs")
+    n, L, h = 14, 3, 0.8
+    p = np.random.default_rng(77).uniform(0, 2 * np.pi, 2 * n * L)
+    for dev in range(torch.cuda.device_count()):
+        with torch.cuda.device(dev):
+            e0, g0 = _noalloc(n, L, h, p)
+            e1, g1 = _regular(n, L, h, p)
+        assert abs(e0 - e1) < TOL, (dev, e0, e1)
+        np.testing.assert_allclose(g0, g1, atol=TOL, rtol=0)
