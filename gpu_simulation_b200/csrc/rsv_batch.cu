@@ -70,18 +70,28 @@ __device__ __forceinline__ void fgates(const PassParams &P, const double2 *km_tb
   }
 }
 
+// Buffer position of amplitude p: the index itself for a state in the global
+// scratch slot; the swizzled tile position for a state held in shared memory
+// (RES, single-tile circuits).
+template <bool RES>
+__device__ __forceinline__ u32 bpos(u32 p) {
+  return RES ? static_cast<u32>(swz(static_cast<int>(p))) : p;
+}
+
+template <bool RES>
 __device__ __forceinline__ double2 load_src(int mode, const double2 *buf, u32 p, int n,
                                             const double2 *prod) {
-  if (mode == kLoadNatural) return buf[p];
-  if (mode == kLoadGatherP) return buf[static_cast<u32>(ring_p(p, n))];
+  if (mode == kLoadNatural) return buf[bpos<RES>(p)];
+  if (mode == kLoadGatherP) return buf[bpos<RES>(static_cast<u32>(ring_p(p, n)))];
   if (mode == kLoadProduct) return table4(prod, static_cast<u32>(ring_pinv(p, n)));
   return table4(prod, p);
 }
 
+template <bool RES>
 __device__ __forceinline__ void store_dst(int mode, double2 *buf, u32 p, int n, double2 v) {
-  if (mode == kStoreNatural) buf[p] = v;
-  else if (mode == kStoreScatterP) buf[static_cast<u32>(ring_p(p, n))] = v;
-  else if (mode == kStoreScatterPinv) buf[static_cast<u32>(ring_pinv(p, n))] = v;
+  if (mode == kStoreNatural) buf[bpos<RES>(p)] = v;
+  else if (mode == kStoreScatterP) buf[bpos<RES>(static_cast<u32>(ring_p(p, n)))] = v;
+  else if (mode == kStoreScatterPinv) buf[bpos<RES>(static_cast<u32>(ring_pinv(p, n)))] = v;
 }
 
 struct Shared {
@@ -101,13 +111,17 @@ struct Shared {
 };
 
 // One pass (forward or backward) of one circuit: tiles q, q + per, q + 2 per, ...
-template <bool BWD>
+// RES: a single-tile circuit whose buffers are the shared staging arrays
+// (P.psi_in ... point into shared memory, positions swizzled): its loads read
+// them directly, its CTA transposes reuse them once every thread holds its
+// amplitudes, and its stores write them back after the pass's last barrier.
+template <bool BWD, bool RES>
 __device__ void run_pass(const PassParams &P, Shared &S, int lane, int warp, double (&acc)[12], u32 q,
                          u32 per) {
   const int n = P.n;
   double2 *wbuf = S.trans + warp * 256;
   const bool has_lo = P.gate_wire[0] >= 0 || P.gate_wire[1] >= 0 || P.gate_wire[2] >= 0;
-  const bool staged = P.psi_load == kLoadNatural || P.psi_load == kLoadGatherP;
+  const bool staged = !RES && (P.psi_load == kLoadNatural || P.psi_load == kLoadGatherP);
   const int tpi = lane | (warp << 5);
   const u32 toffi = thread_offset(P, tpi);
   const u32 v9 = P.vec[9], v10 = P.vec[10], v11 = P.vec[11];
@@ -162,7 +176,8 @@ __device__ void run_pass(const PassParams &P, Shared &S, int lane, int warp, dou
 #pragma unroll
       for (int r = 0; r < kR; ++r) {
         const u32 p = base ^ ((r & 1) ? v9 : 0u) ^ ((r & 2) ? v10 : 0u) ^ ((r & 4) ? v11 : 0u);
-        a[r] = load_src(P.psi_load, P.psi_in, p, n, P.prod);
+        a[r] = load_src<RES>(P.psi_load, P.psi_in, p, n, P.prod);
+        if (RES && BWD) b[r] = load_src<RES>(P.lam_load, P.lam_in, p, n, P.prod);
       }
     }
     if (BWD && P.phase) {
@@ -201,8 +216,8 @@ __device__ void run_pass(const PassParams &P, Shared &S, int lane, int warp, dou
 #pragma unroll
     for (int r = 0; r < kR; ++r) {
       const u32 p = base ^ ((r & 1) ? v3 : 0u) ^ ((r & 2) ? v4 : 0u) ^ ((r & 4) ? v5 : 0u);
-      store_dst(P.psi_store, P.psi_out, p, n, a[r]);
-      if (BWD) store_dst(P.lam_store, P.lam_out, p, n, b[r]);
+      store_dst<RES>(P.psi_store, P.psi_out, p, n, a[r]);
+      if (BWD) store_dst<RES>(P.lam_store, P.lam_out, p, n, b[r]);
     }
   }
   __syncthreads();  // the pass's global writes are visible to the next pass
@@ -210,6 +225,7 @@ __device__ void run_pass(const PassParams &P, Shared &S, int lane, int warp, dou
 
 // lambda = P^T H P chi and this CTA's part of the energy (amplitudes
 // q * blockDim + k * per * blockDim + thread), as rsv_kernels.cu energy_kernel.
+template <bool RES>
 __device__ double run_energy(const double2 *chi, double2 *mu, int n, double field, Shared &S, u32 q, u32 per) {
   u64 masks[kBatchMaxQubits];
 #pragma unroll
@@ -217,19 +233,19 @@ __device__ double run_energy(const double2 *chi, double2 *mu, int n, double fiel
   double e = 0.0;
   const u32 size = 1u << n;
   for (u32 i = q * blockDim.x + threadIdx.x; i < size; i += per * blockDim.x) {
-    const double2 c = chi[i];
+    const double2 c = chi[bpos<RES>(i)];
     const double d = diag_after_ring(i, n);
     double2 x = make_double2(0.0, 0.0);
 #pragma unroll
     for (int w = 0; w < kBatchMaxQubits; ++w) {
       if (w < n) {
-        const double2 t = chi[i ^ static_cast<u32>(masks[w])];
+        const double2 t = chi[bpos<RES>(i ^ static_cast<u32>(masks[w]))];
         x.x += t.x;
         x.y += t.y;
       }
     }
     const double2 m = make_double2(fma(d, c.x, -field * x.x), fma(d, c.y, -field * x.y));
-    mu[i] = m;
+    mu[bpos<RES>(i)] = m;
     e += fma(c.x, m.x, c.y * m.y);
   }
   e = warp_sum(e);
@@ -278,6 +294,17 @@ __global__ void __launch_bounds__(kBatchThreads, 1) batch_kernel(const BatchArgs
     unsigned char *slot = A.scratch + static_cast<size_t>(cbase + sub * per) * A.slot_bytes;
     double2 *bufs[3];
     for (int i = 0; i < 3; ++i) bufs[i] = reinterpret_cast<double2 *>(slot + i * A.state_bytes);
+    // a circuit of at most 12 qubits (one tile, every permutation in place,
+    // two live buffers) keeps its state in this CTA's shared memory for all
+    // of its layers
+    const bool resident = active && n <= kTileBits;
+    if (resident) {
+      bufs[0] = S.stage_a;
+      bufs[1] = S.stage_b;
+      bufs[2] = nullptr;
+      for (int i = threadIdx.x; i < kTileSize; i += blockDim.x)
+        S.stage_a[i] = S.stage_b[i] = make_double2(0.0, 0.0);
+    }
     double4 *coef = reinterpret_cast<double4 *>(slot + 3 * A.state_bytes);
     double2 *rot = reinterpret_cast<double2 *>(coef + kBatchMaxLayers * kBatchMaxQubits);
     double *lscale = reinterpret_cast<double *>(rot + kBatchMaxLayers * kBatchMaxQubits);
@@ -296,11 +323,6 @@ __global__ void __launch_bounds__(kBatchThreads, 1) batch_kernel(const BatchArgs
         coef[k] = make_double4(ct, st, cp, sp);
         rot[k] = (fabs(ct) >= fabs(st)) ? make_double2(st / ct, 1.0) : make_double2(ct / st, -1.0);
       }
-      // zero-padded layout below 12 qubits: the slot holds another circuit's
-      // data, and the padding amplitudes must read as zero
-      if (n < kTileBits)
-        for (int i = threadIdx.x; i < 3 * kTileSize; i += blockDim.x)
-          bufs[i / kTileSize][i % kTileSize] = make_double2(0.0, 0.0);
       __syncthreads();
       // phase tables (tables_kernel): only the entries an index of the
       // (zero-padded, max(n,12)-bit) state can reach; wires >= n contribute 1 to
@@ -352,7 +374,8 @@ __global__ void __launch_bounds__(kBatchThreads, 1) batch_kernel(const BatchArgs
     for (int si = 0; si < PL.num_steps; ++si) {
       const BatchStep &st = A.steps[PL.first_step + si];
       if (st.kind == kBatchEnergy) {
-        if (active) S.energy = run_energy(bufs[st.psi_in], bufs[st.psi_out], n, C.h, S, q, per);
+        if (resident) S.energy = run_energy<true>(bufs[st.psi_in], bufs[st.psi_out], n, C.h, S, q, per);
+        else if (active) S.energy = run_energy<false>(bufs[st.psi_in], bufs[st.psi_out], n, C.h, S, q, per);
         __threadfence();
         cl.sync();
         if (A.grad_out == nullptr) break;  // energies only: skip the backward sweep
@@ -395,9 +418,11 @@ __global__ void __launch_bounds__(kBatchThreads, 1) batch_kernel(const BatchArgs
 #pragma unroll
         for (int i = 0; i < 12; ++i) acc[i] = 0.0;
         if (st.kind == kBatchForward) {
-          run_pass<false>(P, S, lane, warp, acc, static_cast<u32>(q), static_cast<u32>(per));
+          if (resident) run_pass<false, true>(P, S, lane, warp, acc, static_cast<u32>(q), static_cast<u32>(per));
+          else run_pass<false, false>(P, S, lane, warp, acc, static_cast<u32>(q), static_cast<u32>(per));
         } else {
-          run_pass<true>(P, S, lane, warp, acc, static_cast<u32>(q), static_cast<u32>(per));
+          if (resident) run_pass<true, true>(P, S, lane, warp, acc, static_cast<u32>(q), static_cast<u32>(per));
+          else run_pass<true, false>(P, S, lane, warp, acc, static_cast<u32>(q), static_cast<u32>(per));
           // this CTA's theta sums of the pass into its accumulators
 #pragma unroll
           for (int i = 0; i < 12; ++i) {
