@@ -662,12 +662,21 @@ std::vector<int> undo_order_layer(const Plan &pl, int layer) {
     bool start = pl.checkpoint;
     const bool tma = s.kernel == kKernelTma;
     const int count = tma ? (s.tile.dims == 12 ? 12 : 8) : s.tile.dims;
+    // the TMA kernels take the theta sums of their last four rotations (tile
+    // bits 3..6, the end of their order) together on one state
+    const int group_from = tma ? count - 4 : count;
+    bool in_group = false;
     for (int i = 0; i < count; ++i) {
       const int b = tma ? (s.tile.dims == 12 ? kTmaLowRotationOrder[i] : kTmaRotationOrder[i])
                         : (s.tile.dims == 12 ? kBits[i] : kBitsHalf[i]);
       const int w = s.tile.gate_wire[b];
       if (w < 0) continue;
-      ord.push_back(start ? (w | kUndoPassStart) : w);
+      int e = start ? (w | kUndoPassStart) : w;
+      if (i >= group_from) {
+        if (in_group && !start) e |= kUndoSameGroup;
+        in_group = true;
+      }
+      ord.push_back(e);
       start = false;
     }
   }

@@ -134,17 +134,22 @@ __global__ void rot_kernel(const double4 *__restrict__ coef, int n, int L, const
     // psi and lambda both carry K (the phase pass), at the start of every
     // later pass their factors cancel; inside a pass each undone wire divides
     // both by its f.
-    double undone = 1.0;
+    // Wires flagged kUndoSameGroup see the state the group's first wire saw.
+    double undone = 1.0, group = 1.0;
     bool first = true;
     for (int i = 0; i < n; ++i) {
       const int w = order[i] & (kUndoPassStart - 1);
       if (i > 0 && (order[i] & kUndoPassStart)) {
         undone = 1.0;
+        group = 1.0;
         first = false;
+      } else if (!(order[i] & kUndoSameGroup)) {
+        undone *= group;
+        group = 1.0;
       }
       gscale[2 * (layer * n + w)] = undone * undone / (first ? K * K : 1.0);
       gscale[2 * (layer * n + w) + 1] = 1.0 / (K * K);
-      undone *= factor(w);
+      group *= factor(w);
     }
   }
 }

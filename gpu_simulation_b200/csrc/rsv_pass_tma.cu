@@ -181,6 +181,54 @@ __device__ __forceinline__ void gates16(const PassParams &P, const double2 *km_t
   }
 }
 
+// The last layout's four gates: the theta sums of all four on the incoming psi
+// and lambda (the gates act on different wires and commute, so each sum is
+// the one the sequential undo would take), then RY^dagger / f on lambda alone
+// (psi is not needed after the pass).
+template <int TB0, int NT>
+__device__ __forceinline__ void gates_last(const PassParams &P, const double2 *km_tb, const double2 (&a)[kR],
+                                           double2 (&b)[kR], double *acc) {
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int tb = TB0 + j;
+    if (P.gate_wire[tb] < 0) continue;
+    double t0 = 0.0, t1 = 0.0;
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+      if (r & (1 << j)) continue;
+      const int r1 = r | (1 << j);
+      const double2 x0 = a[r], x1 = a[r1], y0 = b[r], y1 = b[r1];
+      double &t = ((r >> ((j + 1) & 3)) & 1) ? t1 : t0;
+      t = fma(y1.x, x0.x, t);
+      t = fma(y1.y, x0.y, t);
+      t = fma(-y0.x, x1.x, t);
+      t = fma(-y0.y, x1.y, t);
+    }
+    acc[(tb - 3) * NT] += t0 + t1;
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int tb = TB0 + j;
+    if (P.gate_wire[tb] < 0) continue;
+    const double2 km = km_tb[tb];
+    const double k = km.x;
+    const bool plus = km.y > 0.0;
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+      if (r & (1 << j)) continue;
+      const int r1 = r | (1 << j);
+      const double2 y0 = b[r], y1 = b[r1];
+      if (plus) {
+        b[r] = make_double2(fma(k, y1.x, y0.x), fma(k, y1.y, y0.y));
+        b[r1] = make_double2(fma(-k, y0.x, y1.x), fma(-k, y0.y, y1.y));
+      } else {
+        b[r] = make_double2(fma(k, y0.x, y1.x), fma(k, y0.y, y1.y));
+        b[r1] = make_double2(fma(k, y1.x, -y0.x), fma(k, y1.y, -y0.y));
+      }
+    }
+  }
+}
+
 // layout P -> layout Q of one vector through the warp's slice
 __device__ __forceinline__ void transpose_pq(double2 *xs, int lane, double2 (&a)[kR]) {
 #pragma unroll
@@ -330,7 +378,7 @@ __global__ void __launch_bounds__(tw::kThreads, 2)
     transpose_pq(xs, lane, a);
     transpose_pq(xs, lane, b);
     if (lane == 0) mbar_arrive(xdone);
-    gates16<3>(P, km_sm, a, b, acc);
+    gates_last<3, kThreads>(P, km_sm, a, b, acc);
     // every warp has left its slice before any warp writes the output box
     if (!mbar_wait(xdone, par)) {
       fail = 4;
@@ -631,7 +679,8 @@ __global__ void __launch_bounds__(tl::kThreads, 1)
 #pragma unroll
     for (int r = 0; r < kR; ++r) b[r] = xbuf[sw(tB(lane, warp, r))];
     __syncwarp();
-    gates<2>(P, km_sm, a, b, acc);
+    // LB: tile bits 3..6 (the acc of tile bit tb is acc[tb * kThreads])
+    tw::gates_last<3, kThreads>(P, km_sm, a, b, acc + 3 * kThreads);
     const u32 cbase = deposit(P, first + static_cast<u32>(j) * gridDim.x);
 #pragma unroll
     for (int r = 0; r < kR; ++r) __stcs(&lam_out[cbase | static_cast<u32>(tB(lane, warp, r))], b[r]);

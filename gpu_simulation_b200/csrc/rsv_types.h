@@ -28,6 +28,11 @@ enum StoreMode : int {
 // a backward pass when the gradient correction restarts at every pass
 // (checkpoint schedule).
 constexpr int kUndoPassStart = 1 << 16;
+// ... and this flag on a wire whose theta sum its pass takes on the same state
+// as the previous wire's (the gates of one register layout, which commute,
+// summed together before any of them is undone): it shares that wire's
+// correction, and the group's factors apply after the group.
+constexpr int kUndoSameGroup = 1 << 17;
 
 // Partial product tables of layer 0 (checkpoint schedule): at most this many,
 // each [4][256] after the full product table.
