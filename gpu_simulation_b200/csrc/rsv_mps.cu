@@ -519,6 +519,261 @@ __global__ void __launch_bounds__(kMpsThreads) mps_grad_kernel(const MpsParams Q
   }
 }
 
+// Bond 4, warp-specialised: the FP64 tensor-core phase of a tile (X1, X2)
+// and its FP64 phase (G, F, Z) overlap instead of alternating.  Sixteen warps:
+//   warps 0..7 ("tensor warps") only read fragments and issue MMAs: wait for
+//     tile k in stage k & 1, compute X1 (warps 0..3) and X2 (warps 4..7) as in
+//     mps_grad_kernel (B fragments from a swizzled shared copy of M1, M2),
+//     release the stage, wait until X buffer k & 1 is free and write it;
+//   warps 8..15 ("FP64 warps") load the tiles (cp.async, up to two ahead) and
+//     take tile k's X1, X2 from buffer k & 1 while the tensor warps work on
+//     tile k + 1.  Thread c owns a = c >> 2 and row i = c & 3: that row of
+//     G(a), F(h = a) and of M1(a) X1(a), whose sum over a (a lane butterfly
+//     over a's bits 0..2, then the eight warps in order) is Z of the tile.
+// Hand-offs on named barriers (bar.arrive by the producer, bar.sync by the
+// consumer; 512 threads): kBarStageFull + s / kBarStageEmpty + s (stage s
+// loaded / read), kBarXFull + b / kBarXEmpty + b (X buffer b written / read);
+// kBarCons synchronises the FP64 warps alone.  Both sides run the same tile
+// count and every arrive is matched by one sync, so every barrier phase
+// completes.
+namespace mg4 {
+constexpr int kThreads = 512;
+constexpr int kTensorThreads = 256;
+constexpr int kFp64Threads = kThreads - kTensorThreads;
+constexpr int kE = 16;
+constexpr int kBarStageFull = 1, kBarStageEmpty = 3, kBarXFull = 5, kBarXEmpty = 7, kBarCons = 9;
+// stages, X buffers, M1 / M2, C (two tiles), Z partials of the eight FP64 warps
+constexpr size_t kSmem = (2 * 4096 + 2 * 2 * 64 * kE + 2 * 64 * kE + 2 * kE + 8 * kE) * sizeof(double2);
+static_assert(kSmem <= 232448, "more shared memory than a block can have");
+// slot of M entry (k, column) in the shared copy: the column's bits 1, 2 XOR
+// k's bits 0, 1, so that the B fragment reads (k = 4 ks + t4, column
+// 8 nt + fg) of a quarter-warp fall in eight different bank groups
+__device__ __forceinline__ int mslot(int k, int col) { return k * kE + (col ^ ((k & 3) << 1)); }
+// slot of X entry e of row r (a for X1, h for X2): bits 0, 1 of e XOR r's bit 0
+// and e's bit 3, so that both the tensor warps' writes (a quarter-warp varies
+// r bit 0 and e bits 1, 2) and the FP64 warps' row reads (r bit 0, e bits 2, 3)
+// fall in eight different bank groups
+__device__ __forceinline__ int xslot(int r, int e) { return r * kE + (e ^ (r & 1) ^ (((e >> 3) & 1) << 1)); }
+__device__ __forceinline__ void bar_sync(int id, int count) {
+  asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(count) : "memory");
+}
+__device__ __forceinline__ void bar_arrive(int id, int count) {
+  asm volatile("bar.arrive %0, %1;\n" ::"r"(id), "r"(count) : "memory");
+}
+__device__ __forceinline__ double2 lds_f64x2(unsigned addr) {
+  double2 v;
+  asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];\n" : "=d"(v.x), "=d"(v.y) : "r"(addr) : "memory");
+  return v;
+}
+__device__ __forceinline__ double2 shfl_xor2(double2 v, int m) {
+  return make_double2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+
+// One tile's X1 (SECOND = false: rows a, K = h, B = M2) or X2 (rows h, K = a,
+// B = M1) rows of a tensor warp: 32 rows x 8 columns as four m8n8k4 row tiles
+// (twelve independent MMA chains), K = 64 in sixteen steps.  The A and B
+// fragments come through volatile shared loads issued one K step ahead of the
+// (volatile) MMAs that use them.  With the stage swizzle mps_slot<4> the A
+// fragment addresses are affine in (K step, row tile) from one or two
+// per-thread bases:
+//   X1: slot = (row ^ s(t4)) + 64 col, row = r0 + 8 rt + fg, col = 4 ks + t4,
+//       s(t4) = (t4 & 1) << 2 | (t4 & 2)                -> base + 4096 B ks + 128 B rt;
+//   X2: slot = (col ^ s(fg)) + 64 row, col ^ s(fg) = 4 (ks ^ (fg & 1)) + (t4 ^ (fg & 2))
+//                                                    -> base(ks parity) + 64 B ks + 8192 B rt;
+// and the B fragment of step ks is M entry (4 ks + t4, 8 nt + fg): mslot
+// keeps column bits 1, 2 ^ t4, so base + 1024 B ks.
+template <bool SECOND>
+__device__ __forceinline__ void tensor_tile(unsigned sst, unsigned mbase, int xr0, int fg, int t4,
+                                            double (&t1)[4][2], double (&t2)[4][2], double (&t3)[4][2]) {
+  unsigned base0, base1;  // even / odd K steps
+  if (SECOND) {
+    const unsigned b = sst + 16u * static_cast<unsigned>((t4 ^ (fg & 2)) + 64 * (xr0 + fg));
+    base0 = b + 64u * static_cast<unsigned>(fg & 1);
+    base1 = b - 64u * static_cast<unsigned>(fg & 1);
+  } else {
+    base0 = base1 = sst + 16u * static_cast<unsigned>(xr0 + (fg ^ (((t4 & 1) << 2) | (t4 & 2))) + 64 * t4);
+  }
+  auto addr = [&](int ks, int rt) {
+    return ((ks & 1) ? base1 : base0) + (SECOND ? 64u * ks + 8192u * rt : 4096u * ks + 128u * rt);
+  };
+  double2 cur[4], nxt[4], bcur, bnxt;
+  bcur = lds_f64x2(mbase);
+#pragma unroll
+  for (int rt = 0; rt < 4; ++rt) cur[rt] = lds_f64x2(addr(0, rt));
+#pragma unroll
+  for (int ks = 0; ks < 16; ++ks) {
+    if (ks + 1 < 16) {
+      bnxt = lds_f64x2(mbase + 1024u * (ks + 1));
+#pragma unroll
+      for (int rt = 0; rt < 4; ++rt) nxt[rt] = lds_f64x2(addr(ks + 1, rt));
+    }
+    const double bsum = bcur.x + bcur.y;
+#pragma unroll
+    for (int rt = 0; rt < 4; ++rt) {
+      const double2 l = cur[rt];
+      mma_f64(t1[rt][0], t1[rt][1], l.x, bcur.x);
+      mma_f64(t2[rt][0], t2[rt][1], l.y, bcur.y);
+      mma_f64(t3[rt][0], t3[rt][1], l.x - l.y, bsum);
+    }
+    if (ks + 1 < 16) {
+      bcur = bnxt;
+#pragma unroll
+      for (int rt = 0; rt < 4; ++rt) cur[rt] = nxt[rt];
+    }
+  }
+}
+}  // namespace mg4
+
+__global__ void __launch_bounds__(mg4::kThreads, 1) mps_grad4_kernel(const MpsParams Q,
+                                                                       const double2 *__restrict__ lam, int gather) {
+  using namespace mg4;
+  constexpr int E = kE;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2 *stage = reinterpret_cast<double2 *>(smem_raw);  // [2][4096]
+  double2 *xbuf = stage + 2 * 4096;                        // [2][X1, X2][64][E]
+  double2 *msm = xbuf + 2 * 2 * 64 * E;                    // [M1, M2][64 mslots]
+  double2 *csm = msm + 2 * 64 * E;                         // [2][E]
+  double2 *zp = csm + 2 * E;                               // [8][E]
+
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int n = Q.n;
+  const u64 num_tiles = Q.num_tiles, first = blockIdx.x;
+  const int my_tiles = first < num_tiles ? static_cast<int>((num_tiles - 1 - first) / gridDim.x) + 1 : 0;
+  for (int i = t; i < 2 * 64 * E; i += kThreads) {
+    const int m = i >> 10, k = (i >> 4) & 63, col = i & 15;
+    msm[m * 64 * E + mslot(k, col)] = Q.mtab[i];
+  }
+  __syncthreads();
+
+  if (warp < 8) {
+    const int fg = lane >> 2, t4 = lane & 3;
+    const bool xsecond = warp >= 4;
+    const int xnt = warp & 1, xr0 = 32 * ((warp >> 1) & 1);
+    // B fragments of step 0: M entry (t4, 8 nt + fg) of M2 (X1) or M1 (X2)
+    const unsigned mbase =
+        static_cast<unsigned>(__cvta_generic_to_shared(msm + (xsecond ? 0 : 64 * E) + mslot(t4, 8 * xnt + fg)));
+    for (int k = 0; k < my_tiles; ++k) {
+      const int b = k & 1;
+      bar_sync(kBarStageFull + b, kThreads);  // tile k is in stage b
+      const unsigned sst = static_cast<unsigned>(__cvta_generic_to_shared(stage + b * 4096));
+      double t1[4][2] = {}, t2[4][2] = {}, t3[4][2] = {};
+      if (xsecond) tensor_tile<true>(sst, mbase, xr0, fg, t4, t1, t2, t3);
+      else tensor_tile<false>(sst, mbase, xr0, fg, t4, t1, t2, t3);
+      if (k + 2 < my_tiles) bar_arrive(kBarStageEmpty + b, kThreads);  // stage b may take tile k + 2
+      if (k >= 2) bar_sync(kBarXEmpty + b, kThreads);                   // X buffer b is done with tile k - 2
+      double2 *xo = xbuf + (2 * b + (xsecond ? 1 : 0)) * 64 * E;
+#pragma unroll
+      for (int rt = 0; rt < 4; ++rt)
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+          xo[xslot(xr0 + 8 * rt + fg, 8 * xnt + 2 * t4 + e)] =
+              make_double2(t1[rt][e] + t2[rt][e], t3[rt][e] - t1[rt][e] + t2[rt][e]);
+      bar_arrive(kBarXFull + b, kThreads);
+    }
+    return;
+  }
+
+  // FP64 warps
+  const int c = t - kTensorThreads, cw = c >> 5;
+  const int a = c >> 2, row = c & 3;
+  // Tile j into stage j & 1, one cp.async group.  (Computing each source
+  // index in full spreads the copies out; issued back to back from
+  // precomputed offsets they slowed the tensor warps' fragment loads.)
+  auto issue = [&](int j) {
+    const u64 base = (first + static_cast<u64>(j) * gridDim.x) << 12;
+    double2 *st = stage + (j & 1) * 4096;
+#pragma unroll
+    for (int r = 0; r < 4096 / kFp64Threads; ++r) {
+      const int tau = c + r * kFp64Threads;
+      const u64 p = base | static_cast<u64>(tau);
+      cp_async16(&st[mps_slot<4>(tau)], &lam[gather ? ring_p(p, n) : p]);
+    }
+    cp_async_commit();
+  };
+  if (my_tiles > 0) issue(0);
+  if (my_tiles > 1) issue(1);
+  if (my_tiles > 0) {
+    if (my_tiles > 1) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    else cp_async_wait_all();
+    bar_arrive(kBarStageFull + 0, kThreads);
+  }
+  double2 g[4], f[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) g[j] = f[j] = make_double2(0.0, 0.0);
+  const unsigned lomask = (1u << Q.m1) - 1u;
+  for (int k = 0; k < my_tiles; ++k) {
+    const int b = k & 1;
+    const u64 tile = first + static_cast<u64>(k) * gridDim.x;
+    if (k + 1 < my_tiles) {  // tile k + 1 (the only group in flight) has landed
+      cp_async_wait_all();
+      bar_arrive(kBarStageFull + (b ^ 1), kThreads);
+    }
+    if (k + 2 < my_tiles) {  // stage b is free once the tensor warps have read tile k
+      bar_sync(kBarStageEmpty + b, kThreads);
+      issue(k + 2);
+    }
+    if (c < E) {
+      // C_t = CosLo(lo) CosHi(hi), entry c
+      const unsigned lo = static_cast<unsigned>(tile) & lomask, hi = static_cast<unsigned>(tile >> Q.m1);
+      const double2 *cl = Q.coslo + lo * E, *ch = Q.coshi + hi * E;
+      const int i = c >> 2, j = c & 3;
+      double2 s = cmul(__ldg(&cl[i * 4]), __ldg(&ch[j]));
+#pragma unroll
+      for (int kk = 1; kk < 4; ++kk) s = cfma(__ldg(&cl[i * 4 + kk]), __ldg(&ch[kk * 4 + j]), s);
+      csm[b * E + c] = s;
+    }
+    // X of tile k written (and C of tile k visible)
+    bar_sync(kBarXFull + b, kThreads);
+    const double2 *x1 = xbuf + 2 * b * 64 * E, *x2 = x1 + 64 * E;
+    const double2 *cc = csm + b * E;
+    // Z partial: row `row` of M1(a) X1(a); G row += X1(a) row C; F row += C row X2(a)
+    double2 p[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) p[j] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+      const double2 xk = x1[xslot(a, row * 4 + kk)], ck = cc[row * 4 + kk];
+      const double2 mk = msm[mslot(a, row * 4 + kk)];  // M1(a) entry (row, kk)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        p[j] = cfma(mk, x1[xslot(a, kk * 4 + j)], p[j]);
+        g[j] = cfma(xk, cc[kk * 4 + j], g[j]);
+        f[j] = cfma(ck, x2[xslot(a, kk * 4 + j)], f[j]);
+      }
+    }
+    if (k + 2 < my_tiles) bar_arrive(kBarXEmpty + b, kThreads);
+    // Z partial summed over a's bits 0..2 (lane bits 2..4): a butterfly that
+    // halves the entries a lane keeps at lane bits 2 and 3 (which end as the
+    // entry's column bits 1 and 0), then a plain sum over lane bit 4
+#pragma unroll
+    for (int lv = 0; lv < 2; ++lv) {
+      const int h = 2 >> lv;
+      const bool up = (lane >> (2 + lv)) & 1;
+#pragma unroll
+      for (int e = 0; e < h; ++e) {
+        const double2 send = up ? p[e] : p[e + h];
+        const double2 keep = up ? p[e + h] : p[e];
+        p[e] = cadd(keep, shfl_xor2(send, 4 << lv));
+      }
+    }
+    p[0] = cadd(p[0], shfl_xor2(p[0], 16));
+    if (lane < 16) zp[cw * E + row * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 3) & 1)] = p[0];
+    bar_sync(kBarCons, kFp64Threads);
+    if (c < E) {
+      double2 z = zp[c];
+#pragma unroll
+      for (int w = 1; w < 8; ++w) z = cadd(z, zp[w * E + c]);
+      Q.zt[tile * E + c] = z;
+    }
+  }
+  double2 *rec = Q.partials + static_cast<size_t>(blockIdx.x) * 2 * 64 * E + a * E + row * 4;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    rec[j] = g[j];
+    rec[64 * E + j] = f[j];
+  }
+}
+
 // Y(lo) = sum_hi CosHi(hi) Z(lo, hi)   (blocks 0 .. 2^m1 - 1)
 // Y'(hi) = sum_lo Z(lo, hi) CosLo(lo)  (blocks 2^m1 .. 2^m1 + 2^m2 - 1)
 template <int D>
@@ -631,12 +886,17 @@ __global__ void __launch_bounds__(64) mps_finalize_kernel(const MpsParams Q, dou
 
 template <int D>
 cudaError_t launch_grad_d(const MpsParams &Q, const double2 *lam, int gather, int grid, cudaStream_t s) {
-  static std::atomic<unsigned long long> configured{0};
-  {
+  if constexpr (D == 4) {
+    static std::atomic<unsigned long long> configured{0};
+    const cudaError_t e = set_smem_limit_once(mps_grad4_kernel, mg4::kSmem, configured);
+    if (e != cudaSuccess) return e;
+    mps_grad4_kernel<<<grid, mg4::kThreads, mg4::kSmem, s>>>(Q, lam, gather);
+  } else {
+    static std::atomic<unsigned long long> configured{0};
     const cudaError_t e = set_smem_limit_once(mps_grad_kernel<D>, mps_grad_smem<D>(), configured);
     if (e != cudaSuccess) return e;
+    mps_grad_kernel<D><<<grid, kMpsThreads, mps_grad_smem<D>(), s>>>(Q, lam, gather);
   }
-  mps_grad_kernel<D><<<grid, kMpsThreads, mps_grad_smem<D>(), s>>>(Q, lam, gather);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   mps_coset_kernel<D><<<(1 << Q.m1) + (1 << Q.m2), 64, 0, s>>>(Q);
