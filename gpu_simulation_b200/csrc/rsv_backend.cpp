@@ -847,8 +847,13 @@ struct rsv_backend {
   rsv::Plan plan;
   rsv::DevBuf<double2> states;  // plan.num_bufs state buffers of state_len amplitudes each
   int backward_mode = RSV_BACKWARD_AUTO;
-  // RSV_KERNELS_* flags (rsv_set_kernels): TMA-fed backward passes where eligible
-  int kernel_flags = RSV_KERNELS_TMA;
+  // RSV_KERNELS_* flags (rsv_set_kernels): TMA-fed backward passes where
+  // eligible, the field terms on the tile of the last layer's first backward
+  // pass applied by that pass in energy_and_grad calls
+  int kernel_flags = RSV_KERNELS_TMA | RSV_KERNELS_FUSED_ENERGY;
+  int energy_fuse_pass = -1;                      // that pass's step index, or -1
+  int energy_fuse_grid = 0;                       // its grid (= its energy partials)
+  std::vector<unsigned long long> energy_rest;    // the other field-term masks
   int force_c = 0;  // contiguous low bits of the high tiles (0: the planner's choice)
   std::string tune_report;  // the last rsv_autotune's candidates and choice
   std::vector<rsv::TmaPass> tma;    // per backward step (used where step.kernel is kKernelTma)
@@ -1075,8 +1080,22 @@ void run_forward(rsv_backend *B, cudaStream_t st) {
   }
 }
 
-void run_energy(rsv_backend *B, cudaStream_t st) {
+// Whether the call's backward applies the field terms on its first pass's
+// tile (then the energy kernel applies the others): energy_and_grad calls of
+// a plan with such a pass.
+bool fused_energy(const rsv_backend *B, bool grad) { return grad && B->energy_fuse_pass >= 0; }
+
+void run_energy(rsv_backend *B, cudaStream_t st, bool fused) {
   const double bytes = 2.0 * 16.0 * static_cast<double>(u64{1} << B->n);
+  if (fused) {
+    timed(B, st, 2, bytes, [&] {
+      check(launch_energy_masks(state_buf(B, B->plan.chi_buf), state_buf(B, B->plan.mu_buf), B->n, B->field,
+                                u64{1} << B->n, B->energy_rest.data(), static_cast<int>(B->energy_rest.size()),
+                                B->energy_partials.p, B->energy_grid, st),
+            "energy launch");
+    });
+    return;
+  }
   timed(B, st, 2, bytes, [&] {
     check(launch_energy(state_buf(B, B->plan.chi_buf), state_buf(B, B->plan.mu_buf), B->n, B->field,
                         u64{1} << B->n, B->energy_partials.p, B->energy_grid, B->sms, st),
@@ -1095,14 +1114,19 @@ Layer0Params layer0_params(rsv_backend *B) {
   return Q;
 }
 
-void run_backward(rsv_backend *B, cudaStream_t st) {
+// fused: the energy kernel left the field terms of pass energy_fuse_pass to it
+void run_backward(rsv_backend *B, cudaStream_t st, bool fused) {
   PassParams P;
   for (size_t i = 0; i < B->plan.bwd.size(); ++i) {
     const Step &s = B->plan.bwd[i];
     fill_pass_params(B, s, P);
     if (s.kernel == kKernelTma) {
+      TmaPass T = B->tma[i];
+      if (!fused || static_cast<int>(i) != B->energy_fuse_pass) T.energy_terms = 0;
+      T.efield = B->field;
+      T.energy_partials = B->energy_partials.p + B->energy_grid;
       timed(B, st, 3, pass_bytes(B, s),
-            [&] { check(launch_bwd_tma(P, B->tma[i], s.grid, st), "backward TMA pass launch"); });
+            [&] { check(launch_bwd_tma(P, T, s.grid, st), "backward TMA pass launch"); });
       continue;
     }
     timed(B, st, 3, pass_bytes(B, s),
@@ -1124,11 +1148,11 @@ void run_backward(rsv_backend *B, cudaStream_t st) {
 }
 
 void run_finalize(rsv_backend *B, bool grad, double *energy_out, double *grad_out,
-                  cudaStream_t st) {
+                  cudaStream_t st, bool fused = false) {
   FinalizeParams F{};
   F.n = B->n;
   F.L = B->L;
-  F.num_energy_partials = B->energy_grid;
+  F.num_energy_partials = B->energy_grid + (fused ? B->energy_fuse_grid : 0);
   F.energy_partials = B->energy_partials.p;
   F.pass_partials = B->pass_partials.p;
   F.max_grid = B->plan.max_grid;
@@ -1228,9 +1252,10 @@ void run_all(rsv_backend *B, bool grad, double *energy_out, double *grad_out, cu
   }
   launch_prep(B, st);
   run_forward(B, st);
-  run_energy(B, st);
-  if (grad) run_backward(B, st);
-  run_finalize(B, grad, energy_out, grad_out, st);
+  const bool fused = fused_energy(B, grad);
+  run_energy(B, st, fused);
+  if (grad) run_backward(B, st, fused);
+  run_finalize(B, grad, energy_out, grad_out, st, fused);
 }
 
 // After a synchronised call: a NaN energy from a backend with TMA passes may
@@ -1605,6 +1630,56 @@ rsv_status run_in_workspace(int n, int L, double field, const double *d_params, 
 // their tensor maps are encoded here, once per plan, over the backend's own
 // state buffers.  A pass whose maps the driver rejects keeps its default
 // kernel.  Two CTAs per SM.
+// The field terms of H' (index masks P^-1(e_w)) that lie inside the tile of
+// the last layer's first backward pass go to that pass when it is a TMA phase
+// pass reading the final state chi as its psi and mu as its lambda (the
+// checkpoint schedule): it adds them to lambda before any of its rotations,
+// so its gradient sums see the whole lambda.  The energy kernel then applies
+// the diagonal and the remaining masks in one grid-stride launch.
+void assign_energy_fusion(rsv_backend *B) {
+  B->energy_fuse_pass = -1;
+  B->energy_fuse_grid = 0;
+  B->energy_rest.clear();
+  if (!(B->kernel_flags & RSV_KERNELS_FUSED_ENERGY) || B->plan.bwd.empty() || B->n < energy_split_qubits()) return;
+  const Step &s = B->plan.bwd[0];
+  TmaPass &T = B->tma[0];
+  if (s.kernel != kKernelTma || T.kind != kTmaHalf || !s.phase || s.layer != B->L - 1 || !s.tile.unit) return;
+  if (s.psi_in != B->plan.chi_buf || s.psi_load != kLoadNatural) return;
+  if (s.lam_in != B->plan.mu_buf || s.lam_load != kLoadNatural) return;
+  u64 span = 0;
+  for (int b = 0; b < s.tile.dims; ++b) span |= s.tile.vec[b];
+  std::vector<unsigned> inside;  // the masks inside the tile, in tile bits
+  for (int w = 0; w < B->n; ++w) {
+    const u64 m = ring_pinv(u64{1} << w, B->n);
+    if ((m & ~span) != 0) {
+      B->energy_rest.push_back(m);
+      continue;
+    }
+    unsigned tm = 0;
+    for (int b = 0; b < s.tile.dims; ++b)
+      if (m & s.tile.vec[b]) tm |= 1u << b;
+    inside.push_back(tm);
+  }
+  // the kernel applies the set tma_energy_mask(U, .) of one of its shapes
+  std::sort(inside.begin(), inside.end());
+  int shape = -1;
+  for (int u = 0; u <= kTmaMaxEnergyU && shape < 0; ++u) {
+    std::vector<unsigned> want;
+    for (int j = 0; j < kTmaNumEnergyMasks; ++j) want.push_back(tma_energy_mask(u, j));
+    std::sort(want.begin(), want.end());
+    if (inside == want) shape = u;
+  }
+  if (shape < 0) {
+    B->energy_rest.clear();
+    return;
+  }
+  T.energy_terms = 1 + shape;
+  B->energy_fuse_pass = 0;
+  B->energy_fuse_grid = s.grid;
+  if (static_cast<size_t>(B->energy_grid + s.grid) > B->energy_partials.count)
+    throw Error(RSV_ERR_INTERNAL, "energy partials too small for the fused energy");
+}
+
 void assign_backward_kernels(rsv_backend *B) {
   B->tma.assign(B->plan.bwd.size(), TmaPass{});
   B->tma_passes = 0;
@@ -1625,6 +1700,7 @@ void assign_backward_kernels(rsv_backend *B) {
     if (s.grid > B->plan.max_grid) throw Error(RSV_ERR_INTERNAL, "TMA pass grid exceeds the partial records");
     ++B->tma_passes;
   }
+  assign_energy_fusion(B);
 }
 
 // (Re)plan a backend for a backward schedule and allocate what depends on the
@@ -1694,7 +1770,8 @@ void setup_plan(rsv_backend *B, int mode) {
 // cpp/ising_cuda_rotation_kernels.cu:562-575) by measurements.
 // ------------------------------------------------------------------------
 struct TuneChoice {
-  int mode = RSV_BACKWARD_AUTO, analytic = kDefaultAnalyticLayers, kernels = RSV_KERNELS_TMA, force_c = 0;
+  int mode = RSV_BACKWARD_AUTO, analytic = kDefaultAnalyticLayers;
+  int kernels = RSV_KERNELS_TMA | RSV_KERNELS_FUSED_ENERGY, force_c = 0;
   double ms = 0.0;
 };
 
@@ -1719,6 +1796,7 @@ std::string choice_str(const rsv_backend *B, const TuneChoice &c) {
   std::ostringstream os;
   os << "mode=" << (B->plan.checkpoint ? "checkpoint" : "uncompute") << " analytic_layers=" << c.analytic
      << " tma=" << ((c.kernels & RSV_KERNELS_TMA) ? 1 : 0) << " tma_passes=" << B->tma_passes
+     << " fused_energy=" << (B->energy_fuse_pass >= 0 ? 1 : 0)
      << " high_tile_c=" << (c.force_c ? std::to_string(c.force_c) : std::string("planner"));
   return os.str();
 }
@@ -1746,7 +1824,8 @@ double time_plan(rsv_backend *B, const double *d_params, int repeats, cudaStream
 }
 
 // The candidates: both backward schedules (checkpoint only where it fits),
-// three or two analytic leading layers, the TMA kernels on or off, and every
+// three or two analytic leading layers, the TMA kernels on (with or without
+// the fused energy) or off, and every
 // contiguous run length c of the high tiles that gives the fewest passes.
 std::vector<TuneChoice> tune_candidates(const rsv_backend *B) {
   std::vector<TuneChoice> out;
@@ -1762,7 +1841,7 @@ std::vector<TuneChoice> tune_candidates(const rsv_backend *B) {
   for (int an : analytic)
     for (int c : cs)
       for (int mode : {RSV_BACKWARD_CHECKPOINT, RSV_BACKWARD_UNCOMPUTE})
-        for (int k : {RSV_KERNELS_TMA, 0}) {
+        for (int k : {RSV_KERNELS_TMA | RSV_KERNELS_FUSED_ENERGY, RSV_KERNELS_TMA, 0}) {
           if (mode == RSV_BACKWARD_CHECKPOINT && !checkpoint_fits(B->n, B->L, an, c)) continue;
           TuneChoice t;
           t.mode = mode;
@@ -1856,6 +1935,9 @@ rsv_status rsv_create(int num_qubits, int num_layers, double field, const char *
       check(configure_pass_kernels(), "configure pass kernels");
       configured = true;
     }
+    // energy partials before the plan: a fused energy adds a pass's share
+    B->energy_grid = energy_grid_size(num_qubits, B->sms);
+    B->energy_partials.alloc(static_cast<size_t>(B->energy_grid) + 2 * static_cast<size_t>(std::max(1, B->sms)));
     setup_plan(B.get(), RSV_BACKWARD_AUTO);
     const size_t nl = static_cast<size_t>(num_qubits) * num_layers;
     if (strat == "dense_scan") {
@@ -1869,8 +1951,6 @@ rsv_status rsv_create(int num_qubits, int num_layers, double field, const char *
     }
     B->coef.alloc(nl);
     B->ptab.alloc(static_cast<size_t>(num_layers) * 1024);
-    B->energy_grid = energy_grid_size(num_qubits, B->sms);
-    B->energy_partials.alloc(B->energy_grid);
     B->outputs.alloc(1 + B->num_params);
     B->rot.alloc(nl);
     B->lscale.alloc(num_layers);
@@ -1954,7 +2034,7 @@ rsv_status rsv_backward_device(rsv_backend *B, unsigned long long generation,
       throw Error(RSV_ERR_STALE_STATE,
                   "backward needs the state of the matching forward; the backend ran another call since");
     cudaStream_t st = device_stream(stream);
-    run_backward(B, st);
+    run_backward(B, st, false);  // the forward call computed the whole energy
     // energy is rewritten with the same value into the outputs scratch slot
     run_finalize(B, true, B->outputs.p, d_gradient_out, st);
     B->forward_only_state = false;
@@ -1995,11 +2075,12 @@ rsv_status rsv_profile_energy_and_grad(rsv_backend *B, const double *params, siz
       cudaEventRecord(ev[1], st);
       run_forward(B, st);
       cudaEventRecord(ev[2], st);
-      run_energy(B, st);
+      const bool fused = fused_energy(B, grad);
+      run_energy(B, st, fused);
       cudaEventRecord(ev[3], st);
-      if (grad) run_backward(B, st);
+      if (grad) run_backward(B, st, fused);
       cudaEventRecord(ev[4], st);
-      run_finalize(B, grad, B->outputs.p, B->outputs.p + 1, st);
+      run_finalize(B, grad, B->outputs.p, B->outputs.p + 1, st, fused);
     }
     const size_t count = grad ? 1 + B->num_params : 1;
     check(cudaMemcpyAsync(B->out_host.p, B->outputs.p, count * sizeof(double),
@@ -2130,7 +2211,7 @@ rsv_status rsv_set_analytic_layers(rsv_backend *B, int max_layers) {
 rsv_status rsv_set_kernels(rsv_backend *B, int flags) {
   return guarded([&] {
     if (B == nullptr) invalid("backend is null");
-    if ((flags & ~RSV_KERNELS_TMA) != 0) invalid("unknown kernel flags");
+    if ((flags & ~(RSV_KERNELS_TMA | RSV_KERNELS_FUSED_ENERGY)) != 0) invalid("unknown kernel flags");
     check(cudaStreamSynchronize(B->stream), "backend synchronize");
     B->kernel_flags = flags;
     setup_plan(B, B->backward_mode);
@@ -2217,8 +2298,12 @@ rsv_status rsv_describe_backend(rsv_backend *B, char *buf, size_t buf_size, size
     std::ostringstream os;
     os << "analytic_layers=" << B->analytic_layers << " kernels=" << B->kernel_flags
        << " high_tile_c=" << (B->force_c ? std::to_string(B->force_c) : std::string("planner"))
-       << " tma_passes=" << B->tma_passes << "\n"
-       << describe(B->plan);
+       << " tma_passes=" << B->tma_passes;
+    if (B->energy_fuse_pass >= 0)
+      os << " fused_energy: backward pass " << B->energy_fuse_pass << " applies "
+         << kTmaNumEnergyMasks << " field terms, the energy kernel "
+         << B->energy_rest.size();
+    os << "\n" << describe(B->plan);
     if (!B->tune_report.empty()) os << "autotune:\n" << B->tune_report;
     const std::string s = os.str();
     if (length_out) *length_out = s.size();

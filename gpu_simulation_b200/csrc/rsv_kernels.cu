@@ -230,6 +230,22 @@ __global__ void __launch_bounds__(THREADS) energy_kernel(const double2 *__restri
   }
 }
 
+// the grid-stride kernel on 1024-thread CTAs without a tile kernel before it
+template <int K>
+cudaError_t launch_energy_masks_k(int count, int grid, cudaStream_t s, const double2 *chi, double2 *mu, int n,
+                                  double field, u64 size, const EnergyMasks &M, double *partials) {
+  if (count == K) {
+    energy_kernel<K, kEnergySplitThreads><<<grid, kEnergySplitThreads, 0, s>>>(chi, mu, n, field, size, M, 0,
+                                                                               partials);
+    return cudaGetLastError();
+  }
+  if constexpr (K < kMaxQubits) {
+    return launch_energy_masks_k<K + 1>(count, grid, s, chi, mu, n, field, size, M, partials);
+  } else {
+    return cudaErrorInvalidValue;
+  }
+}
+
 template <int K>
 cudaError_t launch_energy_k(int count, int grid, cudaStream_t s, const double2 *chi, double2 *mu, int n,
                             double field, u64 size, const EnergyMasks &M, int with_mu_in, double *partials) {
@@ -438,6 +454,17 @@ cudaError_t launch_energy(const double2 *chi, double2 *mu, int n, double field, 
   if (e != cudaSuccess) return e;
   return launch_energy_k<1>(count, grid, s, chi, mu, n, field, size, M, 1, partials);
 }
+
+cudaError_t launch_energy_masks(const double2 *chi, double2 *mu, int n, double field, u64 size,
+                                const unsigned long long *masks, int count, double *partials, int grid,
+                                cudaStream_t s) {
+  if (n < kEnergySplitQubits || n > kMaxQubits || count < 1 || count > n) return cudaErrorInvalidValue;
+  EnergyMasks M{};
+  for (int j = 0; j < count; ++j) M.m[j] = masks[j];
+  return launch_energy_masks_k<1>(count, grid, s, chi, mu, n, field, size, M, partials);
+}
+
+int energy_split_qubits() { return kEnergySplitQubits; }
 
 int energy_kernel_count(int n) { return n < kEnergySplitQubits ? 1 : 2; }
 

@@ -43,6 +43,15 @@ cudaError_t launch_bwd_half(const PassParams &P, int grid, cudaStream_t s);
 // shared-memory tile kernel takes the masks on the top index bits first
 cudaError_t launch_energy(const double2 *chi, double2 *mu, int n, double field,
                           unsigned long long size, double *partials, int grid, int sms, cudaStream_t s);
+// mu = (diagonal - field * sum over the given index masks) chi, with per-CTA
+// energy partials ([grid], grid = energy_grid_size): the energy kernel of an
+// energy_and_grad call whose first backward pass applies the other field
+// terms (count <= n masks, n >= kEnergySplitQubits)
+cudaError_t launch_energy_masks(const double2 *chi, double2 *mu, int n, double field, unsigned long long size,
+                                const unsigned long long *masks, int count, double *partials, int grid,
+                                cudaStream_t s);
+// qubits from which the energy is split (tile kernel + grid-stride kernel)
+int energy_split_qubits();
 // kernels launch_energy launches for n qubits (1, or 2 for the split energy)
 int energy_kernel_count(int n);
 // CTAs of the energy's grid-stride kernel (= its number of partials)

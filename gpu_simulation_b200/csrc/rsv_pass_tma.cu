@@ -229,6 +229,46 @@ __device__ __forceinline__ void gates_last(const PassParams &P, const double2 *k
   }
 }
 
+// Field terms of the tile, layout P: per register r the partner sum
+// s = sum_m psi(t ^ m) over the masks tma_energy_mask(U, .), then lambda[r] -= h s and the
+// energy share -h Re(conj(psi[r]) s) into e.  A mask's tile bits 7..10 are
+// register bits (XOR h = m >> 7) and its bits 0..6 (lo) lane and warp bits;
+// sw128 is linear over XOR and leaves bits 7..10 alone, so the partner of
+// register r is stage[(sw128(tP(r = 0)) ^ sw128(lo)) + ((r ^ h) << 7)]: one base
+// per mask, compile-time offsets; masks on register bits only take the
+// partner from the thread's own registers.
+template <int M>
+__device__ __forceinline__ double2 epartner(const double2 *stage, int s0, int r, const double2 (&a)[kR]) {
+  constexpr int lo = M & 0x7F, h = (M >> 7) & 15;
+  if constexpr (lo == 0) {
+    return a[r ^ h];
+  } else {
+    return stage[(s0 ^ sw128(lo)) + ((r ^ h) << 7)];
+  }
+}
+template <int U>
+__device__ __forceinline__ void emask_apply(double h, const double2 *stage, int lane, int warp,
+                                            const double2 (&a)[kR], double2 (&b)[kR], double &e) {
+  static_assert(kTmaNumEnergyMasks == 10, "the partner sum below lists the masks");
+  const int s0 = sw128(tP(lane, warp, 0));
+  double es = 0.0;  // sum of Re(conj(psi) s); times -h below
+#pragma unroll
+  for (int r = 0; r < kR; ++r) {
+    const double2 q[kTmaNumEnergyMasks] = {
+        epartner<tma_energy_mask(U, 0)>(stage, s0, r, a), epartner<tma_energy_mask(U, 1)>(stage, s0, r, a),
+        epartner<tma_energy_mask(U, 2)>(stage, s0, r, a), epartner<tma_energy_mask(U, 3)>(stage, s0, r, a),
+        epartner<tma_energy_mask(U, 4)>(stage, s0, r, a), epartner<tma_energy_mask(U, 5)>(stage, s0, r, a),
+        epartner<tma_energy_mask(U, 6)>(stage, s0, r, a), epartner<tma_energy_mask(U, 7)>(stage, s0, r, a),
+        epartner<tma_energy_mask(U, 8)>(stage, s0, r, a), epartner<tma_energy_mask(U, 9)>(stage, s0, r, a)};
+    double2 sum = q[0];
+#pragma unroll
+    for (int j = 1; j < kTmaNumEnergyMasks; ++j) sum = make_double2(sum.x + q[j].x, sum.y + q[j].y);
+    b[r] = make_double2(fma(-h, sum.x, b[r].x), fma(-h, sum.y, b[r].y));
+    es = fma(a[r].x, sum.x, fma(a[r].y, sum.y, es));
+  }
+  e = fma(-h, es, e);
+}
+
 // layout P -> layout Q of one vector through the warp's slice
 __device__ __forceinline__ void transpose_pq(double2 *xs, int lane, double2 (&a)[kR]) {
 #pragma unroll
@@ -308,6 +348,7 @@ __global__ void __launch_bounds__(tw::kThreads, 2)
 
   double *acc = acc_sm + tid;
   double *v = v_sm + tid;
+  double e_acc = 0.0;  // energy share of the terms this pass applies
   const u32 toffP = thread_offset(P, tP(lane, warp, 0));
   double2 *xs = obuf + warp * 512;  // the warp's transpose slice (inside the output buffer)
   int fail = 0;
@@ -325,6 +366,14 @@ __global__ void __launch_bounds__(tw::kThreads, 2)
       const int t = sw128(tP(lane, warp, r));
       a[r] = stage[t];
       b[r] = stage[kTile + t];
+    }
+    if (PHASE && T.energy_terms) {
+      switch (T.energy_terms - 1) {
+        case 0: emask_apply<0>(T.efield, stage, lane, warp, a, b, e_acc); break;
+        case 1: emask_apply<1>(T.efield, stage, lane, warp, a, b, e_acc); break;
+        case 2: emask_apply<2>(T.efield, stage, lane, warp, a, b, e_acc); break;
+        default: emask_apply<3>(T.efield, stage, lane, warp, a, b, e_acc); break;
+      }
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(sread);
@@ -424,6 +473,17 @@ __global__ void __launch_bounds__(tw::kThreads, 2)
     if (tid >= 3 && tid <= 10)
       for (int ww = 0; ww < kWarps; ++ww) s += red[ww][tid - 3];
     rec[tid] = s;
+  }
+  if (PHASE && T.energy_terms) {
+    const double es = warp_sum(e_acc);
+    __syncthreads();  // red is reused
+    if (lane == 0) red[warp][0] = es;
+    __syncthreads();
+    if (tid == 0) {
+      double s = 0.0;
+      for (int ww = 0; ww < kWarps; ++ww) s += red[ww][0];
+      T.energy_partials[blockIdx.x] = s;
+    }
   }
   if (PHASE) {
     __syncthreads();  // red is reused

@@ -36,7 +36,26 @@ struct alignas(64) TmaPass {
   unsigned int st_mask[kTmaRank];
   int *err;              // device flag: set when a pipeline wait gives up
   int kind;              // kTmaHalf or kTmaLow
+  // Field terms applied by the layer's first (phase) pass, set per call
+  // (energy_terms = 0: none; 1 + U: the masks tma_energy_mask(U, j), j < 10,
+  // in tile bits): lambda += -efield * sum_m psi(t ^ m) for every tile index t
+  // (psi is the final state chi there), and the CTA's share
+  // -efield * sum_t Re(conj(psi(t)) sum_m psi(t ^ m)) of the energy goes to
+  // energy_partials[blockIdx.x].
+  int energy_terms;
+  double efield;
+  double *energy_partials;
 };
+
+// The field terms P^-1(e_w) inside an 11-bit phase-pass tile whose tile bits
+// 0..2+U are index bits 0..2+U (ungated) and tile bits 3+U..10 the top index
+// bits (gated), U = 0..3: the adjacent pairs inside each run (e_w + e_{w+1})
+// and the last wire's e_{n-1} + e_0 + e_1; ten masks for every U, in tile bits.
+constexpr int kTmaNumEnergyMasks = 10;
+constexpr int kTmaMaxEnergyU = 3;
+__host__ __device__ constexpr unsigned tma_energy_mask(int u, int j) {
+  return j == 9 ? 0x403u : (3u << (j < 2 + u ? j : j + 1));
+}
 
 // Whether a backward pass has the shape and load/store variant of a TMA
 // kernel: psi and lambda loaded in natural order, lambda stored in natural

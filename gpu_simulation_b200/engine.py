@@ -153,15 +153,22 @@ class Engine:
         check(self._lib.rsv_analytic_layers(self._h, ctypes.byref(m), ctypes.byref(u)))
         return {"max_layers": m.value, "used": u.value}
 
-    def set_kernels(self, tma: bool = True) -> None:
-        """Backward passes on the TMA-fed kernel where eligible (default) or
-        all on the cp.async kernels; re-plans the backend."""
-        check(self._lib.rsv_set_kernels(self._h, 1 if tma else 0))
+    KERNELS_TMA = 1
+    KERNELS_FUSED_ENERGY = 2
+
+    def set_kernels(self, tma: bool = True, fused_energy: bool = True) -> None:
+        """Backward passes on the TMA-fed kernels where eligible (default) or
+        all on the cp.async kernels; with the TMA kernels, fused_energy lets
+        the last layer's first backward pass apply the field terms on its
+        tile in energy_and_grad calls.  Re-plans the backend."""
+        flags = (self.KERNELS_TMA | (self.KERNELS_FUSED_ENERGY if fused_energy else 0)) if tma else 0
+        check(self._lib.rsv_set_kernels(self._h, flags))
 
     def kernels(self) -> dict:
         f, t = ctypes.c_int(), ctypes.c_int()
         check(self._lib.rsv_kernels(self._h, ctypes.byref(f), ctypes.byref(t)))
-        return {"tma": bool(f.value & 1), "tma_passes": t.value}
+        return {"tma": bool(f.value & self.KERNELS_TMA), "fused_energy": bool(f.value & self.KERNELS_FUSED_ENERGY),
+                "tma_passes": t.value}
 
     def autotune(self, params, repeats: int = 3, force: bool = False) -> str:
         """Time the plan candidates on these parameters (host array or CUDA

@@ -230,24 +230,32 @@ rsv_status rsv_set_analytic_layers(rsv_backend *backend, int max_layers);
 rsv_status rsv_analytic_layers(rsv_backend *backend, int *max_layers_out, int *used_out);
 
 /*
- * Kernel selection.  With RSV_KERNELS_TMA (the default) the backward passes on
- * 11-bit tiles whose psi comes from a forward checkpoint and whose lambda is
- * updated in place run on the TMA-fed kernel
- * (gpu_simulation_b200/csrc/rsv_pass_tma.cu): a producer warp streams psi and
- * lambda into a two-stage shared-memory ring with tensor copies and writes
- * lambda back with tensor stores, four consumer warps rotate; mbarriers are
- * the only synchronisation.  Its tensor maps are encoded when the backend is
- * planned; a pass the driver cannot map keeps the cp.async kernel.  Flags 0
- * keeps every pass on the cp.async kernels.  Results agree to rounding.
- * rsv_set_kernels re-plans (synchronises the backend's stream); rsv_kernels
- * reports the flags and how many backward passes of the plan are on the TMA
- * kernel.  If a TMA pass ever gives up waiting for its pipeline (after 1.5 s),
- * the call's energy and gradient are NaN and the synchronous entry points
- * return RSV_ERR_CUDA.  No reference counterpart (the reference's backward
- * kernels, cpp/ising_cuda_statevector_grad_kernels.cu:683-1326, stage with
- * cuda::memcpy_async).
+ * Kernel selection (flags, default RSV_KERNELS_TMA | RSV_KERNELS_FUSED_ENERGY).
+ * RSV_KERNELS_TMA: the backward passes on 11-bit tiles whose psi comes from a
+ * forward checkpoint and whose lambda is updated in place, and the 12-wire low
+ * pass, run on the TMA-fed kernels (gpu_simulation_b200/csrc/rsv_pass_tma.cu):
+ * psi and lambda arrive by tensor copies into a swizzled shared-memory stage,
+ * lambda leaves by a tensor store, and the warps of a block synchronise only
+ * through split-phase mbarriers.  Their tensor maps are encoded when the
+ * backend is planned; a pass the driver cannot map keeps the cp.async kernel.
+ * RSV_KERNELS_FUSED_ENERGY (with RSV_KERNELS_TMA): in energy_and_grad calls,
+ * the field terms of H whose index masks lie inside the tile of the last
+ * layer's first backward pass are applied by that pass, which reads the final
+ * state anyway; the energy kernel applies the diagonal and the other field
+ * terms in one launch.  Energy-only calls (and rsv_forward_device) keep the
+ * full energy kernels.  Flags 0 keeps every pass on the cp.async kernels.
+ * Results agree to rounding.  rsv_set_kernels re-plans (synchronises the
+ * backend's stream); rsv_kernels reports the flags and how many backward
+ * passes of the plan are on the TMA kernels.  If a TMA pass ever gives up
+ * waiting for its pipeline (after 1.5 s), the call's energy and gradient are
+ * NaN and the synchronous entry points return RSV_ERR_CUDA.  No reference
+ * counterpart (the reference's backward kernels,
+ * cpp/ising_cuda_statevector_grad_kernels.cu:683-1326, stage with
+ * cuda::memcpy_async; its energy is a separate kernel,
+ * cpp/ising_cuda_kernels.cu:313-358).
  */
 #define RSV_KERNELS_TMA 1
+#define RSV_KERNELS_FUSED_ENERGY 2
 rsv_status rsv_set_kernels(rsv_backend *backend, int flags);
 rsv_status rsv_kernels(rsv_backend *backend, int *flags_out, int *tma_passes_out);
 

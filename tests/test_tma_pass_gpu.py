@@ -66,3 +66,37 @@ def test_tma_passes_match_reference(n, L, h):
     e, g = _both_kernels(n, L, h, p)
     assert abs(e - e_ref) < 1e-10
     np.testing.assert_allclose(g, g_ref, atol=1e-10, rtol=0)
+
+
+@pytest.mark.parametrize("n,L,h", [(23, 4, 0.8), (24, 4, 1.0), (28, 4, 1.0)])
+def test_fused_energy_matches_separate_energy(n, L, h):
+    """The last layer's first backward pass applies the field terms on its tile
+    (default): energy and gradient equal the separate energy kernels' to
+    rounding; energy-only calls and the forward/backward device split keep the
+    whole energy kernel and agree too."""
+    import torch
+
+    from gpu_simulation_b200 import ring_ising_energy
+
+    p = np.random.default_rng(1300 + n + L).uniform(0, 2 * np.pi, 2 * n * L)
+    eng = Engine(n, L, h)
+    try:
+        k = eng.kernels()
+        assert k["tma"] and k["fused_energy"], k
+        assert "fused_energy: backward pass 0 applies" in eng.describe()
+        e1, g1 = eng.energy_and_grad(p)
+        e1b, g1b = eng.energy_and_grad(p)
+        e_only = eng.energy(p)
+        t = torch.tensor(p, device="cuda", requires_grad=True)
+        e_ad = ring_ising_energy(t, eng)
+        e_ad.backward()
+        g_ad = t.grad.cpu().numpy()
+        eng.set_kernels(tma=True, fused_energy=False)
+        assert "fused_energy" not in eng.describe().splitlines()[0]
+        e0, g0 = eng.energy_and_grad(p)
+    finally:
+        eng.close()
+    assert e1 == e1b and np.array_equal(g1, g1b)
+    assert abs(e1 - e0) < 1e-12 and abs(e_only - e0) < 1e-12 and abs(float(e_ad) - e0) < 1e-12
+    np.testing.assert_allclose(g1, g0, atol=1e-12, rtol=0)
+    np.testing.assert_allclose(g_ad, g0, atol=1e-12, rtol=0)
