@@ -581,8 +581,11 @@ def main():
 
     peak, peak_src = measured_peaks()
     KERNEL_NAMES = {
-        "backward_pass": "backward (bwd_pass_kernel 12-bit tiles, bwd_half_kernel 11-bit tiles, mps_grad_kernel)",
-        "forward_pass": "fwd_pass_kernel + mps_fwd_kernel", "energy": "energy_tile_kernel + energy_kernel",
+        "backward_pass": "backward: bwd_tma_kernel<1> (phase pass, with the field terms of its tile), "
+                         "bwd_tma_kernel<0>, bwd_tma_low_kernel, mps_grad4_kernel (+ its two small reductions)",
+        "forward_pass": "fwd_pass_kernel (the first one evaluating the bond-4 matrix-product state)",
+        "energy": "energy_kernel (diagonal and the field terms off the phase pass's tile; "
+                  "energy_tile_kernel + energy_kernel without the fused energy)",
     }
     kernels_launched = int(stats.pop("kernels_launched"))
     kinds = {k: v for k, v in stats.items() if v["launches"]}

@@ -2265,7 +2265,7 @@ rsv_status rsv_autotune(rsv_backend *B, const double *d_params, size_t num_param
         continue;
       }
       // the same launches under another name are timed once
-      std::string sig = describe(B->plan);
+      std::string sig = describe(B->plan) + " fused_energy=" + std::to_string(B->energy_fuse_pass);
       if (std::find(seen.begin(), seen.end(), sig) != seen.end()) continue;
       seen.push_back(sig);
       c.ms = time_plan(B, d_params, repeats, st);
