@@ -853,6 +853,13 @@ struct rsv_backend {
   int kernel_flags = RSV_KERNELS_TMA | RSV_KERNELS_FUSED_ENERGY;
   int energy_fuse_pass = -1;                      // that pass's step index, or -1
   int energy_fuse_grid = 0;                       // its grid (= its energy partials)
+  // the layer's middle pass applying the field terms of its gated wires (phase
+  // table per call from defer_args), or -1
+  int energy_defer_pass = -1;
+  int energy_defer_grid = 0;
+  unsigned int energy_defer_wires = 0;            // its gated wires (their phi from that pass)
+  rsv::DeferPhaseArgs defer_args{};
+  rsv::DevBuf<double2> defer_phase;               // [kTmaDeferTable]
   std::vector<unsigned long long> energy_rest;    // the other field-term masks
   int force_c = 0;  // contiguous low bits of the high tiles (0: the planner's choice)
   std::string tune_report;  // the last rsv_autotune's candidates and choice
@@ -1123,8 +1130,10 @@ void run_backward(rsv_backend *B, cudaStream_t st, bool fused) {
     if (s.kernel == kKernelTma) {
       TmaPass T = B->tma[i];
       if (!fused || static_cast<int>(i) != B->energy_fuse_pass) T.energy_terms = 0;
+      if (!fused || static_cast<int>(i) != B->energy_defer_pass) T.defer_terms = 0;
       T.efield = B->field;
-      T.energy_partials = B->energy_partials.p + B->energy_grid;
+      T.energy_partials = B->energy_partials.p + B->energy_grid +
+                          (static_cast<int>(i) == B->energy_defer_pass ? B->energy_fuse_grid : 0);
       timed(B, st, 3, pass_bytes(B, s),
             [&] { check(launch_bwd_tma(P, T, s.grid, st), "backward TMA pass launch"); });
       continue;
@@ -1152,7 +1161,13 @@ void run_finalize(rsv_backend *B, bool grad, double *energy_out, double *grad_ou
   FinalizeParams F{};
   F.n = B->n;
   F.L = B->L;
-  F.num_energy_partials = B->energy_grid + (fused ? B->energy_fuse_grid : 0);
+  F.num_energy_partials = B->energy_grid + (fused ? B->energy_fuse_grid + B->energy_defer_grid : 0);
+  F.phi_alt_layer = -1;
+  if (B->energy_defer_pass >= 0) {
+    F.phi_alt_layer = B->L - 1;
+    F.phi_alt_pass = B->plan.bwd[static_cast<size_t>(B->energy_defer_pass)].pass_index;
+    F.phi_alt_wires = B->energy_defer_wires;
+  }
   F.energy_partials = B->energy_partials.p;
   F.pass_partials = B->pass_partials.p;
   F.max_grid = B->plan.max_grid;
@@ -1211,6 +1226,12 @@ void launch_prep(rsv_backend *B, cudaStream_t st) {
                      B->gscale.p, st),
           "rot launch");
   });
+  if (B->energy_defer_pass >= 0) {
+    DeferPhaseArgs A = B->defer_args;
+    A.coef = B->coef.p;
+    A.field = B->field;
+    timed(B, st, 0, 0.0, [&] { check(launch_defer_phase(A, B->defer_phase.p, st), "phase table launch"); });
+  }
 }
 
 // Gate-level path: RY, RZ and CNOT as separate kernels and the inverse walk
@@ -1636,7 +1657,65 @@ rsv_status run_in_workspace(int n, int L, double field, const double *d_params, 
 // checkpoint schedule): it adds them to lambda before any of its rotations,
 // so its gradient sums see the whole lambda.  The energy kernel then applies
 // the diagonal and the remaining masks in one grid-stride launch.
+// The field terms on the adjacent pairs of the gated tile bits 3..10 of the
+// layer's second backward pass go to that pass when it is a TMA pass of that
+// shape (low run 0..2): it adds them to lambda at its start from the checkpoint
+// it reads, as the phased masks conj(D) X_m D (the layer's first pass undid the
+// RZ phases D), and takes the phi sums of its own wires there, whose lambda is
+// then complete (finalize reads those wires' phi from this pass, unscaled).
+void assign_energy_deferral(rsv_backend *B) {
+  if (B->plan.bwd.size() < 2 || B->energy_fuse_pass != 0) return;
+  const Step &s0 = B->plan.bwd[0];
+  const Step &s = B->plan.bwd[1];
+  TmaPass &T = B->tma[1];
+  if (s.kernel != kKernelTma || T.kind != kTmaHalf || s.phase || s.layer != B->L - 1 || !s.tile.unit) return;
+  if (s.tile.dims != 11 || s.lam_load != kLoadNatural || s.psi_load != kLoadNatural) return;
+  for (int b = 0; b < 3; ++b)
+    if (s.tile.vec[b] != (u64{1} << b) || s.tile.gate_wire[b] >= 0) return;
+  DeferPhaseArgs A{};
+  A.n = B->n;
+  A.layer = B->L - 1;
+  unsigned wires = 0;
+  for (int b = 3; b < 11; ++b) {
+    const int w = s.tile.gate_wire[b];
+    if (w < 0 || s.tile.vec[b] != (u64{1} << w)) return;  // gated wire w on index bit w
+    if (b > 3 && w != s.tile.gate_wire[b - 1] + 1) return;  // consecutive wires
+    wires |= 1u << w;
+  }
+  // the masks e_w + e_{w+1} of those pairs must be field terms the energy kernel has
+  std::vector<unsigned long long> rest;
+  int found = 0;
+  for (unsigned long long m : B->energy_rest) {
+    bool mine = false;
+    for (int j = 0; j < kTmaNumDeferredMasks; ++j)
+      if (m == (s.tile.vec[3 + j] | s.tile.vec[4 + j])) mine = true;
+    if (mine) ++found;
+    else rest.push_back(m);
+  }
+  if (found != kTmaNumDeferredMasks) return;
+  for (int j = 0; j < 8; ++j) A.wires[j] = s.tile.gate_wire[3 + j];
+  // pending tangent factors at this pass's start: every wire but the first pass's
+  unsigned first = 0;
+  for (int b = 0; b < s0.tile.dims; ++b)
+    if (s0.tile.gate_wire[b] >= 0) first |= 1u << s0.tile.gate_wire[b];
+  A.pending = ((B->n == 32 ? 0u : (1u << B->n)) - 1u) & ~first;
+  if (static_cast<size_t>(B->energy_grid + B->energy_fuse_grid + s.grid) > B->energy_partials.count)
+    throw Error(RSV_ERR_INTERNAL, "energy partials too small for the deferred field terms");
+  if (B->defer_phase.p == nullptr) B->defer_phase.alloc(kTmaDeferTable);
+  T.phi_only = 1;
+  T.defer_terms = 1;
+  T.emask_phase = B->defer_phase.p;
+  B->energy_rest = rest;
+  B->energy_defer_pass = 1;
+  B->energy_defer_grid = s.grid;
+  B->energy_defer_wires = wires;
+  B->defer_args = A;
+}
+
 void assign_energy_fusion(rsv_backend *B) {
+  B->energy_defer_pass = -1;
+  B->energy_defer_grid = 0;
+  B->energy_defer_wires = 0;
   B->energy_fuse_pass = -1;
   B->energy_fuse_grid = 0;
   B->energy_rest.clear();
@@ -1678,6 +1757,7 @@ void assign_energy_fusion(rsv_backend *B) {
   B->energy_fuse_grid = s.grid;
   if (static_cast<size_t>(B->energy_grid + s.grid) > B->energy_partials.count)
     throw Error(RSV_ERR_INTERNAL, "energy partials too small for the fused energy");
+  assign_energy_deferral(B);
 }
 
 void assign_backward_kernels(rsv_backend *B) {
@@ -1937,7 +2017,7 @@ rsv_status rsv_create(int num_qubits, int num_layers, double field, const char *
     }
     // energy partials before the plan: a fused energy adds a pass's share
     B->energy_grid = energy_grid_size(num_qubits, B->sms);
-    B->energy_partials.alloc(static_cast<size_t>(B->energy_grid) + 2 * static_cast<size_t>(std::max(1, B->sms)));
+    B->energy_partials.alloc(static_cast<size_t>(B->energy_grid) + 4 * static_cast<size_t>(std::max(1, B->sms)));
     setup_plan(B.get(), RSV_BACKWARD_AUTO);
     const size_t nl = static_cast<size_t>(num_qubits) * num_layers;
     if (strat == "dense_scan") {
@@ -2265,7 +2345,8 @@ rsv_status rsv_autotune(rsv_backend *B, const double *d_params, size_t num_param
         continue;
       }
       // the same launches under another name are timed once
-      std::string sig = describe(B->plan) + " fused_energy=" + std::to_string(B->energy_fuse_pass);
+      std::string sig = describe(B->plan) + " fused_energy=" + std::to_string(B->energy_fuse_pass) +
+                        std::to_string(B->energy_defer_pass);
       if (std::find(seen.begin(), seen.end(), sig) != seen.end()) continue;
       seen.push_back(sig);
       c.ms = time_plan(B, d_params, repeats, st);
@@ -2301,8 +2382,9 @@ rsv_status rsv_describe_backend(rsv_backend *B, char *buf, size_t buf_size, size
        << " tma_passes=" << B->tma_passes;
     if (B->energy_fuse_pass >= 0)
       os << " fused_energy: backward pass " << B->energy_fuse_pass << " applies "
-         << kTmaNumEnergyMasks << " field terms, the energy kernel "
-         << B->energy_rest.size();
+         << kTmaNumEnergyMasks << " field terms,"
+         << (B->energy_defer_pass >= 0 ? " backward pass 1 applies " + std::to_string(kTmaNumDeferredMasks) + "," : "")
+         << " the energy kernel " << B->energy_rest.size();
     os << "\n" << describe(B->plan);
     if (!B->tune_report.empty()) os << "autotune:\n" << B->tune_report;
     const std::string s = os.str();

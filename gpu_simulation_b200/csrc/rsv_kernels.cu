@@ -359,14 +359,15 @@ __global__ void finalize_kernel(const FinalizeParams F) {
       F.grad_out[2 * k] = s * F.gscale[2 * k];
     }
     {
-      const int pass = F.phi_pass[layer];
+      const bool alt = layer == F.phi_alt_layer && ((F.phi_alt_wires >> w) & 1u);
+      const int pass = alt ? F.phi_alt_pass : F.phi_pass[layer];
       const double *rec = F.pass_partials + static_cast<size_t>(pass) * F.max_grid * kPartialStride;
       double tot = 0.0, bw = 0.0;
       for (int c = 0; c < F.pass_grid[pass]; ++c) {
         tot += rec[static_cast<size_t>(c) * kPartialStride + kPartialTot];
         bw += rec[static_cast<size_t>(c) * kPartialStride + kPartialPhi + w];
       }
-      F.grad_out[2 * k + 1] = (tot - 2.0 * bw) * F.gscale[2 * k + 1];
+      F.grad_out[2 * k + 1] = (tot - 2.0 * bw) * (alt ? 1.0 : F.gscale[2 * k + 1]);
     }
   }
 }
@@ -473,6 +474,41 @@ int energy_grid_size(int n, int sms) {
   if (n >= kEnergySplitQubits)
     return static_cast<int>(std::min<u64>(std::max<u64>(1, size / kEnergySplitThreads), static_cast<u64>(sms) * 2));
   return static_cast<int>(std::min<u64>(std::max<u64>(1, size / kEnergyThreads), static_cast<u64>(sms) * 8));
+}
+
+// Phase table of the field terms a layer's middle pass applies
+// (TmaPass::emask_phase): entry 4 j + q = -h F^2 e^{i((1 - 2 b0) phi_a + (1 - 2 b1) phi_b)}
+// for the pair (a, b) = (wires[j], wires[j + 1]), q = b0 | b1 << 1 (the pair's
+// bits), F the product of the tangent factors of the wires in `pending`.
+// That is -h F^2 conj(D(t)) D(t ^ m) for the layer's RZ phases D.
+__global__ void defer_phase_kernel(const DeferPhaseArgs A, double2 *__restrict__ out) {
+  __shared__ double f2;
+  const int t = threadIdx.x;
+  if (t == 0) {
+    double p = 1.0;
+    for (int v = 0; v < A.n; ++v) {
+      if (!((A.pending >> v) & 1u)) continue;
+      const double4 k = A.coef[A.layer * A.n + v];
+      const double f = fabs(k.x) >= fabs(k.y) ? k.x : k.y;
+      p *= f * f;
+    }
+    f2 = p;
+  }
+  __syncthreads();
+  if (t >= 28) return;
+  const int j = t >> 2, b0 = t & 1, b1 = (t >> 1) & 1;
+  const double4 ka = A.coef[A.layer * A.n + A.wires[j]], kb = A.coef[A.layer * A.n + A.wires[j + 1]];
+  // e^{i phi} from (cos phi/2, sin phi/2); bit 1 conjugates
+  const double2 ea = make_double2(ka.z * ka.z - ka.w * ka.w, (b0 ? -2.0 : 2.0) * ka.z * ka.w);
+  const double2 eb = make_double2(kb.z * kb.z - kb.w * kb.w, (b1 ? -2.0 : 2.0) * kb.z * kb.w);
+  const double c = -A.field * f2;
+  const double2 e = cmul(ea, eb);
+  out[t] = make_double2(c * e.x, c * e.y);
+}
+
+cudaError_t launch_defer_phase(const DeferPhaseArgs &A, double2 *out, cudaStream_t s) {
+  defer_phase_kernel<<<1, 32, 0, s>>>(A, out);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_finalize(const FinalizeParams &F, cudaStream_t s) {

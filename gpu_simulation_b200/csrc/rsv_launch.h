@@ -50,6 +50,15 @@ cudaError_t launch_energy(const double2 *chi, double2 *mu, int n, double field,
 cudaError_t launch_energy_masks(const double2 *chi, double2 *mu, int n, double field, unsigned long long size,
                                 const unsigned long long *masks, int count, double *partials, int grid,
                                 cudaStream_t s);
+// inputs of the phase table of a middle pass's field terms (rsv_kernels.cu)
+struct DeferPhaseArgs {
+  const double4 *coef;
+  int n, layer;
+  unsigned int pending;  // wires whose tangent factors psi and lambda still carry
+  int wires[8];          // the pass's gated wires on tile bits 3..10
+  double field;
+};
+cudaError_t launch_defer_phase(const DeferPhaseArgs &A, double2 *out, cudaStream_t s);
 // qubits from which the energy is split (tile kernel + grid-stride kernel)
 int energy_split_qubits();
 // kernels launch_energy launches for n qubits (1, or 2 for the split energy)

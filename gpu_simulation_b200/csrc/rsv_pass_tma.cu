@@ -269,6 +269,45 @@ __device__ __forceinline__ void emask_apply(double h, const double2 *stage, int 
   e = fma(-h, es, e);
 }
 
+// The middle pass's field terms, layout P: for the adjacent pairs of gated tile
+// bits (3 + j, 4 + j), j < 7, lambda[r] += ph[4 j + q] psi(t ^ m_j) (q = the
+// pair's bits of t; ph holds -h F^2 and the RZ phase ratio) and the energy
+// share Re(conj(psi[r]) delta) into e.  Pairs of register bits (j >= 4) take
+// the partner from the thread's own registers, the others from the stage.
+// (Multiplying the warp's psi in the stage by the phases first, so that one
+// phase per amplitude would do, measured slower: the extra stage writes and
+// partner loads cost more than the six products they save.)
+__device__ __forceinline__ double2 cadd(double2 x, double2 y) { return make_double2(x.x + y.x, x.y + y.y); }
+template <int J>
+__device__ __forceinline__ double2 dpartner(const double2 *stage, int s0, int r, const double2 (&a)[kR]) {
+  return epartner<(3 << (3 + J))>(stage, s0, r, a);
+}
+__device__ __forceinline__ void dmask_apply(const double2 *ph, const double2 *stage, int lane, int warp,
+                                            const double2 (&a)[kR], double2 (&b)[kR], double &e) {
+  static_assert(kTmaNumDeferredMasks == 7, "the sum below lists the masks");
+  const int s0 = sw128(tP(lane, warp, 0));
+  // pairs j = 0..2 lie on lane bits (tile bits 3..6 = lane bits 0..3): one
+  // phase per thread; j = 3 on lane bit 3 and register bit 0: two; j = 4..6 on
+  // register bits: selected per register (compile time), loaded per use
+  const int lq = lane & 15;
+  const double2 p0 = ph[0 + (lq & 3)], p1 = ph[4 + ((lq >> 1) & 3)], p2 = ph[8 + ((lq >> 2) & 3)];
+  const double2 p3e = ph[12 + (lq >> 3)], p3o = ph[12 + (lq >> 3) + 2];
+  double es = 0.0;
+#pragma unroll
+  for (int r = 0; r < kR; ++r) {
+    double2 d = cmul(p0, dpartner<0>(stage, s0, r, a));
+    d = cadd(d, cmul(p1, dpartner<1>(stage, s0, r, a)));
+    d = cadd(d, cmul(p2, dpartner<2>(stage, s0, r, a)));
+    d = cadd(d, cmul((r & 1) ? p3o : p3e, dpartner<3>(stage, s0, r, a)));
+    d = cadd(d, cmul(ph[16 + (r & 3)], dpartner<4>(stage, s0, r, a)));
+    d = cadd(d, cmul(ph[20 + ((r >> 1) & 3)], dpartner<5>(stage, s0, r, a)));
+    d = cadd(d, cmul(ph[24 + ((r >> 2) & 3)], dpartner<6>(stage, s0, r, a)));
+    b[r] = make_double2(b[r].x + d.x, b[r].y + d.y);
+    es = fma(a[r].x, d.x, fma(a[r].y, d.y, es));
+  }
+  e += es;
+}
+
 // layout P -> layout Q of one vector through the warp's slice
 __device__ __forceinline__ void transpose_pq(double2 *xs, int lane, double2 (&a)[kR]) {
 #pragma unroll
@@ -296,6 +335,7 @@ __global__ void __launch_bounds__(tw::kThreads, 2)
   __shared__ double acc_sm[8 * kThreads];
   __shared__ double v_sm[PHASE ? 5 * kThreads : 1];
   __shared__ double2 ratio_sm[4];
+  __shared__ double2 dph_sm[PHASE ? kTmaDeferTable : 1];
   __shared__ volatile int abort_flag;
 
   const unsigned raw = smem_u32(smem_raw);
@@ -328,6 +368,7 @@ __global__ void __launch_bounds__(tw::kThreads, 2)
 #pragma unroll
     for (int i = 0; i < 5; ++i) v_sm[i * kThreads + tid] = 0.0;
     if (tid < 4) ratio_sm[tid] = phase_ratio(P, unit_bit(P.vec[7 + tid]));
+    if (T.defer_terms && tid < kTmaDeferTable) dph_sm[tid] = T.emask_phase[tid];
   }
   __syncthreads();
 
@@ -367,6 +408,7 @@ __global__ void __launch_bounds__(tw::kThreads, 2)
       a[r] = stage[t];
       b[r] = stage[kTile + t];
     }
+    if (PHASE && T.defer_terms) dmask_apply(dph_sm, stage, lane, warp, a, b, e_acc);
     if (PHASE && T.energy_terms) {
       switch (T.energy_terms - 1) {
         case 0: emask_apply<0>(T.efield, stage, lane, warp, a, b, e_acc); break;
@@ -397,12 +439,14 @@ __global__ void __launch_bounds__(tw::kThreads, 2)
 
     const u32 cbase = deposit(P, first + static_cast<u32>(j) * gridDim.x);
     if (PHASE) {
-      // RZ^dagger of the layer (with the layer's factor K) on psi and lambda,
-      // then the phi sums q = Im(conj(lam) psi)
-      const double2 ph = table4(P.ptab, cbase ^ toffP);
-      const double K = P.lscale[P.layer];
-      const double2 ratio[4] = {ratio_sm[0], ratio_sm[1], ratio_sm[2], ratio_sm[3]};
-      apply_phase_gray<4, true, true>(make_double2(K * ph.x, K * ph.y), ratio, a, b);
+      // RZ^dagger of the layer (with the layer's factor K) on psi and lambda
+      // (not in a phi_only pass), then the phi sums q = Im(conj(lam) psi)
+      if (!T.phi_only) {
+        const double2 ph = table4(P.ptab, cbase ^ toffP);
+        const double K = P.lscale[P.layer];
+        const double2 ratio[4] = {ratio_sm[0], ratio_sm[1], ratio_sm[2], ratio_sm[3]};
+        apply_phase_gray<4, true, true>(make_double2(K * ph.x, K * ph.y), ratio, a, b);
+      }
       double tot = 0.0, rb[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
       for (int r = 0; r < kR; ++r) {
@@ -474,7 +518,7 @@ __global__ void __launch_bounds__(tw::kThreads, 2)
       for (int ww = 0; ww < kWarps; ++ww) s += red[ww][tid - 3];
     rec[tid] = s;
   }
-  if (PHASE && T.energy_terms) {
+  if (PHASE && (T.energy_terms || T.defer_terms)) {
     const double es = warp_sum(e_acc);
     __syncthreads();  // red is reused
     if (lane == 0) red[warp][0] = es;
@@ -978,7 +1022,7 @@ cudaError_t launch_bwd_tma(const PassParams &P, const TmaPass &T, int grid, cuda
     bwd_tma_low_kernel<<<grid, tl::kThreads, tl::kSmemBytes, s>>>(P, T);
     return cudaGetLastError();
   }
-  if (P.phase) {
+  if (P.phase || T.phi_only) {
     const cudaError_t e = configure_tma(bwd_tma_kernel<true>, cfg_phase);
     if (e != cudaSuccess) return e;
     bwd_tma_kernel<true><<<grid, tw::kThreads, tw::kSmemBytes, s>>>(P, T);

@@ -45,6 +45,18 @@ struct alignas(64) TmaPass {
   int energy_terms;
   double efield;
   double *energy_partials;
+  // The layer's middle pass with the fused energy (plan-level): phi_only runs
+  // the phase-pass kernel without the layer's RZ^dagger, for the phi sums of
+  // its own wires (their field terms reach lambda only in this pass); per call
+  // defer_terms = 1 adds those terms, the adjacent pairs of its gated tile bits
+  // 3..10 (tile-bit masks m_j = 3 << (3 + j), j < 7), as
+  // lambda(t) += emask_phase[4 j + q] psi(t ^ m_j), q = the pair's two bits of t:
+  // -h F^2 conj(D(t)) D(t ^ m_j) with D the layer's RZ phases (undone by the
+  // layer's first pass) and F the tangent factors still on psi and lambda,
+  // and its energy share goes to energy_partials[blockIdx.x].
+  int phi_only;
+  int defer_terms;
+  const double2 *emask_phase;  // [kTmaDeferTable]
 };
 
 // The field terms P^-1(e_w) inside an 11-bit phase-pass tile whose tile bits
@@ -52,6 +64,8 @@ struct alignas(64) TmaPass {
 // bits (gated), U = 0..3: the adjacent pairs inside each run (e_w + e_{w+1})
 // and the last wire's e_{n-1} + e_0 + e_1; ten masks for every U, in tile bits.
 constexpr int kTmaNumEnergyMasks = 10;
+constexpr int kTmaNumDeferredMasks = 7;
+constexpr int kTmaDeferTable = 4 * kTmaNumDeferredMasks;
 constexpr int kTmaMaxEnergyU = 3;
 __host__ __device__ constexpr unsigned tma_energy_mask(int u, int j) {
   return j == 9 ? 0x403u : (3u << (j < 2 + u ? j : j + 1));

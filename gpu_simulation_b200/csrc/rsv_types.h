@@ -129,6 +129,12 @@ struct FinalizeParams {
   const int *phi_pass;           // [L]
   const double *gscale;          // [2 L n] multiplier of every gradient sum
   const int *pipeline_err;       // non-zero: a TMA pass gave up waiting; outputs become NaN (may be null)
+  // phi of the wires in phi_alt_wires of layer phi_alt_layer (-1: none) from
+  // pass phi_alt_pass's sums, unscaled (a pass after the layer's first, where
+  // psi and lambda carry reciprocal tangent factors)
+  int phi_alt_layer;
+  int phi_alt_pass;
+  unsigned int phi_alt_wires;
   double *energy_out;
   double *grad_out;              // [2 L n] or null
 };

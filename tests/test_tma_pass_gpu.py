@@ -70,10 +70,11 @@ def test_tma_passes_match_reference(n, L, h):
 
 @pytest.mark.parametrize("n,L,h", [(23, 4, 0.8), (24, 4, 1.0), (28, 4, 1.0)])
 def test_fused_energy_matches_separate_energy(n, L, h):
-    """The last layer's first backward pass applies the field terms on its tile
-    (default): energy and gradient equal the separate energy kernels' to
-    rounding; energy-only calls and the forward/backward device split keep the
-    whole energy kernel and agree too."""
+    """The last layer's first backward pass applies the field terms on its tile,
+    and at n=28 the middle pass those of its own wires (default): energy and
+    gradient equal the separate energy kernels' to rounding; energy-only calls
+    and the forward/backward device split keep the whole energy kernel (the
+    middle pass still takes its wires' phi sums) and agree too."""
     import torch
 
     from gpu_simulation_b200 import ring_ising_energy
@@ -83,7 +84,10 @@ def test_fused_energy_matches_separate_energy(n, L, h):
     try:
         k = eng.kernels()
         assert k["tma"] and k["fused_energy"], k
-        assert "fused_energy: backward pass 0 applies" in eng.describe()
+        desc = eng.describe().splitlines()[0]
+        assert "fused_energy: backward pass 0 applies" in desc
+        if n == 28:  # the middle pass (wires 12..19) takes the terms of its wires too
+            assert "backward pass 1 applies 7" in desc, desc
         e1, g1 = eng.energy_and_grad(p)
         e1b, g1b = eng.energy_and_grad(p)
         e_only = eng.energy(p)
