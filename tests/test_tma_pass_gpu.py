@@ -104,3 +104,23 @@ def test_fused_energy_matches_separate_energy(n, L, h):
     assert abs(e1 - e0) < 1e-12 and abs(e_only - e0) < 1e-12 and abs(float(e_ad) - e0) < 1e-12
     np.testing.assert_allclose(g1, g0, atol=1e-12, rtol=0)
     np.testing.assert_allclose(g_ad, g0, atol=1e-12, rtol=0)
+
+
+def test_fused_energy_follows_set_field():
+    """The fused field terms and their phase table take the backend's current
+    field, not the one it was planned with."""
+    n, L = 28, 4
+    p = np.random.default_rng(1400).uniform(0, 2 * np.pi, 2 * n * L)
+    eng = Engine(n, L, 1.0)
+    try:
+        eng.set_field(0.55)
+        e1, g1 = eng.energy_and_grad(p)
+    finally:
+        eng.close()
+    fresh = Engine(n, L, 0.55)
+    try:
+        e0, g0 = fresh.energy_and_grad(p)
+    finally:
+        fresh.close()
+    assert abs(e1 - e0) < 1e-12
+    np.testing.assert_allclose(g1, g0, atol=1e-12, rtol=0)
