@@ -1,4 +1,4 @@
-"""ctypes binding of the engine's C ABI (include/rsv.h, librsv.so).
+"""ctypes binding of the engine's C ABI (include/rsv.h, include/rsv_shard.h, librsv.so).
 
 The library is built in-tree (``python -m gpu_simulation_b200.build``).  There
 is no CPU fallback: if librsv.so is missing or cannot be loaded, every entry
@@ -17,7 +17,7 @@ RSV_OK = 0
 RSV_ERR_INVALID_ARGUMENT = 1
 RSV_ERR_STALE_STATE = 6
 
-# Every function declared in include/rsv.h, with its ctypes signature.
+# Every function declared in include/rsv.h and include/rsv_shard.h, with its ctypes signature.
 _c_double_p = ctypes.POINTER(ctypes.c_double)
 _SIGNATURES = {
     "rsv_version": ([], ctypes.c_char_p),
@@ -104,6 +104,30 @@ _SIGNATURES = {
     "rsv_adam_vqe_step_f64": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
                                ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    # include/rsv_shard.h
+    "rsv_shard_check": ([ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "rsv_shard_scratch_doubles": ([ctypes.c_int, ctypes.c_int], ctypes.c_size_t),
+    "rsv_shard_coef": ([ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+                       ctypes.c_int),
+    "rsv_shard_init": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
+                       ctypes.c_int),
+    "rsv_shard_rotate_local": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.c_void_p], ctypes.c_int),
+    "rsv_shard_rotate_local_adjoint": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_void_p], ctypes.c_int),
+    "rsv_shard_energy_local": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_void_p,
+                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "rsv_shard_ring_pack": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "rsv_shard_ring_unpack": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                               ctypes.c_void_p], ctypes.c_int),
+    "rsv_shard_ring_pack_adjoint": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "rsv_shard_ring_unpack_adjoint": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
 }
 
 _lib = None

@@ -27,7 +27,7 @@ CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 NVCC = str(CUDA_HOME / "bin" / "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["rsv_kernels.cu", "rsv_pass.cu", "rsv_pass_half.cu", "rsv_layer0.cu", "rsv_mps.cu", "rsv_noalloc.cu", "rsv_pass_tma.cu", "rsv_batch.cu", "rsv_mlp.cu", "rsv_gate.cu", "rsv_dense.cu"]
+CU_SOURCES = ["rsv_kernels.cu", "rsv_pass.cu", "rsv_pass_half.cu", "rsv_layer0.cu", "rsv_mps.cu", "rsv_noalloc.cu", "rsv_pass_tma.cu", "rsv_batch.cu", "rsv_mlp.cu", "rsv_gate.cu", "rsv_dense.cu", "rsv_shard.cu"]
 CPP_SOURCES = ["rsv_backend.cpp", "rsv_mlp_host.cpp"]
 HEADERS = ["rsv_device.cuh", "rsv_types.h", "rsv_launch.h", "rsv_workspace.h", "rsv_tma.h", "rsv_tile.cuh", "rsv_batch.h", "rsv_mlp.h", "rsv_gate.h", "rsv_dense.h"]
 
@@ -59,7 +59,7 @@ def _run(cmd: list[str], verbose: bool) -> str:
 def build(verbose: bool = False, ptxas_verbose: bool = False) -> Path:
     """Compile librsv.so and the drop-in module if any source changed."""
     BUILD.mkdir(exist_ok=True)
-    headers = [CSRC / h for h in HEADERS] + [ROOT / "include" / "rsv.h"]
+    headers = [CSRC / h for h in HEADERS] + [ROOT / "include" / "rsv.h", ROOT / "include" / "rsv_shard.h"]
     jobs = []
     objs = []
     for src in CU_SOURCES:

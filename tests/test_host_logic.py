@@ -20,9 +20,11 @@ ROOT = Path(__file__).resolve().parent.parent
 
 
 def declared_functions() -> list[str]:
-    text = (ROOT / "include" / "rsv.h").read_text()
-    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(rsv_[a-z_]+)\s*\(", text)))
+    names = set()
+    for header in sorted((ROOT / "include").glob("*.h")):
+        text = re.sub(r"/\*.*?\*/", "", header.read_text(), flags=re.S)
+        names.update(re.findall(r"\b(rsv_[a-z_]+)\s*\(", text))
+    return sorted(names)
 
 
 def test_library_exports_every_declared_symbol():
