@@ -47,7 +47,7 @@ constexpr int kRec = 2 * kT;      // one CTA's gradient record: (theta, phi) per
 constexpr int kMaxRuns = kT + 1;
 constexpr int kAdjSmem = 2 * kTile * 16;
 constexpr int kRotCtasPerSm = 3;  // 32 KiB of shared memory and <= 170 registers a thread each
-constexpr int kAdjCtasPerSm = 2;  // 64 KiB each
+constexpr int kAdjCtasPerSm = 2;  // 64 KiB of shared memory and <= 255 registers a thread each
 
 struct TileArgs {
   int n, nloc, layer;
@@ -284,52 +284,100 @@ __global__ void rot_records_kernel(const __grid_constant__ TileArgs A, const dou
 }
 
 // ---------------------------------------------------------------- energy (C)
-constexpr int kEThreads = 256;
-
-// lambda = (sum_w -Z_w Z_{w+1} - h sum_{w < nloc} X_w) psi on the shard of
-// rank `rank` in layout C; per-CTA energy records (reference
-// cpp/ising_cuda_kernels.cu:313-358, the X terms of the local wires only)
-__global__ void __launch_bounds__(kEThreads) energy_local_kernel(const double2 *__restrict__ psi,
-                                                                 double2 *__restrict__ lam, int n, int nloc,
-                                                                 int rank, double field,
-                                                                 double *__restrict__ records) {
-  __shared__ double red[kEThreads / 32];
-  const u64 size = u64{1} << nloc;
-  const u64 full = (u64{1} << n) - 1;
-  double e = 0.0;
-  for (u64 v = blockIdx.x * static_cast<u64>(kEThreads) + threadIdx.x; v < size;
-       v += static_cast<u64>(gridDim.x) * kEThreads) {
-    const u64 y = (static_cast<u64>(rank) << nloc) | v;
-    const u64 rot = ((y << 1) & full) | (y >> (n - 1));
-    const double d = static_cast<double>(2 * __popcll(y ^ rot) - n);
-    const double2 c = psi[v];
-    double2 x = make_double2(0.0, 0.0);
-    for (int w = 0; w < nloc; ++w) {
-      const double2 t = psi[v ^ (u64{1} << w)];
-      x.x += t.x;
-      x.y += t.y;
+// lambda = (sum_w -Z_w Z_{w+1} - h sum_{w < n-g} X_w) psi on the shard of
+// rank `rank` in layout C (reference cpp/ising_cuda_kernels.cu:313-358, the X
+// terms of the local wires only), on the tiles of the local rotation passes:
+// the first pass (tile bits = local bits 0..10) starts lambda with the ZZ
+// diagonal, every pass subtracts h psi[v ^ e_b] for the wires on its tile
+// bits, partners taken from registers in the three layouts of rot_kernel, so
+// psi is read once per pass and each partner needs no further memory access.
+// Per-CTA records: the energy share of what the pass added.
+template <int TB0, int NB>
+__device__ __forceinline__ void xsum_gates(const TileArgs &A, double field, const double2 (&a)[kR],
+                                           double2 (&acc)[kR], double &e) {
+#pragma unroll
+  for (int j = 0; j < NB; ++j) {
+    if (A.wire[TB0 + j] < 0) continue;
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+      const double2 p = a[r ^ (1 << j)];
+      acc[r].x = fma(-field, p.x, acc[r].x);
+      acc[r].y = fma(-field, p.y, acc[r].y);
+      e -= field * fma(a[r].x, p.x, a[r].y * p.y);
     }
-    const double2 m = make_double2(fma(d, c.x, -field * x.x), fma(d, c.y, -field * x.y));
-    lam[v] = m;
-    e += fma(c.x, m.x, c.y * m.y);
-  }
-  e = warp_sum(e);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = e;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int w = 0; w < kEThreads / 32; ++w) s += red[w];
-    records[blockIdx.x] = s;
   }
 }
 
-__global__ void sum_records_kernel(const double *__restrict__ records, int grid, int stride, int count,
-                                   double *__restrict__ out) {
-  const int i = threadIdx.x;
-  if (i >= count) return;
+template <bool FIRST>
+__global__ void __launch_bounds__(kRotThreads, kAdjCtasPerSm) energy_tile_kernel(const __grid_constant__ TileArgs A,
+                                                                                 int rank, double field,
+                                                                                 const double2 *__restrict__ psi,
+                                                                                 double2 *__restrict__ lam,
+                                                                                 double *__restrict__ records) {
+  extern __shared__ double2 sm2[];
+  __shared__ double red[kRotThreads / 32];
+  const int tau = threadIdx.x;
+  u32 otau = 0;
+#pragma unroll
+  for (int j = 0; j < 7; ++j)
+    if ((tau >> j) & 1) otau |= 1u << A.bits[j];
+  u32 rb[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) rb[j] = 1u << A.bits[7 + j];
+  const u64 full = (u64{1} << A.n) - 1;
+  const u64 rhi = static_cast<u64>(rank) << A.nloc;
+  double e = 0.0;
+  for (u32 k = blockIdx.x; k < A.num_tiles; k += gridDim.x) {
+    const u32 base = tile_base(A, k) | otau;
+    double2 a[kR], acc[kR];
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+      const u32 off = base | reg_off(r, rb);
+      a[r] = __ldcs(&psi[off]);
+      if (FIRST) {
+        const u64 y = rhi | off;
+        const u64 rot = ((y << 1) & full) | (y >> (A.n - 1));
+        const double d = static_cast<double>(2 * __popcll(y ^ rot) - A.n);
+        acc[r] = make_double2(d * a[r].x, d * a[r].y);
+        e += d * fma(a[r].x, a[r].x, a[r].y * a[r].y);
+      } else {
+        acc[r] = __ldcs(&lam[off]);
+      }
+    }
+    xsum_gates<7, 4>(A, field, a, acc, e);
+    if (A.need_b) {
+      xpose2<0, 1>(sm2, tau, a, acc);
+      xsum_gates<3, 4>(A, field, a, acc, e);
+      if (A.need_c) {
+        xpose2<1, 2>(sm2, tau, a, acc);
+        xsum_gates<0, 3>(A, field, a, acc, e);
+        xpose<2, 0>(sm2, tau, acc);
+      } else {
+        xpose<1, 0>(sm2, tau, acc);
+      }
+    }
+    u32 sbase = base;  // store addresses derived again (not kept live across the sums)
+    asm volatile("" : "+r"(sbase));
+#pragma unroll
+    for (int r = 0; r < kR; ++r) __stcs(&lam[sbase | reg_off(r, rb)], acc[r]);
+  }
+  e = warp_sum(e);
+  if ((tau & 31) == 0) red[tau >> 5] = e;
+  __syncthreads();
+  if (tau == 0) {
+    double sum = 0.0;
+    for (int w = 0; w < kRotThreads / 32; ++w) sum += red[w];
+    records[blockIdx.x] = sum;
+  }
+}
+
+// result[0] = (first pass) or += the pass's CTA records, in CTA order
+__global__ void energy_records_kernel(const double *__restrict__ records, int grid, int first,
+                                      double *__restrict__ result) {
+  if (threadIdx.x != 0) return;
   double s = 0.0;
-  for (int b = 0; b < grid; ++b) s += records[static_cast<size_t>(b) * stride + i];
-  out[i] = s;
+  for (int b = 0; b < grid; ++b) s += records[b];
+  result[0] = first ? s : result[0] + s;
 }
 
 // ---------------------------------------------------------------- ring exchange
@@ -804,13 +852,24 @@ extern "C" rsv_status rsv_shard_energy_local(int num_qubits, int g, int rank, do
     check_ptr(d_lam, "d_lam");
     check_ptr(d_scratch, "d_scratch");
     check_ptr(d_result, "d_result");
-    const int nloc = num_qubits - g;
-    const int grid = grid_for((u64{1} << nloc) / kEThreads, kMaxCtasPerSm);
-    energy_local_kernel<<<grid, kEThreads, 0, as_stream(stream)>>>(reinterpret_cast<const double2 *>(d_psi),
-                                                                   reinterpret_cast<double2 *>(d_lam), num_qubits,
-                                                                   nloc, rank, field, d_scratch);
-    sum_records_kernel<<<1, 32, 0, as_stream(stream)>>>(d_scratch, grid, 1, 1, d_result);
-    cuda_check(cudaGetLastError(), "shard energy launch");
+    static std::atomic<unsigned long long> cfg_first{0}, cfg_rest{0};
+    cuda_check(set_smem_limit_once(energy_tile_kernel<true>, kAdjSmem, cfg_first), "shard energy smem limit");
+    cuda_check(set_smem_limit_once(energy_tile_kernel<false>, kAdjSmem, cfg_rest), "shard energy smem limit");
+    TileArgs passes[kMaxPasses];
+    const int np = local_passes(num_qubits, num_qubits - g, 0, passes);
+    const auto *psi = reinterpret_cast<const double2 *>(d_psi);
+    auto *lam = reinterpret_cast<double2 *>(d_lam);
+    for (int p = 0; p < np; ++p) {
+      const int grid = grid_for(passes[p].num_tiles, kAdjCtasPerSm);
+      if (p == 0)
+        energy_tile_kernel<true><<<grid, kRotThreads, kAdjSmem, as_stream(stream)>>>(passes[p], rank, field, psi, lam,
+                                                                                     d_scratch);
+      else
+        energy_tile_kernel<false><<<grid, kRotThreads, kAdjSmem, as_stream(stream)>>>(passes[p], rank, field, psi,
+                                                                                      lam, d_scratch);
+      energy_records_kernel<<<1, 32, 0, as_stream(stream)>>>(d_scratch, grid, p == 0 ? 1 : 0, d_result);
+      cuda_check(cudaGetLastError(), "shard energy launch");
+    }
   });
 }
 
