@@ -30,7 +30,12 @@ all-gather), against a per-circuit loop of the single-circuit entry point;
 network's prediction at n=16, L=6 on 128 held-out fields (N=1 only);
 ``adam_n12_l3`` and ``autograd_n20_l8`` -- torch Adam loops through the
 autograd Function at n=12, L=3 (20 steps) and n=20, L=8 (100 steps), with the
-bare device entry point and the CPU oracle beside them (N=1 only).
+bare device entry point and the CPU oracle beside them (N=1 only);
+``sharded`` -- one circuit split over 2^g ranks (gpu_simulation_b200/
+sharded.py): with N > 1, n=30 over the N ranks (NCCL all-to-alls), against
+the single-GPU engine's energy and gradient; with N = 1, the headline circuit
+over two virtual ranks on the one GPU, and the per-rank kernels of an n=33
+circuit over 8 ranks at their full shard size (2^30 amplitudes), timed alone.
 """
 
 from __future__ import annotations
@@ -70,6 +75,7 @@ def parse_args():
     ap.add_argument("--no-warmstart", action="store_true", help="skip the warm-start section")
     ap.add_argument("--no-small", action="store_true", help="skip the n=12 Adam and n=20 autograd sections")
     ap.add_argument("--no-autotune", action="store_true", help="keep the planner's default plan (no autotune)")
+    ap.add_argument("--no-sharded", action="store_true", help="skip the sharded single-circuit section")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="reference arm: skip timing the reference's sm_100a rebuild on the GPU")
     return ap.parse_args()
@@ -492,6 +498,113 @@ def autotune_summary(eng, n, L, seed, repeats=2):
 
 
 # ---------------------------------------------------------------- GPU arm
+def sharded_section(args, rank, world, dist, barrier, max_over_ranks, single=None):
+    """Sharded single circuit: timed energy_and_grad through ShardedEngine,
+    compared with the single-GPU engine on the same parameters."""
+    import torch
+
+    from gpu_simulation_b200 import Engine
+    from gpu_simulation_b200.sharded import ShardedEngine
+
+    L, h = args.layers, args.field
+    out = {}
+    try:
+        if world > 1:
+            n, kw, how = 30, dict(group=dist.group.WORLD), f"{world} ranks, NCCL all_to_all_single"
+        else:
+            n, kw, how = args.qubits, dict(virtual_ranks=2), "2 virtual ranks on one GPU (exchanges as device copies)"
+        p = workload_params(n, L, 7)
+        ref = None
+        if single is not None and single[0] == n:
+            ref = single[1]
+        elif rank == 0:
+            e1 = Engine(n, L, h)
+            ref = e1.energy_and_grad(p)
+            e1.close()
+            torch.cuda.empty_cache()
+        barrier()
+        sh = ShardedEngine(n, L, h, **kw)
+        e, g = sh.energy_and_grad(p)
+        steps = max(2, min(args.steps, 5))
+        barrier()
+        s, t = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(steps):
+            sh.energy_and_grad(p)
+        t.record()
+        torch.cuda.synchronize()
+        ms = max_over_ranks(s.elapsed_time(t) / steps)
+        out = {"workload": f"energy_and_grad n={n} L={L} h={h}", "ranks": how, "ms_per_call": ms,
+               "energy_and_grad_per_s": 1000.0 / ms, "energy": e,
+               "timing": "CUDA events over host-parameter calls (host result), max over ranks"}
+        if ref is not None:
+            out["vs_single_gpu_engine"] = {"energy_abs_diff": abs(e - ref[0]),
+                                           "grad_max_abs_diff": float(np.max(np.abs(g - ref[1])))}
+        del sh
+        torch.cuda.empty_cache()
+        if world == 1:
+            out["rank_kernels_n33_8_ranks"] = shard_rank_kernels(33, 3, L)
+    except Exception as exc:  # report, do not hide
+        out["error"] = str(exc)
+    return out
+
+
+def shard_rank_kernels(n, g, L, reps=3):
+    """One rank's kernels of a sharded call at full shard size (no exchange),
+    and the exchange volume that the call's all-to-alls move per rank."""
+    import torch
+
+    from gpu_simulation_b200.sharded import CudaShardOps
+
+    ops = CudaShardOps()
+    local = 1 << (n - g)
+    vec = lambda: torch.zeros(local, dtype=torch.complex128, device="cuda")  # noqa: E731
+    psi, psi2, lam, lam2 = vec(), vec(), vec(), vec()
+    psi.real.normal_()
+    lam.real.normal_()
+    p = torch.tensor(workload_params(n, L, 7), device="cuda")
+    coef = torch.zeros(4 * n * L, dtype=torch.float64, device="cuda")
+    ops.coef(n, L, p, coef)
+    scratch = torch.zeros(ops.scratch_doubles(n, g), dtype=torch.float64, device="cuda")
+    res = torch.zeros(2 + 2 * n * L, dtype=torch.float64, device="cuda")
+    vbytes = local * 16
+    peak, _ = measured_peaks()
+    table = {}
+
+    def timed(name, fn, vectors, per_call):
+        fn()
+        torch.cuda.synchronize()
+        s, t = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(reps):
+            fn()
+        t.record()
+        torch.cuda.synchronize()
+        ms = s.elapsed_time(t) / reps
+        gbs = vectors * vbytes / (ms * 1e-3) / 1e9
+        table[name] = {"ms": ms, "per_call": per_call, "bytes": vectors * vbytes, "gbs": gbs, "frac_of_peak": gbs / peak}
+
+    timed("rotate_local (wires 0..n-g-1, 4 tile passes)", lambda: ops.rotate_local(n, g, 1, coef, psi), 8, L)
+    timed("ring_pack (wires n-g..n-1 + sort by destination)", lambda: ops.ring_pack(n, g, 0, 1, coef, psi, psi2), 2, L)
+    timed("ring_unpack", lambda: ops.ring_unpack(n, g, 0, psi2, psi), 2, L)
+    timed("energy_local (4 tile passes)", lambda: ops.energy_local(n, g, 0, 1.0, psi, lam, scratch, res), 11, 1)
+    timed("ring_pack_adjoint", lambda: ops.ring_pack_adjoint(n, g, 0, psi, lam, psi2, lam2), 4, L)
+    timed("ring_unpack_adjoint", lambda: ops.ring_unpack_adjoint(n, g, 0, L, 1, coef, 1.0, 0, psi2, lam2, psi, lam,
+                                                                scratch, res), 4, L)
+    timed("rotate_local_adjoint (4 tile passes)", lambda: ops.rotate_local_adjoint(n, g, L, 1, coef, psi, lam,
+                                                                                  scratch, res), 16, L)
+    kernels_ms = sum(v["ms"] * v["per_call"] for v in table.values())
+    # all-to-alls per call: forward 2 vectors a layer, backward 4; (N-1)/N of
+    # each crosses NVLink in each direction
+    N = 1 << g
+    cross = 6 * L * vbytes * (N - 1) / N
+    link = 770.0  # GB/s per direction, measured peer copy on this pool's NVLink
+    return {"shard_amplitudes": local, "ops": table, "kernels_ms_per_call": kernels_ms,
+            "exchange_bytes_per_rank_per_call": cross,
+            "exchange_ms_at_770_gbs": cross / (link * 1e9) * 1e3,
+            "note": "per-rank kernels timed alone on one GPU (CUDA events); the all-to-alls are not run here"}
+
+
 def device_time(eng, n, L, field, steps, warmup, seed, timing=False):
     import torch
 
@@ -672,7 +785,13 @@ def main():
         }
     if world == 1 and rank == 0:
         line["pennylane_lightning_qubit"] = pennylane_baseline()
+    single = (n, eng.energy_and_grad(workload_params(n, L, 7))) if not args.no_sharded else None
     eng.close()
+    if not args.no_sharded:
+        import torch as _t
+
+        _t.cuda.empty_cache()
+        line["sharded"] = sharded_section(args, rank, world, dist, barrier, max_over_ranks, single)
     if not args.no_batch:
         line["batch"] = batch_section(args, rank, world, dist, barrier, max_over_ranks)
     if world == 1 and not args.no_warmstart:
