@@ -172,6 +172,25 @@ __device__ __forceinline__ u32 tile_base(const TileArgs &A, u32 k) {
   return base;
 }
 
+// offsets of layout B (thread bits = tile bits 0..2 and 7..10, register bits =
+// tile bits 3..6): a pass whose last gates are in layout B stores from there
+// (rows of 128 contiguous bytes per register, the two halves of each 256-byte
+// row from consecutive registers) instead of transposing back to layout A
+__device__ __forceinline__ u32 thread_off_b(const TileArgs &A, int tau) {
+  u32 o = 0;
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+    if ((tau >> j) & 1) o |= 1u << A.bits[j];
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+    if ((tau >> (3 + j)) & 1) o |= 1u << A.bits[7 + j];
+  return o;
+}
+__device__ __forceinline__ u32 reg_off_b(const TileArgs &A, int r) {
+  return ((r & 1) ? 1u << A.bits[3] : 0u) | ((r & 2) ? 1u << A.bits[4] : 0u) | ((r & 4) ? 1u << A.bits[5] : 0u) |
+         ((r & 8) ? 1u << A.bits[6] : 0u);
+}
+
 __device__ __forceinline__ u32 reg_off(int r, const u32 (&rb)[4]) {
   return ((r & 1) ? rb[0] : 0u) | ((r & 2) ? rb[1] : 0u) | ((r & 4) ? rb[2] : 0u) | ((r & 8) ? rb[3] : 0u);
 }
@@ -197,6 +216,7 @@ __global__ void __launch_bounds__(kRotThreads, kRotCtasPerSm) rot_kernel(const _
 #pragma unroll
     for (int r = 0; r < kR; ++r) a[r] = __ldcs(&psi[base | reg_off(r, rb)]);
     fwd_gates<7, 4>(A, cf, a);
+    bool from_b = false;
     if (A.need_b) {
       xpose<0, 1>(sm, tau, a);
       fwd_gates<3, 4>(A, cf, a);
@@ -205,13 +225,19 @@ __global__ void __launch_bounds__(kRotThreads, kRotCtasPerSm) rot_kernel(const _
         fwd_gates<0, 3>(A, cf, a);
         xpose<2, 0>(sm, tau, a);
       } else {
-        xpose<1, 0>(sm, tau, a);
+        from_b = true;
       }
     }
     u32 sbase = base;  // store addresses derived again (not kept live across the gates)
     asm volatile("" : "+r"(sbase));
+    if (from_b) {
+      const u32 ob = (sbase ^ otau) | thread_off_b(A, tau);
 #pragma unroll
-    for (int r = 0; r < kR; ++r) __stcs(&psi[sbase | reg_off(r, rb)], a[r]);
+      for (int r = 0; r < kR; ++r) __stcs(&psi[ob | reg_off_b(A, r)], a[r]);
+    } else {
+#pragma unroll
+      for (int r = 0; r < kR; ++r) __stcs(&psi[sbase | reg_off(r, rb)], a[r]);
+    }
   }
 }
 
@@ -243,6 +269,7 @@ __global__ void __launch_bounds__(kRotThreads, kAdjCtasPerSm) rot_adjoint_kernel
       l[r] = __ldcs(&lam[base | reg_off(r, rb)]);
     }
     adj_gates<7, 4>(A, cf, a, l, rec[warp], lane);
+    bool from_b = false;
     if (A.need_b) {
       xpose2<0, 1>(sm2, tau, a, l);
       adj_gates<3, 4>(A, cf, a, l, rec[warp], lane);
@@ -251,17 +278,26 @@ __global__ void __launch_bounds__(kRotThreads, kAdjCtasPerSm) rot_adjoint_kernel
         adj_gates<0, 3>(A, cf, a, l, rec[warp], lane);
         xpose2<2, 0>(sm2, tau, a, l);
       } else {
-        xpose2<1, 0>(sm2, tau, a, l);
+        from_b = true;
       }
     }
     // the store addresses are derived again here rather than kept live from
     // the loads (32 addresses would not fit next to the 64 amplitudes)
     u32 sbase = base;
     asm volatile("" : "+r"(sbase));
+    if (from_b) {
+      const u32 ob = (sbase ^ otau) | thread_off_b(A, tau);
 #pragma unroll
-    for (int r = 0; r < kR; ++r) {
-      __stcs(&psi[sbase | reg_off(r, rb)], a[r]);
-      __stcs(&lam[sbase | reg_off(r, rb)], l[r]);
+      for (int r = 0; r < kR; ++r) {
+        __stcs(&psi[ob | reg_off_b(A, r)], a[r]);
+        __stcs(&lam[ob | reg_off_b(A, r)], l[r]);
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < kR; ++r) {
+        __stcs(&psi[sbase | reg_off(r, rb)], a[r]);
+        __stcs(&lam[sbase | reg_off(r, rb)], l[r]);
+      }
     }
   }
   __syncthreads();
@@ -345,6 +381,7 @@ __global__ void __launch_bounds__(kRotThreads, kAdjCtasPerSm) energy_tile_kernel
       }
     }
     xsum_gates<7, 4>(A, field, a, acc, e);
+    bool from_b = false;
     if (A.need_b) {
       xpose2<0, 1>(sm2, tau, a, acc);
       xsum_gates<3, 4>(A, field, a, acc, e);
@@ -353,13 +390,19 @@ __global__ void __launch_bounds__(kRotThreads, kAdjCtasPerSm) energy_tile_kernel
         xsum_gates<0, 3>(A, field, a, acc, e);
         xpose<2, 0>(sm2, tau, acc);
       } else {
-        xpose<1, 0>(sm2, tau, acc);
+        from_b = true;
       }
     }
     u32 sbase = base;  // store addresses derived again (not kept live across the sums)
     asm volatile("" : "+r"(sbase));
+    if (from_b) {
+      const u32 ob = (sbase ^ otau) | thread_off_b(A, tau);
 #pragma unroll
-    for (int r = 0; r < kR; ++r) __stcs(&lam[sbase | reg_off(r, rb)], acc[r]);
+      for (int r = 0; r < kR; ++r) __stcs(&lam[ob | reg_off_b(A, r)], acc[r]);
+    } else {
+#pragma unroll
+      for (int r = 0; r < kR; ++r) __stcs(&lam[sbase | reg_off(r, rb)], acc[r]);
+    }
   }
   e = warp_sum(e);
   if ((tau & 31) == 0) red[tau >> 5] = e;
