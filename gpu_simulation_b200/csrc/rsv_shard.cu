@@ -113,12 +113,12 @@ __device__ __forceinline__ void rot_pair(const double4 c, double2 &x0, double2 &
 // inverse walk, RZ^dagger and RY^dagger applied in between.
 __device__ __forceinline__ void unrot_pair(const double4 c, double2 &a0, double2 &a1, double2 &l0, double2 &l1,
                                            double &gt, double &gp) {
-  gp += (l0.x * a0.y - l0.y * a0.x) - (l1.x * a1.y - l1.y * a1.x);
+  gp += fma(l0.x, a0.y, -l0.y * a0.x) - fma(l1.x, a1.y, -l1.y * a1.x);
   a0 = make_double2(c.z * a0.x - c.w * a0.y, c.z * a0.y + c.w * a0.x);
   a1 = make_double2(c.z * a1.x + c.w * a1.y, c.z * a1.y - c.w * a1.x);
   l0 = make_double2(c.z * l0.x - c.w * l0.y, c.z * l0.y + c.w * l0.x);
   l1 = make_double2(c.z * l1.x + c.w * l1.y, c.z * l1.y - c.w * l1.x);
-  gt += (l1.x * a0.x + l1.y * a0.y) - (l0.x * a1.x + l0.y * a1.y);
+  gt += fma(l1.x, a0.x, l1.y * a0.y) - fma(l0.x, a1.x, l0.y * a1.y);
   const double2 b0 = make_double2(c.x * a0.x + c.y * a1.x, c.x * a0.y + c.y * a1.y);
   const double2 b1 = make_double2(c.x * a1.x - c.y * a0.x, c.x * a1.y - c.y * a0.y);
   const double2 m0 = make_double2(c.x * l0.x + c.y * l1.x, c.x * l0.y + c.y * l1.y);
@@ -150,10 +150,17 @@ __device__ __forceinline__ void adj_gates(const TileArgs &A, const double4 *cf, 
   for (int j = 0; j < NB; ++j) {
     if (A.wire[TB0 + j] < 0) continue;
     const double4 c = cf[TB0 + j];
-    double gt = 0.0, gp = 0.0;
+    // four partial sums each: the eight pairs' terms are not one dependent chain
+    double gt4[4] = {0.0, 0.0, 0.0, 0.0}, gp4[4] = {0.0, 0.0, 0.0, 0.0};
+    int q = 0;
 #pragma unroll
     for (int r = 0; r < kR; ++r)
-      if (!(r & (1 << j))) unrot_pair(c, a[r], a[r | (1 << j)], l[r], l[r | (1 << j)], gt, gp);
+      if (!(r & (1 << j))) {
+        unrot_pair(c, a[r], a[r | (1 << j)], l[r], l[r | (1 << j)], gt4[q & 3], gp4[q & 3]);
+        ++q;
+      }
+    double gt = (gt4[0] + gt4[1]) + (gt4[2] + gt4[3]);
+    double gp = (gp4[0] + gp4[1]) + (gp4[2] + gp4[3]);
     gt = warp_sum(gt);
     gp = warp_sum(gp);
     if (lane == 0) {
@@ -330,7 +337,7 @@ __global__ void rot_records_kernel(const __grid_constant__ TileArgs A, const dou
 // Per-CTA records: the energy share of what the pass added.
 template <int TB0, int NB>
 __device__ __forceinline__ void xsum_gates(const TileArgs &A, double field, const double2 (&a)[kR],
-                                           double2 (&acc)[kR], double &e) {
+                                           double2 (&acc)[kR], double (&e4)[4]) {
 #pragma unroll
   for (int j = 0; j < NB; ++j) {
     if (A.wire[TB0 + j] < 0) continue;
@@ -339,7 +346,7 @@ __device__ __forceinline__ void xsum_gates(const TileArgs &A, double field, cons
       const double2 p = a[r ^ (1 << j)];
       acc[r].x = fma(-field, p.x, acc[r].x);
       acc[r].y = fma(-field, p.y, acc[r].y);
-      e -= field * fma(a[r].x, p.x, a[r].y * p.y);
+      e4[r & 3] = fma(-field, fma(a[r].x, p.x, a[r].y * p.y), e4[r & 3]);
     }
   }
 }
@@ -362,7 +369,7 @@ __global__ void __launch_bounds__(kRotThreads, kAdjCtasPerSm) energy_tile_kernel
   for (int j = 0; j < 4; ++j) rb[j] = 1u << A.bits[7 + j];
   const u64 full = (u64{1} << A.n) - 1;
   const u64 rhi = static_cast<u64>(rank) << A.nloc;
-  double e = 0.0;
+  double e4[4] = {0.0, 0.0, 0.0, 0.0};  // partial sums (independent chains)
   for (u32 k = blockIdx.x; k < A.num_tiles; k += gridDim.x) {
     const u32 base = tile_base(A, k) | otau;
     double2 a[kR], acc[kR];
@@ -375,19 +382,19 @@ __global__ void __launch_bounds__(kRotThreads, kAdjCtasPerSm) energy_tile_kernel
         const u64 rot = ((y << 1) & full) | (y >> (A.n - 1));
         const double d = static_cast<double>(2 * __popcll(y ^ rot) - A.n);
         acc[r] = make_double2(d * a[r].x, d * a[r].y);
-        e += d * fma(a[r].x, a[r].x, a[r].y * a[r].y);
+        e4[r & 3] = fma(d, fma(a[r].x, a[r].x, a[r].y * a[r].y), e4[r & 3]);
       } else {
         acc[r] = __ldcs(&lam[off]);
       }
     }
-    xsum_gates<7, 4>(A, field, a, acc, e);
+    xsum_gates<7, 4>(A, field, a, acc, e4);
     bool from_b = false;
     if (A.need_b) {
       xpose2<0, 1>(sm2, tau, a, acc);
-      xsum_gates<3, 4>(A, field, a, acc, e);
+      xsum_gates<3, 4>(A, field, a, acc, e4);
       if (A.need_c) {
         xpose2<1, 2>(sm2, tau, a, acc);
-        xsum_gates<0, 3>(A, field, a, acc, e);
+        xsum_gates<0, 3>(A, field, a, acc, e4);
         xpose<2, 0>(sm2, tau, acc);
       } else {
         from_b = true;
@@ -404,7 +411,7 @@ __global__ void __launch_bounds__(kRotThreads, kAdjCtasPerSm) energy_tile_kernel
       for (int r = 0; r < kR; ++r) __stcs(&lam[sbase | reg_off(r, rb)], acc[r]);
     }
   }
-  e = warp_sum(e);
+  const double e = warp_sum((e4[0] + e4[1]) + (e4[2] + e4[3]));
   if ((tau & 31) == 0) red[tau >> 5] = e;
   __syncthreads();
   if (tau == 0) {
