@@ -500,7 +500,10 @@ def autotune_summary(eng, n, L, seed, repeats=2):
 # ---------------------------------------------------------------- GPU arm
 def sharded_section(args, rank, world, dist, barrier, max_over_ranks, single=None):
     """Sharded single circuit: timed energy_and_grad through ShardedEngine,
-    compared with the single-GPU engine on the same parameters."""
+    compared with the single-GPU engine on the same parameters.  With several
+    ranks every step that can fail on one rank alone (allocation, the
+    single-GPU reference on rank 0) is followed by an agreement on its status,
+    so all ranks take the same collectives or skip together."""
     import torch
 
     from gpu_simulation_b200 import Engine
@@ -508,13 +511,21 @@ def sharded_section(args, rank, world, dist, barrier, max_over_ranks, single=Non
 
     L, h = args.layers, args.field
     out = {}
+
+    def all_ok(ok):
+        if dist is None:
+            return ok
+        flag = torch.tensor([1.0 if ok else 0.0], dtype=torch.float64, device="cuda")
+        dist.all_reduce(flag, op=dist.ReduceOp.MIN)
+        return flag.item() > 0.5
+
+    if world > 1:
+        n, kw, how = 30, dict(group=dist.group.WORLD), f"{world} ranks, NCCL all_to_all_single"
+    else:
+        n, kw, how = args.qubits, dict(virtual_ranks=2), "2 virtual ranks on one GPU (exchanges as device copies)"
+    p = workload_params(n, L, 7)
+    ref, ok = None, True
     try:
-        if world > 1:
-            n, kw, how = 30, dict(group=dist.group.WORLD), f"{world} ranks, NCCL all_to_all_single"
-        else:
-            n, kw, how = args.qubits, dict(virtual_ranks=2), "2 virtual ranks on one GPU (exchanges as device copies)"
-        p = workload_params(n, L, 7)
-        ref = None
         if single is not None and single[0] == n:
             ref = single[1]
         elif rank == 0:
@@ -522,30 +533,40 @@ def sharded_section(args, rank, world, dist, barrier, max_over_ranks, single=Non
             ref = e1.energy_and_grad(p)
             e1.close()
             torch.cuda.empty_cache()
-        barrier()
-        sh = ShardedEngine(n, L, h, **kw)
-        e, g = sh.energy_and_grad(p)
-        steps = max(2, min(args.steps, 5))
-        barrier()
-        s, t = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record()
-        for _ in range(steps):
-            sh.energy_and_grad(p)
-        t.record()
-        torch.cuda.synchronize()
-        ms = max_over_ranks(s.elapsed_time(t) / steps)
-        out = {"workload": f"energy_and_grad n={n} L={L} h={h}", "ranks": how, "ms_per_call": ms,
-               "energy_and_grad_per_s": 1000.0 / ms, "energy": e,
-               "timing": "CUDA events over host-parameter calls (host result), max over ranks"}
-        if ref is not None:
-            out["vs_single_gpu_engine"] = {"energy_abs_diff": abs(e - ref[0]),
-                                           "grad_max_abs_diff": float(np.max(np.abs(g - ref[1])))}
-        del sh
-        torch.cuda.empty_cache()
-        if world == 1:
-            out["rank_kernels_n33_8_ranks"] = shard_rank_kernels(33, 3, L)
     except Exception as exc:  # report, do not hide
+        out["reference_error"] = str(exc)
+    sh = None
+    try:
+        sh = ShardedEngine(n, L, h, **kw)
+    except Exception as exc:
         out["error"] = str(exc)
+        ok = False
+    if not all_ok(ok):
+        out.setdefault("error", "a rank could not set up the sharded engine")
+        return out
+    e, g = sh.energy_and_grad(p)
+    steps = max(2, min(args.steps, 5))
+    barrier()
+    s, t = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(steps):
+        sh.energy_and_grad(p)
+    t.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(s.elapsed_time(t) / steps)
+    out.update({"workload": f"energy_and_grad n={n} L={L} h={h}", "ranks": how, "ms_per_call": ms,
+                "energy_and_grad_per_s": 1000.0 / ms, "energy": e,
+                "timing": "CUDA events over host-parameter calls (host result), max over ranks"})
+    if ref is not None:
+        out["vs_single_gpu_engine"] = {"energy_abs_diff": abs(e - ref[0]),
+                                       "grad_max_abs_diff": float(np.max(np.abs(g - ref[1])))}
+    del sh
+    torch.cuda.empty_cache()
+    if world == 1:
+        try:
+            out["rank_kernels_n33_8_ranks"] = shard_rank_kernels(33, 3, L)
+        except Exception as exc:  # report, do not hide
+            out["rank_kernels_error"] = str(exc)
     return out
 
 
