@@ -76,6 +76,8 @@ def parse_args():
     ap.add_argument("--no-small", action="store_true", help="skip the n=12 Adam and n=20 autograd sections")
     ap.add_argument("--no-autotune", action="store_true", help="keep the planner's default plan (no autotune)")
     ap.add_argument("--no-sharded", action="store_true", help="skip the sharded single-circuit section")
+    ap.add_argument("--shard-rank-kernels", default=None, metavar="N,G",
+                    help="only time one rank's sharded kernels for N qubits over 2^G ranks, print them, exit")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="reference arm: skip timing the reference's sm_100a rebuild on the GPU")
     return ap.parse_args()
@@ -664,6 +666,10 @@ def main():
     import torch
 
     torch.cuda.set_device(local_rank)
+    if args.shard_rank_kernels:
+        ns, gs = (int(v) for v in args.shard_rank_kernels.split(","))
+        print(json.dumps(shard_rank_kernels(ns, gs, args.layers)), flush=True)
+        return 0
     dist = None
     if world > 1:
         import datetime

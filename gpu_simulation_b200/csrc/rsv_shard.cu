@@ -512,7 +512,10 @@ __global__ void __launch_bounds__(kXThreads) ring_unpack_kernel(const double2 *_
        v += static_cast<u64>(gridDim.x) * kXThreads) {
     const u64 x = ring_inv((static_cast<u64>(rank) << nloc) | v, n);
     const u64 rs = (x >> (n - 2 * G)) & (N - 1);
-    __stcs(&psi_c[v], __ldcs(&recv[rs * B + (x & (B - 1))]));
+    // a warp's 32 reads fall in one 64-amplitude window, half of each 32-byte
+    // sector; the other half is read by the warp with y bit 5 flipped, so the
+    // loads keep their lines in L1 (__ldg) rather than streaming them
+    __stcs(&psi_c[v], __ldg(&recv[rs * B + (x & (B - 1))]));
   }
 }
 
