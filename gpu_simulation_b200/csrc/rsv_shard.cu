@@ -20,6 +20,7 @@
 // layer's local wires go in any grouping of passes.
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <string>
 
 #include <cuda_runtime.h>
@@ -100,12 +101,45 @@ __device__ __forceinline__ void xpose2(double2 *sm, int tau, double2 (&a)[kR], d
   __syncthreads();
 }
 
-// (x0, x1) <- RZ(phi) RY(theta) (x0, x1), c = (cos t/2, sin t/2, cos p/2, sin p/2)
+// Forward gate in the form the shard kernels apply it: (1/f) RZ'(phi) RY(theta)
+// with RZ' = diag(1, e^{i phi}) = e^{i phi/2} RZ(phi) and f = cos(theta/2) or
+// sin(theta/2), whichever is larger in magnitude, so that RY/f is
+// [[1, -k], [k, 1]] (k = tan, mode +1) or [[k, -1], [1, k]] (k = cot, mode -1):
+// four multiply-adds for the rotation and four for the phase instead of
+// sixteen.  The state differs from the true one by the scalar prod 1/f times a
+// global phase; the host multiplies the energy and the gradient by prod f^2
+// (the phase cancels in both).
+// fwd_coef: (cos t/2, sin t/2, cos p/2, sin p/2) -> (k, mode, cos p, sin p)
+__device__ __forceinline__ double4 fwd_coef(const double4 c) {
+  const bool plus = fabs(c.x) >= fabs(c.y);
+  return make_double4(plus ? c.y / c.x : c.x / c.y, plus ? 1.0 : -1.0, c.z * c.z - c.w * c.w, 2.0 * c.z * c.w);
+}
+// adj_coef: (cos t/2, sin t/2, cos p, sin p) for the exact adjoint (RY^dagger
+// and diag(1, e^{-i phi}) = e^{-i phi/2} RZ^dagger: the common phase of psi and
+// lambda cancels in every gradient sum)
+__device__ __forceinline__ double4 adj_coef(const double4 c) {
+  return make_double4(c.x, c.y, c.z * c.z - c.w * c.w, 2.0 * c.z * c.w);
+}
+
+__device__ __forceinline__ void phase_mul(double2 &x, double cp, double sp) {
+  x = make_double2(fma(x.x, cp, -x.y * sp), fma(x.x, sp, x.y * cp));
+}
+
+// (x0, x1) <- (1/f) RZ'(phi) RY(theta) (x0, x1), c = fwd_coef(...)
+template <bool PLUS>
 __device__ __forceinline__ void rot_pair(const double4 c, double2 &x0, double2 &x1) {
-  const double2 y0 = make_double2(c.x * x0.x - c.y * x1.x, c.x * x0.y - c.y * x1.y);
-  const double2 y1 = make_double2(c.y * x0.x + c.x * x1.x, c.y * x0.y + c.x * x1.y);
-  x0 = make_double2(c.z * y0.x + c.w * y0.y, c.z * y0.y - c.w * y0.x);  // e^{-i p/2}
-  x1 = make_double2(c.z * y1.x - c.w * y1.y, c.z * y1.y + c.w * y1.x);  // e^{+i p/2}
+  const double k = c.x;
+  double2 y0, y1;
+  if (PLUS) {
+    y0 = make_double2(fma(-k, x1.x, x0.x), fma(-k, x1.y, x0.y));
+    y1 = make_double2(fma(k, x0.x, x1.x), fma(k, x0.y, x1.y));
+  } else {
+    y0 = make_double2(fma(k, x0.x, -x1.x), fma(k, x0.y, -x1.y));
+    y1 = make_double2(fma(k, x1.x, x0.x), fma(k, x1.y, x0.y));
+  }
+  phase_mul(y1, c.z, c.w);
+  x0 = y0;
+  x1 = y1;
 }
 
 // Inverse walk of one wire on a psi pair (a0, a1) and lambda pair (l0, l1)
@@ -114,10 +148,8 @@ __device__ __forceinline__ void rot_pair(const double4 c, double2 &x0, double2 &
 __device__ __forceinline__ void unrot_pair(const double4 c, double2 &a0, double2 &a1, double2 &l0, double2 &l1,
                                            double &gt, double &gp) {
   gp += fma(l0.x, a0.y, -l0.y * a0.x) - fma(l1.x, a1.y, -l1.y * a1.x);
-  a0 = make_double2(c.z * a0.x - c.w * a0.y, c.z * a0.y + c.w * a0.x);
-  a1 = make_double2(c.z * a1.x + c.w * a1.y, c.z * a1.y - c.w * a1.x);
-  l0 = make_double2(c.z * l0.x - c.w * l0.y, c.z * l0.y + c.w * l0.x);
-  l1 = make_double2(c.z * l1.x + c.w * l1.y, c.z * l1.y - c.w * l1.x);
+  phase_mul(a1, c.z, -c.w);  // diag(1, e^{-i phi}) on psi and lambda
+  phase_mul(l1, c.z, -c.w);
   gt += fma(l1.x, a0.x, l1.y * a0.y) - fma(l0.x, a1.x, l0.y * a1.y);
   const double2 b0 = make_double2(c.x * a0.x + c.y * a1.x, c.x * a0.y + c.y * a1.y);
   const double2 b1 = make_double2(c.x * a1.x - c.y * a0.x, c.x * a1.y - c.y * a0.y);
@@ -135,9 +167,15 @@ __device__ __forceinline__ void fwd_gates(const TileArgs &A, const double4 *cf, 
   for (int j = 0; j < NB; ++j) {
     if (A.wire[TB0 + j] < 0) continue;
     const double4 c = cf[TB0 + j];
+    if (c.y > 0.0) {
 #pragma unroll
-    for (int r = 0; r < kR; ++r)
-      if (!(r & (1 << j))) rot_pair(c, a[r], a[r | (1 << j)]);
+      for (int r = 0; r < kR; ++r)
+        if (!(r & (1 << j))) rot_pair<true>(c, a[r], a[r | (1 << j)]);
+    } else {
+#pragma unroll
+      for (int r = 0; r < kR; ++r)
+        if (!(r & (1 << j))) rot_pair<false>(c, a[r], a[r | (1 << j)]);
+    }
   }
 }
 
@@ -208,7 +246,7 @@ __global__ void __launch_bounds__(kRotThreads, kRotCtasPerSm) rot_kernel(const _
   __shared__ double2 sm[kTile];
   __shared__ double4 cf[kT];
   const int tau = threadIdx.x;
-  if (tau < kT) cf[tau] = A.wire[tau] >= 0 ? coef[A.layer * A.n + A.wire[tau]] : make_double4(1.0, 0.0, 1.0, 0.0);
+  if (tau < kT) cf[tau] = A.wire[tau] >= 0 ? fwd_coef(coef[A.layer * A.n + A.wire[tau]]) : make_double4(0.0, 1.0, 1.0, 0.0);
   u32 otau = 0;
 #pragma unroll
   for (int j = 0; j < 7; ++j)
@@ -257,7 +295,7 @@ __global__ void __launch_bounds__(kRotThreads, kAdjCtasPerSm) rot_adjoint_kernel
   __shared__ double4 cf[kT];
   __shared__ double rec[kRotThreads / 32][kRec];
   const int tau = threadIdx.x, lane = tau & 31, warp = tau >> 5;
-  if (tau < kT) cf[tau] = A.wire[tau] >= 0 ? coef[A.layer * A.n + A.wire[tau]] : make_double4(1.0, 0.0, 1.0, 0.0);
+  if (tau < kT) cf[tau] = A.wire[tau] >= 0 ? adj_coef(coef[A.layer * A.n + A.wire[tau]]) : make_double4(1.0, 0.0, 1.0, 0.0);
   for (int i = tau; i < (kRotThreads / 32) * kRec; i += kRotThreads) (&rec[0][0])[i] = 0.0;
   u32 otau = 0;
 #pragma unroll
@@ -478,7 +516,7 @@ __global__ void __launch_bounds__(kXThreads) ring_pack_kernel(const double2 *__r
   constexpr int N = 1 << G;
   double4 cf[G > 0 ? G : 1];
 #pragma unroll
-  for (int j = 0; j < G; ++j) cf[j] = coef[layer * n + (n - G + j)];
+  for (int j = 0; j < G; ++j) cf[j] = fwd_coef(coef[layer * n + (n - G + j)]);
   const int rpar = __popc(rank) & 1;
   for (u64 u = blockIdx.x * static_cast<u64>(kXThreads) + threadIdx.x; u < B;
        u += static_cast<u64>(gridDim.x) * kXThreads) {
@@ -489,7 +527,12 @@ __global__ void __launch_bounds__(kXThreads) ring_pack_kernel(const double2 *__r
     for (int j = 0; j < G; ++j)
 #pragma unroll
       for (int t = 0; t < N; ++t)
-        if (!(t & (1 << j))) rot_pair(cf[j], a[t], a[t | (1 << j)]);
+        if (!(t & (1 << j))) {
+          if (cf[j].y > 0.0)
+            rot_pair<true>(cf[j], a[t], a[t | (1 << j)]);
+          else
+            rot_pair<false>(cf[j], a[t], a[t | (1 << j)]);
+        }
     const int pi = (__popcll(u) & 1) ^ rpar;
 #pragma unroll
     for (int t = 0; t < N; ++t) {
@@ -562,7 +605,7 @@ __global__ void __launch_bounds__(kXThreads) ring_unpack_adjoint_kernel(
   double4 cf[G > 0 ? G : 1];
   if (layer >= 0) {
 #pragma unroll
-    for (int j = 0; j < G; ++j) cf[j] = coef[layer * n + (n - G + j)];
+    for (int j = 0; j < G; ++j) cf[j] = adj_coef(coef[layer * n + (n - G + j)]);
   }
   const int rpar = __popc(rank) & 1;
   double acc[kRecX];
@@ -827,6 +870,16 @@ extern "C" rsv_status rsv_shard_check(int num_qubits, int g) {
 extern "C" size_t rsv_shard_scratch_doubles(int num_qubits, int g) {
   if (geometry_error(num_qubits, g)) return 0;
   return kMaxGrid * std::max(kRec, 1 + 2 * kMaxG);
+}
+
+extern "C" double rsv_shard_result_scale(int num_qubits, int num_layers, const double *h_params) {
+  if (h_params == nullptr || num_qubits < 1 || num_layers < 1) return std::nan("");
+  double scale = 1.0;
+  for (int k = 0; k < num_qubits * num_layers; ++k) {
+    const double c = std::cos(0.5 * h_params[2 * k]), s = std::sin(0.5 * h_params[2 * k]);
+    scale *= std::max(c * c, s * s);
+  }
+  return scale;
 }
 
 extern "C" rsv_status rsv_shard_coef(int num_qubits, int num_layers, const double *d_params, double *d_coef,

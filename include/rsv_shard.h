@@ -25,9 +25,15 @@
  * all-to-all, ring_unpack.  The collectives are the caller's (NCCL
  * all_to_all_single over NVLink between ranks).
  *
+ * Forward gates are applied as (1/f) diag(1, e^{i phi}) RY(theta), f the larger
+ * in magnitude of cos(theta/2) and sin(theta/2): the rotation is two
+ * multiply-adds per amplitude and the phase four, and the state after the
+ * forward is the true one times prod_{l,w} 1/f_{l,w} times a global phase.
  * Per-rank results go to d_result, f64[2 + 2 n L]: [0] the energy terms of
  * energy_local, [1] the field terms of ring_unpack_adjoint, [2 + k] gradient
- * entry k.  The caller sums the ranks' vectors in rank order (deterministic).
+ * entry k, each prod 1/f^2 times its true value (the global phase cancels).
+ * The caller sums the ranks' vectors in rank order (deterministic) and
+ * multiplies the sum by rsv_shard_result_scale.
  * Every pointer is device memory of the current device; `stream` is a
  * cudaStream_t (NULL: the legacy default stream).  Calls are asynchronous.
  * Geometry limits: 0 <= g <= 3, n - 2g >= 12, n - g <= 31.
@@ -50,6 +56,11 @@ rsv_status rsv_shard_check(int num_qubits, int g);
 /* Doubles of scratch (d_scratch) the adjoint and energy calls need. */
 size_t rsv_shard_scratch_doubles(int num_qubits, int g);
 
+/* prod over the n L forward gates of f^2 = max(cos^2(theta/2), sin^2(theta/2)),
+ * from host parameters f64[2 n L]: the factor that turns the summed result
+ * vectors into the energy and gradient.  Host only; NaN for null params. */
+double rsv_shard_result_scale(int num_qubits, int num_layers, const double *h_params);
+
 /* d_coef[l*n + w] = (cos theta/2, sin theta/2, cos phi/2, sin phi/2) as 4
  * doubles, from d_params f64[2 n L] (reference host coefficients:
  * cpp/ising_cuda_rotation_kernels.cu:661-675). */
@@ -59,12 +70,14 @@ rsv_status rsv_shard_coef(int num_qubits, int num_layers, const double *d_params
 /* |0...0> in layout C on this rank's shard (2^(n-g) complex128). */
 rsv_status rsv_shard_init(int num_qubits, int g, int rank, double *d_psi, void *stream);
 
-/* RZ(phi) RY(theta) of layer `layer` on wires 0..n-g-1 (local in C), in place. */
+/* The forward gates of layer `layer` on wires 0..n-g-1 (local in C), in place. */
 rsv_status rsv_shard_rotate_local(int num_qubits, int g, int layer, const double *d_coef, double *d_psi,
                                   void *stream);
 
-/* Adjoint of rsv_shard_rotate_local on psi and lambda, writing the gradient of
- * wires 0..n-g-1 of `layer` to d_result (this rank's share). */
+/* The inverse walk of layer `layer` on wires 0..n-g-1 on psi and lambda: per
+ * wire the phi sum, diag(1, e^{-i phi}) (RZ^dagger up to a phase common to psi
+ * and lambda), the theta sum, RY^dagger; the sums go to d_result (this
+ * rank's share). */
 rsv_status rsv_shard_rotate_local_adjoint(int num_qubits, int g, int num_layers, int layer,
                                           const double *d_coef, double *d_psi, double *d_lam,
                                           double *d_scratch, double *d_result, void *stream);
@@ -74,8 +87,8 @@ rsv_status rsv_shard_rotate_local_adjoint(int num_qubits, int g, int num_layers,
 rsv_status rsv_shard_energy_local(int num_qubits, int g, int rank, double field, const double *d_psi,
                                   double *d_lam, double *d_scratch, double *d_result, void *stream);
 
-/* Forward ring exchange, sender side (layout S): RZ RY of layer `layer` on
- * wires n-g..n-1, then the amplitude of x goes to chunk rank_C(P(x)) of
+/* Forward ring exchange, sender side (layout S): the forward gates of layer
+ * `layer` on wires n-g..n-1, then the amplitude of x goes to chunk rank_C(P(x)) of
  * d_send (2^g chunks of 2^(n-2g) amplitudes, in the order of x bits [0, n-2g)). */
 rsv_status rsv_shard_ring_pack(int num_qubits, int g, int rank, int layer, const double *d_coef,
                                const double *d_psi_s, double *d_send, void *stream);
@@ -95,8 +108,8 @@ rsv_status rsv_shard_ring_pack_adjoint(int num_qubits, int g, int rank, const do
  * x = P^-1(y); with add_field_terms, lambda += -h sum_{w >= n-g} X'_w psi
  * (the X terms of the wires that are global in C, in the pre-ring frame:
  * masks {w, w+1}, {0, 1, n-1} for w = n-1) and d_result[1] = their energy
- * share; with layer >= 0, the adjoint of RZ RY of `layer` on wires n-g..n-1
- * and their gradient into d_result. */
+ * share; with layer >= 0, the inverse walk of `layer` on wires n-g..n-1
+ * (as in rsv_shard_rotate_local_adjoint) and their sums into d_result. */
 rsv_status rsv_shard_ring_unpack_adjoint(int num_qubits, int g, int rank, int num_layers, int layer,
                                          const double *d_coef, double field, int add_field_terms,
                                          const double *d_recv_psi, const double *d_recv_lam,

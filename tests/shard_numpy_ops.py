@@ -76,13 +76,16 @@ class Geometry:
 
 
 def _rot(a: np.ndarray, bit: int, c) -> None:
-    """RZ(phi) RY(theta) on local bit `bit` of the vector a, in place."""
+    """The forward gate on local bit `bit` of the vector a, in place, as the
+    shard kernels apply it: (1/f) diag(1, e^{i phi}) RY(theta), f the larger in
+    magnitude of cos(theta/2), sin(theta/2)."""
     ct, st, cp, sp = c
+    f = ct if abs(ct) >= abs(st) else st
     v = a.reshape(-1, 2, 1 << bit)
     x0, x1 = v[:, 0, :].copy(), v[:, 1, :].copy()
-    y0, y1 = ct * x0 - st * x1, st * x0 + ct * x1
-    v[:, 0, :] = y0 * (cp - 1j * sp)
-    v[:, 1, :] = y1 * (cp + 1j * sp)
+    y0, y1 = (ct * x0 - st * x1) / f, (st * x0 + ct * x1) / f
+    v[:, 0, :] = y0
+    v[:, 1, :] = y1 * (cp + 1j * sp) ** 2
 
 
 def _unrot(a: np.ndarray, l: np.ndarray, bit: int, c) -> tuple[float, float]:
@@ -92,8 +95,8 @@ def _unrot(a: np.ndarray, l: np.ndarray, bit: int, c) -> tuple[float, float]:
     a0, a1 = va[:, 0, :].copy(), va[:, 1, :].copy()
     l0, l1 = vl[:, 0, :].copy(), vl[:, 1, :].copy()
     gp = float(np.sum(np.imag(np.conj(l0) * a0)) - np.sum(np.imag(np.conj(l1) * a1)))
-    a0, a1 = a0 * (cp + 1j * sp), a1 * (cp - 1j * sp)
-    l0, l1 = l0 * (cp + 1j * sp), l1 * (cp - 1j * sp)
+    ph = (cp - 1j * sp) ** 2  # diag(1, e^{-i phi}): RZ^dagger up to a common phase
+    a1, l1 = a1 * ph, l1 * ph
     gt = float(np.sum(np.real(np.conj(l1) * a0)) - np.sum(np.real(np.conj(l0) * a1)))
     va[:, 0, :], va[:, 1, :] = ct * a0 + st * a1, ct * a1 - st * a0
     vl[:, 0, :], vl[:, 1, :] = ct * l0 + st * l1, ct * l1 - st * l0
@@ -109,6 +112,10 @@ class NumpyShardOps:
 
     def scratch_doubles(self, n: int, g: int) -> int:
         return 1
+
+    def result_scale(self, n: int, L: int, params: np.ndarray) -> float:
+        th = np.asarray(params, dtype=np.float64).reshape(-1, 2)[:, 0] / 2
+        return float(np.prod(np.maximum(np.cos(th) ** 2, np.sin(th) ** 2)))
 
     @staticmethod
     def _coef(coef, layer, n, w):
