@@ -107,7 +107,6 @@ _SIGNATURES = {
     # include/rsv_shard.h
     "rsv_shard_check": ([ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "rsv_shard_scratch_doubles": ([ctypes.c_int, ctypes.c_int], ctypes.c_size_t),
-    "rsv_shard_result_scale": ([ctypes.c_int, ctypes.c_int, ctypes.c_void_p], ctypes.c_double),
     "rsv_shard_coef": ([ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
                        ctypes.c_int),
     "rsv_shard_init": ([ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],

@@ -20,7 +20,6 @@
 // layer's local wires go in any grouping of passes.
 #include <algorithm>
 #include <atomic>
-#include <cmath>
 #include <string>
 
 #include <cuda_runtime.h>
@@ -106,9 +105,11 @@ __device__ __forceinline__ void xpose2(double2 *sm, int tau, double2 (&a)[kR], d
 // sin(theta/2), whichever is larger in magnitude, so that RY/f is
 // [[1, -k], [k, 1]] (k = tan, mode +1) or [[k, -1], [1, k]] (k = cot, mode -1):
 // four multiply-adds for the rotation and four for the phase instead of
-// sixteen.  The state differs from the true one by the scalar prod 1/f times a
-// global phase; the host multiplies the energy and the gradient by prod f^2
-// (the phase cancels in both).
+// sixteen.  Within a layer the state differs from the true one by the scalar
+// prod 1/f times a global phase; ring_pack, which ends every layer's gates,
+// multiplies by the layer's prod f, so each layer starts at the true scale
+// (no growth over many layers) and only the global phase remains, which
+// cancels in the energy and in every gradient sum.
 // fwd_coef: (cos t/2, sin t/2, cos p/2, sin p/2) -> (k, mode, cos p, sin p)
 __device__ __forceinline__ double4 fwd_coef(const double4 c) {
   const bool plus = fabs(c.x) >= fabs(c.y);
@@ -514,15 +515,29 @@ __global__ void __launch_bounds__(kXThreads) ring_pack_kernel(const double2 *__r
                                                               int layer, const double4 *__restrict__ coef,
                                                               u64 B) {
   constexpr int N = 1 << G;
+  __shared__ double layer_f;  // prod over the layer's wires of f (signed)
+  if (threadIdx.x == 0) {
+    double p = 1.0;
+    for (int w = 0; w < n; ++w) {
+      const double4 c = coef[layer * n + w];
+      p *= fabs(c.x) >= fabs(c.y) ? c.x : c.y;
+    }
+    layer_f = p;
+  }
   double4 cf[G > 0 ? G : 1];
 #pragma unroll
   for (int j = 0; j < G; ++j) cf[j] = fwd_coef(coef[layer * n + (n - G + j)]);
   const int rpar = __popc(rank) & 1;
+  __syncthreads();
+  const double sf = layer_f;
   for (u64 u = blockIdx.x * static_cast<u64>(kXThreads) + threadIdx.x; u < B;
        u += static_cast<u64>(gridDim.x) * kXThreads) {
     double2 a[N];
 #pragma unroll
-    for (int t = 0; t < N; ++t) a[t] = __ldcs(&psi_s[u + B * t]);
+    for (int t = 0; t < N; ++t) {
+      a[t] = __ldcs(&psi_s[u + B * t]);
+      a[t] = make_double2(sf * a[t].x, sf * a[t].y);
+    }
 #pragma unroll
     for (int j = 0; j < G; ++j)
 #pragma unroll
@@ -870,16 +885,6 @@ extern "C" rsv_status rsv_shard_check(int num_qubits, int g) {
 extern "C" size_t rsv_shard_scratch_doubles(int num_qubits, int g) {
   if (geometry_error(num_qubits, g)) return 0;
   return kMaxGrid * std::max(kRec, 1 + 2 * kMaxG);
-}
-
-extern "C" double rsv_shard_result_scale(int num_qubits, int num_layers, const double *h_params) {
-  if (h_params == nullptr || num_qubits < 1 || num_layers < 1) return std::nan("");
-  double scale = 1.0;
-  for (int k = 0; k < num_qubits * num_layers; ++k) {
-    const double c = std::cos(0.5 * h_params[2 * k]), s = std::sin(0.5 * h_params[2 * k]);
-    scale *= std::max(c * c, s * s);
-  }
-  return scale;
 }
 
 extern "C" rsv_status rsv_shard_coef(int num_qubits, int num_layers, const double *d_params, double *d_coef,

@@ -12,8 +12,8 @@ Each rank holds 2^(n-g) amplitudes in one of two layouts of the global index
 0..n-2g-1 and n-g..n-1 are.  One layer forward:
 
   1. ``rotate_local``: the gates of wires 0..n-g-1 (local in C), own tile
-     kernels, in tangent form: (1/f) diag(1, e^{i phi}) RY(theta), so the
-     results are rescaled once at the end by prod f^2;
+     kernels, in tangent form: (1/f) diag(1, e^{i phi}) RY(theta), the
+     layer's prod f restored in step 3;
   2. C -> S: one all-to-all of 2^(n-2g)-amplitude blocks, no packing;
   3. ``ring_pack``: the gates of wires n-g..n-1 (local in S) fused with the sort of
      every amplitude by the rank that owns its image under the CNOT ring;
@@ -64,10 +64,6 @@ class CudaShardOps:
 
     def scratch_doubles(self, n: int, g: int) -> int:
         return int(self._lib.rsv_shard_scratch_doubles(int(n), int(g)))
-
-    def result_scale(self, n: int, L: int, params: np.ndarray) -> float:
-        flat = np.ascontiguousarray(params, dtype=np.float64)
-        return float(self._lib.rsv_shard_result_scale(int(n), int(L), flat.ctypes.data))
 
     def coef(self, n, L, params, coef):
         check(self._lib.rsv_shard_coef(n, L, params.data_ptr(), coef.data_ptr(), self._stream(params)))
@@ -224,8 +220,6 @@ class ShardedEngine:
             flat = torch.from_numpy(np.ascontiguousarray(np.asarray(params, dtype=np.float64).reshape(-1)))
         if flat.numel() != self.num_params:
             raise ValueError(f"expected {self.num_params} parameters, got {flat.numel()}")
-        # the forward gates scale the state by prod 1/f (include/rsv_shard.h)
-        self._scale = self.ops.result_scale(self.n, self.L, flat.detach().cpu().numpy())
         for s in self.shards:
             s.params.copy_(flat, non_blocking=False)
             s.result.zero_()
@@ -274,7 +268,7 @@ class ShardedEngine:
                 self._swap_layout(both=True)
                 for s in self.shards:
                     ops.rotate_local_adjoint(n, g, self.L, layer, s.coef, s.psi, s.lam, s.scratch, s.result)
-        total = self._sum_results().cpu().numpy() * self._scale
+        total = self._sum_results().cpu().numpy()
         energy = float(total[0] + total[1])
         return energy, (total[2:].copy() if compute_gradient else None)
 

@@ -27,13 +27,13 @@
  *
  * Forward gates are applied as (1/f) diag(1, e^{i phi}) RY(theta), f the larger
  * in magnitude of cos(theta/2) and sin(theta/2): the rotation is two
- * multiply-adds per amplitude and the phase four, and the state after the
- * forward is the true one times prod_{l,w} 1/f_{l,w} times a global phase.
+ * multiply-adds per amplitude and the phase four.  ring_pack, which ends each
+ * layer's gates, multiplies by the layer's prod_w f_w, so after every layer
+ * the state is the true one times a global phase, which cancels in the energy
+ * and in every gradient sum.
  * Per-rank results go to d_result, f64[2 + 2 n L]: [0] the energy terms of
  * energy_local, [1] the field terms of ring_unpack_adjoint, [2 + k] gradient
- * entry k, each prod 1/f^2 times its true value (the global phase cancels).
- * The caller sums the ranks' vectors in rank order (deterministic) and
- * multiplies the sum by rsv_shard_result_scale.
+ * entry k.  The caller sums the ranks' vectors in rank order (deterministic).
  * Every pointer is device memory of the current device; `stream` is a
  * cudaStream_t (NULL: the legacy default stream).  Calls are asynchronous.
  * Geometry limits: 0 <= g <= 3, n - 2g >= 12, n - g <= 31.
@@ -55,11 +55,6 @@ rsv_status rsv_shard_check(int num_qubits, int g);
 
 /* Doubles of scratch (d_scratch) the adjoint and energy calls need. */
 size_t rsv_shard_scratch_doubles(int num_qubits, int g);
-
-/* prod over the n L forward gates of f^2 = max(cos^2(theta/2), sin^2(theta/2)),
- * from host parameters f64[2 n L]: the factor that turns the summed result
- * vectors into the energy and gradient.  Host only; NaN for null params. */
-double rsv_shard_result_scale(int num_qubits, int num_layers, const double *h_params);
 
 /* d_coef[l*n + w] = (cos theta/2, sin theta/2, cos phi/2, sin phi/2) as 4
  * doubles, from d_params f64[2 n L] (reference host coefficients:
@@ -88,7 +83,7 @@ rsv_status rsv_shard_energy_local(int num_qubits, int g, int rank, double field,
                                   double *d_lam, double *d_scratch, double *d_result, void *stream);
 
 /* Forward ring exchange, sender side (layout S): the forward gates of layer
- * `layer` on wires n-g..n-1, then the amplitude of x goes to chunk rank_C(P(x)) of
+ * `layer` on wires n-g..n-1 and the layer's factor prod_w f_w, then the amplitude of x goes to chunk rank_C(P(x)) of
  * d_send (2^g chunks of 2^(n-2g) amplitudes, in the order of x bits [0, n-2g)). */
 rsv_status rsv_shard_ring_pack(int num_qubits, int g, int rank, int layer, const double *d_coef,
                                const double *d_psi_s, double *d_send, void *stream);

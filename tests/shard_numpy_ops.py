@@ -113,10 +113,6 @@ class NumpyShardOps:
     def scratch_doubles(self, n: int, g: int) -> int:
         return 1
 
-    def result_scale(self, n: int, L: int, params: np.ndarray) -> float:
-        th = np.asarray(params, dtype=np.float64).reshape(-1, 2)[:, 0] / 2
-        return float(np.prod(np.maximum(np.cos(th) ** 2, np.sin(th) ** 2)))
-
     @staticmethod
     def _coef(coef, layer, n, w):
         c = coef.numpy().reshape(-1, 4)[layer * n + w]
@@ -165,6 +161,8 @@ class NumpyShardOps:
     def ring_pack(self, n, g, rank, layer, coef, psi_s, send):
         G = Geometry(n, g)
         a = psi_s.numpy().copy()
+        cf = coef.numpy().reshape(-1, 4)[layer * n:(layer + 1) * n]
+        a *= float(np.prod(np.where(np.abs(cf[:, 0]) >= np.abs(cf[:, 1]), cf[:, 0], cf[:, 1])))
         for j in range(g):
             _rot(a, n - 2 * g + j, self._coef(coef, layer, n, n - g + j))
         x = G.global_s(rank)

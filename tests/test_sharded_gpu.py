@@ -121,6 +121,21 @@ def test_virtual_ranks_match_oracle(n, L, h, ranks):
     np.testing.assert_allclose(g, g_ref, atol=1e-10, rtol=0)
 
 
+def test_many_layers_keep_their_scale():
+    """Forward gates run in tangent form ((1/f) RY, f >= 1/sqrt(2)); each
+    layer's ring exchange restores the layer's prod f, so 96 layers with every
+    theta near pi/2 (the largest 1/f) neither overflow nor lose accuracy."""
+    n, L, h, ranks = 14, 96, 0.9, 2
+    rng = np.random.default_rng(96)
+    p = rng.uniform(0, 2 * np.pi, (L, n, 2))
+    p[..., 0] = np.pi / 2 + rng.uniform(-0.01, 0.01, (L, n))
+    p = p.reshape(-1)
+    e, g = ShardedEngine(n, L, h, virtual_ranks=ranks).energy_and_grad(p)
+    e_ref, g_ref = oracle.energy_and_grad(n, L, h, p)
+    assert np.isfinite(e) and abs(e - e_ref) < 1e-10
+    np.testing.assert_allclose(g, g_ref, atol=1e-10, rtol=0)
+
+
 @pytest.mark.parametrize("n,L,h,ranks", [(24, 4, 1.0, 4), (26, 4, 0.8, 8), (28, 4, 1.0, 2)])
 def test_virtual_ranks_match_single_gpu_engine(n, L, h, ranks):
     p = np.random.default_rng(7).uniform(0, 2 * np.pi, 2 * n * L)
