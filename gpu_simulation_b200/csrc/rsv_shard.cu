@@ -162,6 +162,38 @@ __device__ __forceinline__ void unrot_pair(const double4 c, double2 &a0, double2
   l1 = m1;
 }
 
+// As unrot_pair with RY^dagger in tangent form, RY^dagger / f: [[1, k], [-k, 1]]
+// (PLUS, f = cos, k = tan) or [[k, 1], [-1, k]] (f = sin, k = cot); c =
+// (k, mode, cos phi, sin phi).  psi and lambda come out scaled by 1/f each, so
+// the sums of every later gate of the pass are 1/f^2 too large; the pass
+// corrects each gate's sums by the product of f^2 over the gates before it and
+// restores psi and lambda with the product of f when it stores them.
+template <bool PLUS>
+__device__ __forceinline__ void unrot_pair_tan(const double4 c, double2 &a0, double2 &a1, double2 &l0, double2 &l1,
+                                               double &gt, double &gp) {
+  gp += fma(l0.x, a0.y, -l0.y * a0.x) - fma(l1.x, a1.y, -l1.y * a1.x);
+  phase_mul(a1, c.z, -c.w);  // diag(1, e^{-i phi}) on psi and lambda
+  phase_mul(l1, c.z, -c.w);
+  gt += fma(l1.x, a0.x, l1.y * a0.y) - fma(l0.x, a1.x, l0.y * a1.y);
+  const double k = c.x;
+  double2 b0, b1, m0, m1;
+  if (PLUS) {
+    b0 = make_double2(fma(k, a1.x, a0.x), fma(k, a1.y, a0.y));
+    b1 = make_double2(fma(-k, a0.x, a1.x), fma(-k, a0.y, a1.y));
+    m0 = make_double2(fma(k, l1.x, l0.x), fma(k, l1.y, l0.y));
+    m1 = make_double2(fma(-k, l0.x, l1.x), fma(-k, l0.y, l1.y));
+  } else {
+    b0 = make_double2(fma(k, a0.x, a1.x), fma(k, a0.y, a1.y));
+    b1 = make_double2(fma(k, a1.x, -a0.x), fma(k, a1.y, -a0.y));
+    m0 = make_double2(fma(k, l0.x, l1.x), fma(k, l0.y, l1.y));
+    m1 = make_double2(fma(k, l1.x, -l0.x), fma(k, l1.y, -l0.y));
+  }
+  a0 = b0;
+  a1 = b1;
+  l0 = m0;
+  l1 = m1;
+}
+
 template <int TB0, int NB>
 __device__ __forceinline__ void fwd_gates(const TileArgs &A, const double4 *cf, double2 (&a)[kR]) {
 #pragma unroll
@@ -180,31 +212,44 @@ __device__ __forceinline__ void fwd_gates(const TileArgs &A, const double4 *cf, 
   }
 }
 
-// adjoint gates of tile bits TB0..TB0+NB-1; their sums are reduced over the
-// warp and added to the warp's row of the CTA record
+// adjoint gates of tile bits TB0..TB0+NB-1 (tangent form, cf from
+// adj_tan_coef); their sums are corrected by kap (the product of f^2 of the
+// pass's earlier gates), reduced over the warp and added to the warp's row of
+// the CTA record
 template <int TB0, int NB>
-__device__ __forceinline__ void adj_gates(const TileArgs &A, const double4 *cf, double2 (&a)[kR], double2 (&l)[kR],
-                                          double *rec_row, int lane) {
+__device__ __forceinline__ void adj_gates(const TileArgs &A, const double4 *cf, const double *kap, double2 (&a)[kR],
+                                          double2 (&l)[kR], double *rec_row, int lane) {
 #pragma unroll
   for (int j = 0; j < NB; ++j) {
     if (A.wire[TB0 + j] < 0) continue;
     const double4 c = cf[TB0 + j];
     // four partial sums each: the eight pairs' terms are not one dependent chain
     double gt4[4] = {0.0, 0.0, 0.0, 0.0}, gp4[4] = {0.0, 0.0, 0.0, 0.0};
-    int q = 0;
+    if (c.y > 0.0) {
+      int q = 0;
 #pragma unroll
-    for (int r = 0; r < kR; ++r)
-      if (!(r & (1 << j))) {
-        unrot_pair(c, a[r], a[r | (1 << j)], l[r], l[r | (1 << j)], gt4[q & 3], gp4[q & 3]);
-        ++q;
-      }
+      for (int r = 0; r < kR; ++r)
+        if (!(r & (1 << j))) {
+          unrot_pair_tan<true>(c, a[r], a[r | (1 << j)], l[r], l[r | (1 << j)], gt4[q & 3], gp4[q & 3]);
+          ++q;
+        }
+    } else {
+      int q = 0;
+#pragma unroll
+      for (int r = 0; r < kR; ++r)
+        if (!(r & (1 << j))) {
+          unrot_pair_tan<false>(c, a[r], a[r | (1 << j)], l[r], l[r | (1 << j)], gt4[q & 3], gp4[q & 3]);
+          ++q;
+        }
+    }
     double gt = (gt4[0] + gt4[1]) + (gt4[2] + gt4[3]);
     double gp = (gp4[0] + gp4[1]) + (gp4[2] + gp4[3]);
     gt = warp_sum(gt);
     gp = warp_sum(gp);
     if (lane == 0) {
-      rec_row[2 * (TB0 + j)] += gt;
-      rec_row[2 * (TB0 + j) + 1] += gp;
+      const double kp = kap[TB0 + j];
+      rec_row[2 * (TB0 + j)] += gt * kp;
+      rec_row[2 * (TB0 + j) + 1] += gp * kp;
     }
   }
 }
@@ -294,9 +339,30 @@ __global__ void __launch_bounds__(kRotThreads, kAdjCtasPerSm) rot_adjoint_kernel
                                                                   double *__restrict__ records) {
   extern __shared__ double2 sm2[];
   __shared__ double4 cf[kT];
+  __shared__ double kap[kT];
+  __shared__ double pass_f;
   __shared__ double rec[kRotThreads / 32][kRec];
   const int tau = threadIdx.x, lane = tau & 31, warp = tau >> 5;
-  if (tau < kT) cf[tau] = A.wire[tau] >= 0 ? adj_coef(coef[A.layer * A.n + A.wire[tau]]) : make_double4(1.0, 0.0, 1.0, 0.0);
+  if (tau == 0) {
+    // the pass's gates in the order they are undone: layout A (tile bits
+    // 7..10), B (3..6), C (0..2)
+    constexpr int order[kT] = {7, 8, 9, 10, 3, 4, 5, 6, 0, 1, 2};
+    double run = 1.0, fprod = 1.0;
+    for (int i = 0; i < kT; ++i) {
+      const int tb = order[i];
+      cf[tb] = make_double4(0.0, 1.0, 1.0, 0.0);
+      kap[tb] = 1.0;
+      if (A.wire[tb] < 0) continue;
+      const double4 c = coef[A.layer * A.n + A.wire[tb]];
+      const bool plus = fabs(c.x) >= fabs(c.y);
+      const double f = plus ? c.x : c.y;
+      cf[tb] = make_double4(plus ? c.y / c.x : c.x / c.y, plus ? 1.0 : -1.0, c.z * c.z - c.w * c.w, 2.0 * c.z * c.w);
+      kap[tb] = run;
+      run *= f * f;
+      fprod *= f;
+    }
+    pass_f = fprod;
+  }
   for (int i = tau; i < (kRotThreads / 32) * kRec; i += kRotThreads) (&rec[0][0])[i] = 0.0;
   u32 otau = 0;
 #pragma unroll
@@ -314,18 +380,24 @@ __global__ void __launch_bounds__(kRotThreads, kAdjCtasPerSm) rot_adjoint_kernel
       a[r] = __ldcs(&psi[base | reg_off(r, rb)]);
       l[r] = __ldcs(&lam[base | reg_off(r, rb)]);
     }
-    adj_gates<7, 4>(A, cf, a, l, rec[warp], lane);
+    adj_gates<7, 4>(A, cf, kap, a, l, rec[warp], lane);
     bool from_b = false;
     if (A.need_b) {
       xpose2<0, 1>(sm2, tau, a, l);
-      adj_gates<3, 4>(A, cf, a, l, rec[warp], lane);
+      adj_gates<3, 4>(A, cf, kap, a, l, rec[warp], lane);
       if (A.need_c) {
         xpose2<1, 2>(sm2, tau, a, l);
-        adj_gates<0, 3>(A, cf, a, l, rec[warp], lane);
+        adj_gates<0, 3>(A, cf, kap, a, l, rec[warp], lane);
         xpose2<2, 0>(sm2, tau, a, l);
       } else {
         from_b = true;
       }
+    }
+    const double sf = pass_f;  // back to the true scale
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+      a[r] = make_double2(sf * a[r].x, sf * a[r].y);
+      l[r] = make_double2(sf * l[r].x, sf * l[r].y);
     }
     // the store addresses are derived again here rather than kept live from
     // the loads (32 addresses would not fit next to the 64 amplitudes)
