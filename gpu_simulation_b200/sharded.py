@@ -169,6 +169,8 @@ class ShardedEngine:
         if device is None:
             device = torch.device("cuda", torch.cuda.current_device())
         self.device = torch.device(device)
+        if self.device.type == "cuda" and self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
         self.local_size = 1 << (self.n - self.g)
         self.block = 1 << (self.n - 2 * self.g)
         scratch = self.ops.scratch_doubles(self.n, self.g)
@@ -255,6 +257,13 @@ class ShardedEngine:
 
     def energy_and_grad(self, params, compute_gradient: bool = True):
         """(energy, gradient f64[2nL] or None), the same on every rank."""
+        if self.device.type == "cuda":
+            # the library launches on the current device: make it the shards' device
+            with self._torch.cuda.device(self.device):
+                return self._energy_and_grad(params, compute_gradient)
+        return self._energy_and_grad(params, compute_gradient)
+
+    def _energy_and_grad(self, params, compute_gradient: bool):
         n, g, ops = self.n, self.g, self.ops
         self._load_params(params)
         self._forward()
