@@ -1307,6 +1307,27 @@ void validate_params(rsv_backend *B, const void *params, size_t num_params) {
   if (params == nullptr) invalid("params is null");
 }
 
+// A backend lives on the device that was current when it was created; every
+// entry point that touches its memory or launches makes that device current
+// for the call and restores the caller's device afterwards.
+class OnDevice {
+ public:
+  explicit OnDevice(int device) {
+    if (device < 0) return;
+    if (cudaGetDevice(&prev_) == cudaSuccess && prev_ != device && cudaSetDevice(device) == cudaSuccess)
+      changed_ = true;
+  }
+  ~OnDevice() {
+    if (changed_) cudaSetDevice(prev_);
+  }
+  OnDevice(const OnDevice &) = delete;
+  OnDevice &operator=(const OnDevice &) = delete;
+
+ private:
+  int prev_ = -1;
+  bool changed_ = false;
+};
+
 template <typename F>
 rsv_status guarded(F &&f) {
   try {
@@ -2044,6 +2065,7 @@ rsv_status rsv_create(int num_qubits, int num_layers, double field, const char *
 
 rsv_status rsv_destroy(rsv_backend *backend) {
   return guarded([&] {
+    const OnDevice on_device(backend ? backend->device : -1);
     if (backend == nullptr) return;
     cudaStreamSynchronize(backend->stream);
     for (auto &r : backend->recs) {
@@ -2060,6 +2082,7 @@ rsv_status rsv_energy_and_grad(rsv_backend *B, const double *params, size_t num_
                                int compute_gradient, double *energy_out, double *gradient_out,
                                void *stream) {
   return guarded([&] {
+    const OnDevice on_device(B ? B->device : -1);
     validate_params(B, params, num_params);
     if (energy_out == nullptr) invalid("energy_out is null");
     if (compute_gradient && gradient_out == nullptr) invalid("gradient_out is null");
@@ -2081,6 +2104,7 @@ rsv_status rsv_energy_and_grad(rsv_backend *B, const double *params, size_t num_
 rsv_status rsv_energy_and_grad_device(rsv_backend *B, const double *d_params, size_t num_params,
                                       double *d_energy_out, double *d_gradient_out, void *stream) {
   return guarded([&] {
+    const OnDevice on_device(B ? B->device : -1);
     validate_params(B, d_params, num_params);
     if (d_energy_out == nullptr) invalid("d_energy_out is null");
     cudaStream_t st = device_stream(stream);
@@ -2095,6 +2119,7 @@ rsv_status rsv_forward_device(rsv_backend *B, const double *d_params, size_t num
                               double *d_energy_out, unsigned long long *generation_out,
                               void *stream) {
   return guarded([&] {
+    const OnDevice on_device(B ? B->device : -1);
     validate_params(B, d_params, num_params);
     if (d_energy_out == nullptr) invalid("d_energy_out is null");
     cudaStream_t st = device_stream(stream);
@@ -2108,6 +2133,7 @@ rsv_status rsv_forward_device(rsv_backend *B, const double *d_params, size_t num
 rsv_status rsv_backward_device(rsv_backend *B, unsigned long long generation,
                                double *d_gradient_out, void *stream) {
   return guarded([&] {
+    const OnDevice on_device(B ? B->device : -1);
     if (B == nullptr) invalid("backend is null");
     if (d_gradient_out == nullptr) invalid("d_gradient_out is null");
     if (!B->forward_only_state || generation != B->generation)
@@ -2126,6 +2152,7 @@ rsv_status rsv_profile_energy_and_grad(rsv_backend *B, const double *params, siz
                                        int compute_gradient, double *energy_out,
                                        double *gradient_out, double *stage_ms_out) {
   return guarded([&] {
+    const OnDevice on_device(B ? B->device : -1);
     validate_params(B, params, num_params);
     if (energy_out == nullptr || stage_ms_out == nullptr) invalid("output pointer is null");
     if (compute_gradient && gradient_out == nullptr) invalid("gradient_out is null");
@@ -2189,6 +2216,7 @@ rsv_status rsv_benchmark_forward_graph(rsv_backend *B, const double *params, siz
                                        size_t repeats, double *normal_ms_out,
                                        double *graph_ms_out) {
   return guarded([&] {
+    const OnDevice on_device(B ? B->device : -1);
     validate_params(B, params, num_params);
     if (repeats == 0) invalid("repeats must be at least 1.");
     if (normal_ms_out == nullptr || graph_ms_out == nullptr) invalid("output pointer is null");
@@ -2272,6 +2300,7 @@ rsv_status rsv_launch_stats(rsv_backend *B, int *counts, double *total_ms, doubl
 
 rsv_status rsv_set_backward_mode(rsv_backend *B, int mode) {
   return guarded([&] {
+    const OnDevice on_device(B ? B->device : -1);
     if (B == nullptr) invalid("backend is null");
     check(cudaStreamSynchronize(B->stream), "backend synchronize");
     setup_plan(B, mode);
@@ -2280,6 +2309,7 @@ rsv_status rsv_set_backward_mode(rsv_backend *B, int mode) {
 
 rsv_status rsv_set_analytic_layers(rsv_backend *B, int max_layers) {
   return guarded([&] {
+    const OnDevice on_device(B ? B->device : -1);
     if (B == nullptr) invalid("backend is null");
     if (max_layers < 0 || max_layers > 3) invalid("max_layers must be in [0, 3]");
     check(cudaStreamSynchronize(B->stream), "backend synchronize");
@@ -2290,6 +2320,7 @@ rsv_status rsv_set_analytic_layers(rsv_backend *B, int max_layers) {
 
 rsv_status rsv_set_kernels(rsv_backend *B, int flags) {
   return guarded([&] {
+    const OnDevice on_device(B ? B->device : -1);
     if (B == nullptr) invalid("backend is null");
     if ((flags & ~(RSV_KERNELS_TMA | RSV_KERNELS_FUSED_ENERGY)) != 0) invalid("unknown kernel flags");
     check(cudaStreamSynchronize(B->stream), "backend synchronize");
@@ -2309,6 +2340,7 @@ rsv_status rsv_kernels(rsv_backend *B, int *flags_out, int *tma_passes_out) {
 rsv_status rsv_autotune(rsv_backend *B, const double *d_params, size_t num_params, int repeats, int flags,
                         void *stream) {
   return guarded([&] {
+    const OnDevice on_device(B ? B->device : -1);
     validate_params(B, d_params, num_params);
     if (repeats < 1 || repeats > 1000) invalid("repeats must be in [1, 1000]");
     if ((flags & ~RSV_AUTOTUNE_FORCE) != 0) invalid("unknown autotune flags");
@@ -2428,6 +2460,7 @@ rsv_status rsv_zgemm_batched(const void *d_a, const void *d_b, void *d_c, int di
 
 rsv_status rsv_set_field(rsv_backend *B, double field) {
   return guarded([&] {
+    const OnDevice on_device(B ? B->device : -1);
     if (B == nullptr) invalid("backend is null");
     if (!std::isfinite(field)) invalid("field is not finite");
     B->field = field;
@@ -2477,6 +2510,7 @@ rsv_status rsv_batch_create(int max_qubits, int slots, rsv_batch **out) {
 
 rsv_status rsv_batch_destroy(rsv_batch *batch) {
   return guarded([&] {
+    const OnDevice on_device(batch ? batch->device : -1);
     if (batch == nullptr) return;
     cudaStreamSynchronize(batch->stream);
     cudaStreamDestroy(batch->stream);
@@ -2487,6 +2521,7 @@ rsv_status rsv_batch_destroy(rsv_batch *batch) {
 rsv_status rsv_batch_set_circuits(rsv_batch *batch, int count, const int *num_qubits,
                                   const int *num_layers, const double *fields) {
   return guarded([&] {
+    const OnDevice on_device(batch ? batch->device : -1);
     if (batch == nullptr) invalid("batch is null");
     batch_set_circuits(batch, count, num_qubits, num_layers, fields);
   });
@@ -2505,6 +2540,7 @@ rsv_status rsv_batch_info(rsv_batch *batch, int *count, size_t *num_params, int 
 
 rsv_status rsv_batch_set_active_slots(rsv_batch *batch, int slots) {
   return guarded([&] {
+    const OnDevice on_device(batch ? batch->device : -1);
     if (batch == nullptr) invalid("batch is null");
     if (slots < 1 || slots > batch->slots)
       invalid("slots must be in [1, " + std::to_string(batch->slots) + "]");
@@ -2514,6 +2550,7 @@ rsv_status rsv_batch_set_active_slots(rsv_batch *batch, int slots) {
 
 rsv_status rsv_batch_set_cluster(rsv_batch *batch, int cluster) {
   return guarded([&] {
+    const OnDevice on_device(batch ? batch->device : -1);
     if (batch == nullptr) invalid("batch is null");
     if (cluster != 1 && cluster != 2 && cluster != 4 && cluster != 8) invalid("cluster must be 1, 2, 4 or 8");
     if (cluster > batch->slots) invalid("cluster exceeds the scratch slots");
@@ -2536,6 +2573,7 @@ rsv_status rsv_batch_cluster(rsv_batch *batch, int *cluster_out, int *groups_out
 rsv_status rsv_batch_run_device(rsv_batch *batch, const double *d_params, double *d_energy_out,
                                 double *d_gradient_out, void *stream) {
   return guarded([&] {
+    const OnDevice on_device(batch ? batch->device : -1);
     if (batch == nullptr) invalid("batch is null");
     batch_run(batch, d_params, d_energy_out, d_gradient_out, static_cast<cudaStream_t>(stream));
   });
@@ -2546,6 +2584,7 @@ rsv_status rsv_batch_energy_and_grad(rsv_batch *batch, int count, const int *num
                                      const double *params, size_t num_params,
                                      double *energy_out, double *gradient_out, void *stream) {
   return guarded([&] {
+    const OnDevice on_device(batch ? batch->device : -1);
     if (batch == nullptr) invalid("batch is null");
     batch_set_circuits(batch, count, num_qubits, num_layers, fields);
     if (num_params != batch->num_params)

@@ -58,7 +58,10 @@ int rsv_num_stages(void);
 const char *rsv_stage_name(int i);
 
 /*
- * Create a backend bound to the current CUDA device.
+ * Create a backend bound to the current CUDA device.  Later calls on the
+ * backend run on that device whichever device is current when they are made
+ * (the caller's current device is restored before they return); stream
+ * arguments must belong to it.
  * Replaces RingIsingCudaBackend::RingIsingCudaBackend
  * (reference cpp/ising_cuda_backend.hpp:26-29, cpp/ising_cuda_backend.cu:388-404,
  *  bound at cpp/ising_cuda_bindings.cpp:74-80).
@@ -346,7 +349,8 @@ unsigned long long rsv_ring_map(unsigned long long index, int num_qubits, int in
 typedef struct rsv_batch rsv_batch;
 
 /* Handle whose scratch holds circuits of up to max_qubits qubits; slots = the
- * number of circuits in flight (0 = one per SM). */
+ * number of circuits in flight (0 = one per SM).  Bound to the current
+ * device as rsv_create is. */
 rsv_status rsv_batch_create(int max_qubits, int slots, rsv_batch **out);
 rsv_status rsv_batch_destroy(rsv_batch *batch);
 
