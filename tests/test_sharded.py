@@ -170,3 +170,17 @@ def test_many_layers_keep_their_scale():
     e_ref, g_ref = oracle.energy_and_grad(n, L, h, p)
     assert np.isfinite(e) and abs(e - e_ref) < 1e-10
     np.testing.assert_allclose(g, g_ref, atol=1e-10, rtol=0)
+
+
+def test_edge_cases_and_successive_calls():
+    """h = 0 and L = 1, parameters as a tensor, and calls with different angles
+    in a row on the same engine (every call starts from |0...0>)."""
+    n = 16
+    for L, h, ranks in ((1, 0.0, 4), (3, 1.2, 2)):
+        eng = _engine(n, L, h, ranks)
+        for seed in (1, 2):
+            p = np.random.default_rng(seed).uniform(0, 2 * np.pi, 2 * n * L)
+            e_ref, g_ref = oracle.energy_and_grad(n, L, h, p)
+            e, g = eng.energy_and_grad(torch.tensor(p))
+            assert abs(e - e_ref) < 1e-10
+            np.testing.assert_allclose(g, g_ref, atol=1e-10, rtol=0)

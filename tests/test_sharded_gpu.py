@@ -156,3 +156,18 @@ def test_virtual_ranks_match_single_gpu_engine(n, L, h, ranks):
 def test_cuda_ops_refuse_cpu_tensors():
     with pytest.raises(ValueError):
         CudaShardOps().init(12, 0, 0, torch.zeros(4096, dtype=torch.complex128))
+
+
+def test_edge_cases_and_successive_calls():
+    """h = 0 and L = 1, parameters as a CUDA tensor, and calls with different
+    angles in a row on the same engine (every call starts from |0...0>)."""
+    n = 16
+    for L, h, ranks in ((1, 0.0, 4), (3, 1.2, 2)):
+        eng = ShardedEngine(n, L, h, virtual_ranks=ranks)
+        for seed in (1, 2):
+            p = np.random.default_rng(seed).uniform(0, 2 * np.pi, 2 * n * L)
+            e_ref, g_ref = oracle.energy_and_grad(n, L, h, p)
+            e, g = eng.energy_and_grad(torch.tensor(p, device="cuda"))
+            assert abs(e - e_ref) < 1e-10
+            np.testing.assert_allclose(g, g_ref, atol=1e-10, rtol=0)
+            assert abs(eng.energy(p) - e_ref) < 1e-10
