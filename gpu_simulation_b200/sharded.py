@@ -283,3 +283,40 @@ class ShardedEngine:
 
     def energy(self, params) -> float:
         return self.energy_and_grad(params, compute_gradient=False)[0]
+
+
+def _autograd_function():
+    import torch
+
+    class ShardedRingIsingEnergy(torch.autograd.Function):
+        """Energy of the ring-Ising ansatz through a ``ShardedEngine``, for
+        torch optimisers on circuits too large for one GPU.  The adjoint sweep
+        yields the energy and the whole gradient in one call, so the forward
+        keeps the gradient and the backward only scales it by the incoming
+        grad; every rank gets the same energy and gradient."""
+
+        @staticmethod
+        def forward(ctx, params, engine):
+            energy, grad = engine.energy_and_grad(params.detach())
+            ctx.shape = params.shape
+            ctx.save_for_backward(torch.as_tensor(grad, dtype=params.dtype, device=params.device))
+            return torch.tensor(energy, dtype=params.dtype, device=params.device)
+
+        @staticmethod
+        def backward(ctx, grad_output):
+            (grad,) = ctx.saved_tensors
+            return (grad * grad_output).reshape(ctx.shape), None
+
+    return ShardedRingIsingEnergy
+
+
+_SHARDED_FN = None
+
+
+def sharded_ring_ising_energy(params, engine: ShardedEngine):
+    """Differentiable energy (0-d tensor) of params of shape (L, n, 2) or flat,
+    evaluated by ``engine`` (a ``ShardedEngine``)."""
+    global _SHARDED_FN
+    if _SHARDED_FN is None:
+        _SHARDED_FN = _autograd_function()
+    return _SHARDED_FN.apply(params, engine)

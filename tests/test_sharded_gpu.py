@@ -171,3 +171,23 @@ def test_edge_cases_and_successive_calls():
             assert abs(e - e_ref) < 1e-10
             np.testing.assert_allclose(g, g_ref, atol=1e-10, rtol=0)
             assert abs(eng.energy(p) - e_ref) < 1e-10
+
+
+def test_autograd_function_matches_single_gpu_autograd():
+    from gpu_simulation_b200 import ring_ising_energy
+    from gpu_simulation_b200.sharded import sharded_ring_ising_energy
+
+    n, L, h = 16, 3, 0.8
+    p0 = np.random.default_rng(31).uniform(0, 2 * np.pi, (L, n, 2))
+    a = torch.tensor(p0, device="cuda", requires_grad=True)
+    b = torch.tensor(p0, device="cuda", requires_grad=True)
+    eng = Engine(n, L, h)
+    try:
+        ea = ring_ising_energy(a, eng)
+        ea.backward()
+    finally:
+        eng.close()
+    eb = sharded_ring_ising_energy(b, ShardedEngine(n, L, h, virtual_ranks=4))
+    eb.backward()
+    assert abs(float(ea.detach()) - float(eb.detach())) < 1e-10
+    np.testing.assert_allclose(b.grad.cpu().numpy(), a.grad.cpu().numpy(), atol=1e-10, rtol=0)
