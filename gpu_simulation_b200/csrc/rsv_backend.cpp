@@ -120,21 +120,29 @@ Tile antipodal_tile(int n) {
 }
 
 // Split wires [lo, n) into high tiles with `c` contiguous low bits each;
-// c is chosen to minimise the number of passes, then maximised (longer DRAM
-// segments), unless force_c (2..10) fixes it (the autotuner's candidates).
-// Returns the tiles (gates on the split wires).
-std::vector<Tile> high_tiles(int n, int lo, int min_c = 2, int force_c = 0) {
+// c is chosen to minimise the number of passes, then -- with wide_last, for
+// the forward tiles of the checkpoint schedule -- to leave the last tile at
+// most 8 gated wires (at least 4 contiguous low bits: its backward half tile
+// then runs on the tensor-copy kernel and takes the fused field terms), then
+// maximised (longer DRAM segments), unless force_c (2..10) fixes it (the
+// autotuner's candidates).  Returns the tiles (gates on the split wires).
+std::vector<Tile> high_tiles(int n, int lo, int min_c = 2, int force_c = 0, bool wide_last = false) {
   std::vector<Tile> out;
   const int m = n - lo;
   if (m <= 0) return out;
   int best_c = min_c, best_passes = 1 << 30;
+  bool best_wide = false;
   for (int c = min_c; c <= 10; ++c) {
     const int g = 12 - c;
     if (c > lo) break;  // contiguity bits must lie below the gated wires
     const int passes = (m + g - 1) / g;
-    if (passes < best_passes || (passes == best_passes && c > best_c)) {
+    const bool wide = wide_last && m - (passes - 1) * g <= 8;
+    const bool better = passes < best_passes ||
+                        (passes == best_passes && (wide != best_wide ? wide : c > best_c));
+    if (better) {
       best_passes = passes;
       best_c = c;
+      best_wide = wide;
     }
   }
   if (force_c >= min_c && force_c <= std::min(10, lo)) best_c = force_c;
@@ -524,7 +532,7 @@ Plan make_plan_full(int n, int L, int sms, bool checkpoint, int force_c) {
     fwd_tiles.push_back(unit_tile(pl.phys, all_bits, real_wires));
     bwd_tiles.push_back(unit_tile(pl.phys, all_bits, real_wires));
   } else {
-    fwd_tiles = high_tiles(n, 12, 2, force_c);
+    fwd_tiles = high_tiles(n, 12, 2, force_c, checkpoint);
     fwd_tiles.insert(fwd_tiles.begin(), unit_tile(n, all_bits, all_bits));
     bwd_tiles = high_tiles(n, 11, 2, force_c);
     std::reverse(bwd_tiles.begin(), bwd_tiles.end());  // highest wires first
