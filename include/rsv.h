@@ -202,7 +202,7 @@ rsv_status rsv_launch_stats(rsv_backend *backend, int *counts, double *total_ms,
  * buffers of 16 * 2^n bytes; passes = 3 for 20 <= n <= 31) so that the
  * backward reads psi and writes only lambda.
  * RSV_BACKWARD_AUTO (the default of rsv_create) picks the checkpoint schedule
- * for n >= 13 while its buffers fit 96 GiB (and its allocation succeeds).
+ * for n >= 13 while its buffers fit 128 GiB (and its allocation succeeds).
  * rsv_set_backward_mode re-plans and reallocates (synchronises the backend's
  * stream); rsv_backward_mode reports the mode, whether the checkpoint schedule
  * is in use and the number of state buffers.  No reference counterpart.

@@ -66,3 +66,25 @@ def test_checkpoint_device_split_forward_backward():
     e.backward()
     assert abs(e.item() - e_ref) < TOL
     np.testing.assert_allclose(x.grad.cpu().numpy(), g_ref, atol=TOL, rtol=0)
+
+
+def test_largest_single_gpu_circuit_takes_the_checkpoint_schedule():
+    """n = 31, L = 4: the checkpoint schedule's four state buffers (128 GiB, as
+    many bytes as the reference's four buffers) are the automatic choice and
+    agree with the two-buffer uncompute schedule."""
+    import torch
+
+    torch.cuda.empty_cache()
+    n, L, h = 31, 4, 1.0
+    p = np.random.default_rng(31).uniform(0.0, 2.0 * np.pi, 2 * n * L)
+    eng = Engine(n, L, h)
+    try:
+        info = eng.backward_mode()
+        assert info["mode"] == "auto" and info["checkpoint"] and info["state_buffers"] == 4, info
+        e_ck, g_ck = eng.energy_and_grad(p)
+        eng.set_backward_mode("uncompute")
+        e_un, g_un = eng.energy_and_grad(p)
+    finally:
+        eng.close()
+    assert abs(e_ck - e_un) < 1e-12
+    np.testing.assert_allclose(g_ck, g_un, atol=1e-12, rtol=0)

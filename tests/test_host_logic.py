@@ -76,10 +76,10 @@ def test_large_plans_cover_every_wire_once(n, L):
     for mode in (plan_sim.AUTO, plan_sim.UNCOMPUTE, plan_sim.CHECKPOINT):
         plan = plan_sim.parse_plan(plan_sim.describe_plan(n, L, mode))
         check_large_plan(plan, n, L)
-    # automatic choice: the checkpoint schedule while its buffers fit 96 GiB
+    # automatic choice: the checkpoint schedule while its buffers fit 128 GiB
     auto = plan_sim.parse_plan(describe_plan(n, L))
     ck = plan_sim.parse_plan(plan_sim.describe_plan(n, L, plan_sim.CHECKPOINT))
-    fits = ck["bufs"] * 16 * 2 ** n <= 96 * 2 ** 30
+    fits = ck["bufs"] * 16 * 2 ** n <= 128 * 2 ** 30
     assert auto["mode"] == ("checkpoint" if fits else "uncompute")
     # uncompute: psi, lambda and the target of the inverse-ring scatter (not
     # needed when the leading layers are one read of lambda)
