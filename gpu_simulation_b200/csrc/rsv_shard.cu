@@ -194,20 +194,23 @@ __device__ __forceinline__ void unrot_pair_tan(const double4 c, double2 &a0, dou
   l1 = m1;
 }
 
-template <int TB0, int NB>
+// The gate helpers act on tile bits TB0..TB0+NB-1, held in register bits
+// RB0..RB0+NB-1 of the current layout.
+template <int TB0, int NB, int RB0 = 0>
 __device__ __forceinline__ void fwd_gates(const TileArgs &A, const double4 *cf, double2 (&a)[kR]) {
 #pragma unroll
   for (int j = 0; j < NB; ++j) {
     if (A.wire[TB0 + j] < 0) continue;
     const double4 c = cf[TB0 + j];
+    const int m = 1 << (RB0 + j);
     if (c.y > 0.0) {
 #pragma unroll
       for (int r = 0; r < kR; ++r)
-        if (!(r & (1 << j))) rot_pair<true>(c, a[r], a[r | (1 << j)]);
+        if (!(r & m)) rot_pair<true>(c, a[r], a[r | m]);
     } else {
 #pragma unroll
       for (int r = 0; r < kR; ++r)
-        if (!(r & (1 << j))) rot_pair<false>(c, a[r], a[r | (1 << j)]);
+        if (!(r & m)) rot_pair<false>(c, a[r], a[r | m]);
     }
   }
 }
@@ -216,29 +219,30 @@ __device__ __forceinline__ void fwd_gates(const TileArgs &A, const double4 *cf, 
 // adj_tan_coef); their sums are corrected by kap (the product of f^2 of the
 // pass's earlier gates), reduced over the warp and added to the warp's row of
 // the CTA record
-template <int TB0, int NB>
+template <int TB0, int NB, int RB0 = 0>
 __device__ __forceinline__ void adj_gates(const TileArgs &A, const double4 *cf, const double *kap, double2 (&a)[kR],
                                           double2 (&l)[kR], double *rec_row, int lane) {
 #pragma unroll
   for (int j = 0; j < NB; ++j) {
     if (A.wire[TB0 + j] < 0) continue;
     const double4 c = cf[TB0 + j];
+    const int m = 1 << (RB0 + j);
     // four partial sums each: the eight pairs' terms are not one dependent chain
     double gt4[4] = {0.0, 0.0, 0.0, 0.0}, gp4[4] = {0.0, 0.0, 0.0, 0.0};
     if (c.y > 0.0) {
       int q = 0;
 #pragma unroll
       for (int r = 0; r < kR; ++r)
-        if (!(r & (1 << j))) {
-          unrot_pair_tan<true>(c, a[r], a[r | (1 << j)], l[r], l[r | (1 << j)], gt4[q & 3], gp4[q & 3]);
+        if (!(r & m)) {
+          unrot_pair_tan<true>(c, a[r], a[r | m], l[r], l[r | m], gt4[q & 3], gp4[q & 3]);
           ++q;
         }
     } else {
       int q = 0;
 #pragma unroll
       for (int r = 0; r < kR; ++r)
-        if (!(r & (1 << j))) {
-          unrot_pair_tan<false>(c, a[r], a[r | (1 << j)], l[r], l[r | (1 << j)], gt4[q & 3], gp4[q & 3]);
+        if (!(r & m)) {
+          unrot_pair_tan<false>(c, a[r], a[r | m], l[r], l[r | m], gt4[q & 3], gp4[q & 3]);
           ++q;
         }
     }
@@ -308,16 +312,16 @@ __global__ void __launch_bounds__(kRotThreads, kRotCtasPerSm) rot_kernel(const _
     for (int r = 0; r < kR; ++r) a[r] = __ldcs(&psi[base | reg_off(r, rb)]);
     fwd_gates<7, 4>(A, cf, a);
     bool from_b = false;
-    if (A.need_b) {
+    if (A.need_c) {  // A -> C (tile bits 0..3) -> B (tile bits 4..6), stored from B
+      xpose<0, 2>(sm, tau, a);
+      fwd_gates<0, 4>(A, cf, a);
+      xpose<2, 1>(sm, tau, a);
+      fwd_gates<4, 3, 1>(A, cf, a);
+      from_b = true;
+    } else if (A.need_b) {
       xpose<0, 1>(sm, tau, a);
       fwd_gates<3, 4>(A, cf, a);
-      if (A.need_c) {
-        xpose<1, 2>(sm, tau, a);
-        fwd_gates<0, 3>(A, cf, a);
-        xpose<2, 0>(sm, tau, a);
-      } else {
-        from_b = true;
-      }
+      from_b = true;
     }
     u32 sbase = base;  // store addresses derived again (not kept live across the gates)
     asm volatile("" : "+r"(sbase));
@@ -345,8 +349,9 @@ __global__ void __launch_bounds__(kRotThreads, kAdjCtasPerSm) rot_adjoint_kernel
   const int tau = threadIdx.x, lane = tau & 31, warp = tau >> 5;
   if (tau == 0) {
     // the pass's gates in the order they are undone: layout A (tile bits
-    // 7..10), B (3..6), C (0..2)
-    constexpr int order[kT] = {7, 8, 9, 10, 3, 4, 5, 6, 0, 1, 2};
+    // 7..10), then C (0..3) and B (4..6) when bits 0..2 carry gates, else B
+    // (3..6); bits 0..2 carry none in the second case, so one list serves both
+    constexpr int order[kT] = {7, 8, 9, 10, 0, 1, 2, 3, 4, 5, 6};
     double run = 1.0, fprod = 1.0;
     for (int i = 0; i < kT; ++i) {
       const int tb = order[i];
@@ -382,16 +387,16 @@ __global__ void __launch_bounds__(kRotThreads, kAdjCtasPerSm) rot_adjoint_kernel
     }
     adj_gates<7, 4>(A, cf, kap, a, l, rec[warp], lane);
     bool from_b = false;
-    if (A.need_b) {
+    if (A.need_c) {  // A -> C (tile bits 0..3) -> B (tile bits 4..6), stored from B
+      xpose2<0, 2>(sm2, tau, a, l);
+      adj_gates<0, 4>(A, cf, kap, a, l, rec[warp], lane);
+      xpose2<2, 1>(sm2, tau, a, l);
+      adj_gates<4, 3, 1>(A, cf, kap, a, l, rec[warp], lane);
+      from_b = true;
+    } else if (A.need_b) {
       xpose2<0, 1>(sm2, tau, a, l);
       adj_gates<3, 4>(A, cf, kap, a, l, rec[warp], lane);
-      if (A.need_c) {
-        xpose2<1, 2>(sm2, tau, a, l);
-        adj_gates<0, 3>(A, cf, kap, a, l, rec[warp], lane);
-        xpose2<2, 0>(sm2, tau, a, l);
-      } else {
-        from_b = true;
-      }
+      from_b = true;
     }
     const double sf = pass_f;  // back to the true scale
 #pragma unroll
@@ -446,7 +451,7 @@ __global__ void rot_records_kernel(const __grid_constant__ TileArgs A, const dou
 // bits, partners taken from registers in the three layouts of rot_kernel, so
 // psi is read once per pass and each partner needs no further memory access.
 // Per-CTA records: the energy share of what the pass added.
-template <int TB0, int NB>
+template <int TB0, int NB, int RB0 = 0>
 __device__ __forceinline__ void xsum_gates(const TileArgs &A, double field, const double2 (&a)[kR],
                                            double2 (&acc)[kR], double (&e4)[4]) {
 #pragma unroll
@@ -454,7 +459,7 @@ __device__ __forceinline__ void xsum_gates(const TileArgs &A, double field, cons
     if (A.wire[TB0 + j] < 0) continue;
 #pragma unroll
     for (int r = 0; r < kR; ++r) {
-      const double2 p = a[r ^ (1 << j)];
+      const double2 p = a[r ^ (1 << (RB0 + j))];
       acc[r].x = fma(-field, p.x, acc[r].x);
       acc[r].y = fma(-field, p.y, acc[r].y);
       e4[r & 3] = fma(-field, fma(a[r].x, p.x, a[r].y * p.y), e4[r & 3]);
@@ -500,16 +505,16 @@ __global__ void __launch_bounds__(kRotThreads, kAdjCtasPerSm) energy_tile_kernel
     }
     xsum_gates<7, 4>(A, field, a, acc, e4);
     bool from_b = false;
-    if (A.need_b) {
+    if (A.need_c) {  // A -> C (tile bits 0..3) -> B (tile bits 4..6), stored from B
+      xpose2<0, 2>(sm2, tau, a, acc);
+      xsum_gates<0, 4>(A, field, a, acc, e4);
+      xpose2<2, 1>(sm2, tau, a, acc);
+      xsum_gates<4, 3, 1>(A, field, a, acc, e4);
+      from_b = true;
+    } else if (A.need_b) {
       xpose2<0, 1>(sm2, tau, a, acc);
       xsum_gates<3, 4>(A, field, a, acc, e4);
-      if (A.need_c) {
-        xpose2<1, 2>(sm2, tau, a, acc);
-        xsum_gates<0, 3>(A, field, a, acc, e4);
-        xpose<2, 0>(sm2, tau, acc);
-      } else {
-        from_b = true;
-      }
+      from_b = true;
     }
     u32 sbase = base;  // store addresses derived again (not kept live across the sums)
     asm volatile("" : "+r"(sbase));
